@@ -1,0 +1,204 @@
+/*
+ * mplbgpu.h - C ABI of the B200 lattice Boltzmann stream-collision path.
+ *
+ * The path replaces one MPLB time step, StreamCollision()
+ * (Src/evolution.cpp:137-193: moments, body force, BGK collision, halo
+ * transfer, streaming, boundary conditions), and the check-period calls that
+ * Iterate() makes around it (UpdateMacroVars3D/UpdateMacroVars,
+ * CalcResidualError, GetMaximumResidual: Src/evolution.cpp:102-135,
+ * Src/flowfield_wrapper.cpp:31-89, Src/flowfield.cpp:148-158).
+ *
+ * A context is built from a description of what the reference's setup API
+ * holds after Partition(): the blocks (DefineBlocks, Src/flowfield.cpp:189),
+ * the block connections (DefineBlockConnection, Src/flowfield.cpp:258-283),
+ * the boundary list in definition order (DefineBlockBoundary,
+ * Src/boundary.cpp:61-130), the lattice (DefineComponents, Src/model.cpp:208),
+ * tauRef, TimeStep() and the body-force type.  Every enum value below is the
+ * reference's own value, so a descriptor can be filled field by field from
+ * Block, Neighbor and BlockBoundary (Src/block.h:55-104, Src/boundary.h:85-93).
+ *
+ * Plain pointers and sizes only; all device memory belongs to the context.
+ * Host arrays are dense, z slowest and x fastest over a block's nodes
+ * (size[0] x size[1] x size[2], size[2] = 1 in 2D); distributions are
+ * point-major with Q = 9 or 19 values per node in the reference's lattice
+ * order (SetupD2Q9Latt / SetupD3Q19Latt, Src/model.cpp:99-131).
+ *
+ * All calls return an mplbgpu_status; there are no exceptions across the ABI.
+ * One context is driven by one host thread at a time.
+ */
+#ifndef MPLBGPU_H
+#define MPLBGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPLBGPU_ABI_VERSION 1
+
+typedef int mplbgpu_status;
+enum {
+    MPLBGPU_OK = 0,
+    MPLBGPU_ERR_INVALID = 1,     /* bad argument or inconsistent description */
+    MPLBGPU_ERR_UNSUPPORTED = 2, /* valid reference input this path rejects */
+    MPLBGPU_ERR_CUDA = 3,        /* CUDA runtime error (message has detail)  */
+    MPLBGPU_ERR_DIVERGED = 4,    /* non-finite or non-positive density seen  */
+    MPLBGPU_ERR_TIMEOUT = 5,     /* a bounded device wait gave up            */
+    MPLBGPU_ERR_NO_DEVICE = 6,   /* no usable CUDA device                    */
+    MPLBGPU_ERR_STATE = 7        /* call out of order (e.g. step before init) */
+};
+
+/* BoundarySurface, Src/boundary_host_device.h:7-29 */
+enum {
+    MPLBGPU_LEFT = 0, MPLBGPU_RIGHT = 1, MPLBGPU_TOP = 2, MPLBGPU_BOTTOM = 3,
+    MPLBGPU_FRONT = 4, MPLBGPU_BACK = 5,
+    MPLBGPU_LEFT_BACK = 50, MPLBGPU_LEFT_FRONT = 40,
+    MPLBGPU_RIGHT_BACK = 51, MPLBGPU_RIGHT_FRONT = 41,
+    MPLBGPU_TOP_BACK = 52, MPLBGPU_TOP_FRONT = 42,
+    MPLBGPU_BOTTOM_BACK = 53, MPLBGPU_BOTTOM_FRONT = 43,
+    MPLBGPU_LEFT_TOP = 20, MPLBGPU_LEFT_BOTTOM = 30,
+    MPLBGPU_RIGHT_TOP = 21, MPLBGPU_RIGHT_BOTTOM = 31
+};
+
+/* VertexType, Src/flowfield_host_device.h:21-37 */
+enum {
+    MPLBGPU_VT_FLUID = 10, MPLBGPU_VT_INLET = 11, MPLBGPU_VT_OUTLET = 12,
+    MPLBGPU_VT_MDPERIODIC = 13, MPLBGPU_VT_SYMMETRY = 14,
+    MPLBGPU_VT_FDPERIODIC = 15, MPLBGPU_VT_WALL = 1000,
+    MPLBGPU_VT_IMMERSED_SOLID = -1, MPLBGPU_VT_IMMERSED_BOUNDARY = -2,
+    MPLBGPU_VT_VIRTUAL_BOUNDARY = -3
+};
+
+/* BoundaryScheme, Src/boundary.h:70-83, plus one scheme of this path. */
+enum {
+    MPLBGPU_BC_KINETIC_DIFFUSE_WALL = 11,
+    MPLBGPU_BC_KINETIC_SPECULAR_WALL = 12,
+    MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST = 16,
+    MPLBGPU_BC_EXTRAPOL_PRESSURE_2ND = 17,
+    MPLBGPU_BC_MDPERIODIC = 18,
+    MPLBGPU_BC_FDPERIODIC = 19,
+    MPLBGPU_BC_BOUNCE_BACK = 20, /* reference: no kernel dispatched (no-op) */
+    MPLBGPU_BC_FREE_FLUX = 21,
+    MPLBGPU_BC_ZOUHE_VELOCITY = 22,
+    MPLBGPU_BC_EQN_NOSLIP = 23,
+    MPLBGPU_BC_EQM_DIFFUSE_REFL = 24,
+    MPLBGPU_BC_NONE = -1,
+    /* Not in the reference: link-wise halfway bounce-back with a moving-wall
+     * correction (the wall sits half a spacing outside the surface nodes). */
+    MPLBGPU_BC_HALFWAY_BOUNCE_BACK = 100
+};
+
+enum { MPLBGPU_D2Q9 = 9, MPLBGPU_D3Q19 = 19 };
+
+/* Storage/arithmetic forms of the distributions. */
+enum {
+    MPLBGPU_FP64 = 0,          /* reference arithmetic, FP64 storage          */
+    MPLBGPU_FP32_SHIFTED = 1,  /* stores f_i - w_i in FP32, FP32 arithmetic   */
+    MPLBGPU_FP16_SHIFTED = 2   /* stores f_i - w_i in FP16, FP32 arithmetic   */
+};
+
+/* BodyForceType, Src/model.h:101-106 */
+enum { MPLBGPU_FORCE_NONE = 0, MPLBGPU_FORCE_1ST = 1 };
+
+typedef struct {
+    int id;       /* block id as given to DefineBlocks */
+    int size[3];  /* nodes per axis; size[2] = 1 for 2D */
+} mplbgpu_block;
+
+typedef struct {  /* one entry of DefineBlockConnection */
+    int from_block;
+    int from_surface;
+    int to_block;
+    int to_surface;
+    int type;     /* VertexType: VirtualBoundary, MDPeriodic, FDPeriodic */
+} mplbgpu_connection;
+
+typedef struct {  /* one DefineBlockBoundary call, in call order */
+    int block;
+    int surface;
+    int scheme;       /* BoundaryScheme */
+    int vertex_type;  /* VertexType written to the surface's nodes */
+    double given[3];  /* GivenVars: (u, v[, w]) for walls, (rho) for
+                         ExtrapolPressure1ST, unused otherwise */
+} mplbgpu_boundary;
+
+typedef struct {
+    int abi_version;  /* MPLBGPU_ABI_VERSION */
+    int space_dim;    /* 2 or 3 */
+    int lattice;      /* MPLBGPU_D2Q9 (2D) or MPLBGPU_D3Q19 (3D) */
+    int precision;    /* MPLBGPU_FP64 / _FP32_SHIFTED / _FP16_SHIFTED */
+    int nblocks;
+    const mplbgpu_block* blocks;
+    int nconnections;
+    const mplbgpu_connection* connections;
+    int nboundaries;
+    const mplbgpu_boundary* boundaries;
+    double tau_ref;   /* Component::tauRef */
+    double dt;        /* TimeStep() */
+    double cs;        /* SoundSpeed(), sqrt(3) for D2Q9/D3Q19 */
+    int body_force;   /* BodyForceType */
+    double accel[3];  /* uniform body acceleration (MPLB units) */
+    int force_velocity; /* 1 when the velocity moments are Variable_U_Force
+                           etc.: u += dt*a/2 at Fluid/MDPeriodic nodes */
+} mplbgpu_desc;
+
+typedef struct mplbgpu_ctx mplbgpu_ctx;
+
+/* Builds node classification, boundary tables and halo plans, allocates the
+ * device state (Partition + DefineScheme + PrepareFlowField). */
+mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out);
+mplbgpu_status mplbgpu_destroy(mplbgpu_ctx* ctx);
+
+/* Message for the last failed call on ctx (ctx may be NULL for create). */
+const char* mplbgpu_last_error(const mplbgpu_ctx* ctx);
+
+/* Initial macroscopic state of one block followed by f = feq(rho, u)
+ * (app SetInitialMacrosVars + PreDefinedInitialCondition3D,
+ * Src/model_wrapper.cpp:347-391).  Any of u, v, w may be NULL (zero);
+ * rho NULL means 1. */
+mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
+                                  const double* rho, const double* u,
+                                  const double* v, const double* w);
+
+/* Replaces the distributions of one block (restart from saved f). */
+mplbgpu_status mplbgpu_upload_f(mplbgpu_ctx* ctx, int block, const double* f);
+
+/* nsteps calls of StreamCollision(). */
+mplbgpu_status mplbgpu_step(mplbgpu_ctx* ctx, int nsteps);
+
+/* Moments of the current f into the context's macro fields
+ * (UpdateMacroVars3D / UpdateMacroVars). */
+mplbgpu_status mplbgpu_update_macro(mplbgpu_ctx* ctx);
+
+/* CalcResidualError + GetMaximumResidual(check_period): per variable
+ * (rho, u, v[, w]) sum((q - q_old)^2) / sum(q^2) over all blocks, then the
+ * maximum of those divided by check_period * dt; q_old becomes q.  per_var
+ * (space_dim + 1 entries) may be NULL. */
+mplbgpu_status mplbgpu_residual(mplbgpu_ctx* ctx, int check_period,
+                                double* per_var, double* max_residual);
+
+/* Copies of the macro fields / distributions of one block to the host. */
+mplbgpu_status mplbgpu_download_macro(mplbgpu_ctx* ctx, int block,
+                                      double* rho, double* u, double* v,
+                                      double* w);
+mplbgpu_status mplbgpu_download_f(mplbgpu_ctx* ctx, int block, double* f);
+
+/* FP64 sum of rho over all nodes of all blocks, from the current f. */
+mplbgpu_status mplbgpu_mass(mplbgpu_ctx* ctx, double* mass);
+
+/* Scans the current state for non-finite or non-positive density:
+ * MPLBGPU_OK or MPLBGPU_ERR_DIVERGED. */
+mplbgpu_status mplbgpu_check_health(mplbgpu_ctx* ctx);
+
+/* Waits for all work issued on the context's stream. */
+mplbgpu_status mplbgpu_synchronize(mplbgpu_ctx* ctx);
+
+/* Number of kernel launches the context has issued since creation. */
+long long mplbgpu_launch_count(const mplbgpu_ctx* ctx);
+
+/* Device time of the most recent mplbgpu_step call's kernels (ms). */
+mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPLBGPU_H */

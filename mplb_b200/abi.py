@@ -1,0 +1,150 @@
+"""ctypes mirror of include/mplbgpu.h and the loader of the native library.
+
+The product path is the CUDA library ``libmplbgpu.so`` built next to this
+file; there is no Python or CPU fallback for the stream-collision step, so a
+missing or unloadable library raises ``NativeLibraryError``.
+"""
+import ctypes
+import os
+
+ABI_VERSION = 1
+
+OK = 0
+ERR_INVALID = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_DIVERGED = 4
+ERR_TIMEOUT = 5
+ERR_NO_DEVICE = 6
+ERR_STATE = 7
+STATUS_NAMES = {
+    OK: "OK", ERR_INVALID: "INVALID", ERR_UNSUPPORTED: "UNSUPPORTED",
+    ERR_CUDA: "CUDA", ERR_DIVERGED: "DIVERGED", ERR_TIMEOUT: "TIMEOUT",
+    ERR_NO_DEVICE: "NO_DEVICE", ERR_STATE: "STATE",
+}
+
+# BoundarySurface (Src/boundary_host_device.h:7-29)
+SURFACES = {
+    "Left": 0, "Right": 1, "Top": 2, "Bottom": 3, "Front": 4, "Back": 5,
+    "LeftBack": 50, "LeftFront": 40, "RightBack": 51, "RightFront": 41,
+    "TopBack": 52, "TopFront": 42, "BottomBack": 53, "BottomFront": 43,
+    "LeftTop": 20, "LeftBottom": 30, "RightTop": 21, "RightBottom": 31,
+}
+# VertexType (Src/flowfield_host_device.h:21-37)
+VERTEX_TYPES = {
+    "Fluid": 10, "Inlet": 11, "OutLet": 12, "MDPeriodic": 13, "Symmetry": 14,
+    "FDPeriodic": 15, "Wall": 1000, "ImmersedSolid": -1,
+    "ImmersedBoundary": -2, "VirtualBoundary": -3,
+}
+# BoundaryScheme (Src/boundary.h:70-83) + this path's halfway bounce-back.
+# "EQMDiffuseREfl" is the reference's own JSON spelling
+# (Src/configuration.cpp:86).
+BC_SCHEMES = {
+    "KineticDiffuseWall": 11, "KineticSpelluarWall": 12,
+    "ExtrapolPressure1ST": 16, "ExtrapolPressure2ND": 17, "MDPeriodic": 18,
+    "FDPeriodic": 19, "BounceBack": 20, "FreeFlux": 21, "ZouHeVelocity": 22,
+    "EQNNoSlip": 23, "EQMDiffuseRefl": 24, "EQMDiffuseREfl": 24, "None": -1,
+    "HalfwayBounceBack": 100,
+}
+D2Q9 = 9
+D3Q19 = 19
+FP64 = 0
+FP32_SHIFTED = 1
+FP16_SHIFTED = 2
+PRECISIONS = {"fp64": FP64, "fp32": FP32_SHIFTED, "fp16": FP16_SHIFTED}
+FORCE_NONE = 0
+FORCE_1ST = 1
+
+
+class Block(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int), ("size", ctypes.c_int * 3)]
+
+
+class Connection(ctypes.Structure):
+    _fields_ = [("from_block", ctypes.c_int), ("from_surface", ctypes.c_int),
+                ("to_block", ctypes.c_int), ("to_surface", ctypes.c_int),
+                ("type", ctypes.c_int)]
+
+
+class Boundary(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int), ("surface", ctypes.c_int),
+                ("scheme", ctypes.c_int), ("vertex_type", ctypes.c_int),
+                ("given", ctypes.c_double * 3)]
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int), ("space_dim", ctypes.c_int),
+        ("lattice", ctypes.c_int), ("precision", ctypes.c_int),
+        ("nblocks", ctypes.c_int), ("blocks", ctypes.POINTER(Block)),
+        ("nconnections", ctypes.c_int),
+        ("connections", ctypes.POINTER(Connection)),
+        ("nboundaries", ctypes.c_int),
+        ("boundaries", ctypes.POINTER(Boundary)),
+        ("tau_ref", ctypes.c_double), ("dt", ctypes.c_double),
+        ("cs", ctypes.c_double), ("body_force", ctypes.c_int),
+        ("accel", ctypes.c_double * 3), ("force_velocity", ctypes.c_int),
+    ]
+
+
+class NativeLibraryError(RuntimeError):
+    """The CUDA library is missing or failed to load."""
+
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(PACKAGE_DIR, "libmplbgpu.so")
+
+_lib = None
+
+_SIGNATURES = {
+    "mplbgpu_create": (ctypes.c_int, [ctypes.POINTER(Desc),
+                                      ctypes.POINTER(ctypes.c_void_p)]),
+    "mplbgpu_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "mplbgpu_init_macro": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] +
+                           [ctypes.c_void_p] * 4),
+    "mplbgpu_upload_f": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p]),
+    "mplbgpu_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mplbgpu_update_macro": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_residual": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
+    "mplbgpu_download_macro": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int] +
+                               [ctypes.c_void_p] * 4),
+    "mplbgpu_download_f": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p]),
+    "mplbgpu_mass": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mplbgpu_check_health": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "mplbgpu_last_step_ms": (ctypes.c_int, [ctypes.c_void_p,
+                                            ctypes.c_void_p]),
+}
+
+
+def exported_symbols():
+    """Names every build of the library must export (from mplbgpu.h)."""
+    return sorted(_SIGNATURES)
+
+
+def load_library(path=None):
+    """Loads libmplbgpu.so (fails loudly; there is no fallback path)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIBRARY_PATH
+    if not os.path.exists(p):
+        raise NativeLibraryError(
+            f"{p} is missing: build it with `python -m mplb_b200.build` "
+            "(nvcc, sm_100a)")
+    try:
+        lib = ctypes.CDLL(p)
+    except OSError as exc:
+        raise NativeLibraryError(f"cannot load {p}: {exc}") from exc
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
