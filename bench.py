@@ -1,0 +1,311 @@
+"""Benchmark of the fused stream-collision step.
+
+Workload (N = 1): the 3D lid-driven cavity, D3Q19 BGK, FP64, 256^3 nodes,
+lid 0.05 (lattice units) along +x on the z-max face, Re = 400 - MPLB's
+StreamCollision step through the C ABI.  One "step" is one StreamCollision
+over the whole 256^3 block.  Each population array is 2.7 GB, far larger
+than the 126 MB L2, so consecutive timed steps cannot hit in L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs its own cavity (no
+data-path exchange; weak scaling) and the value is the total node updates
+of all ranks divided by the slowest rank's device time.
+
+Printed (rank 0, one JSON line): MLUPS of the device-resident timed steps
+(`value`), the end-to-end MLUPS through the C ABI with host buffers (`e2e`:
+initial macroscopic fields uploaded from pinned host memory, K steps,
+moments downloaded), the HBM roofline of the step kernel (304 algorithmic
+bytes per node update), the reference's own CPU implementation timed on a
+bounded sample on this host (`cpu_baseline`), SM clocks sampled during the
+timed region and the number of kernel launches in it.
+
+--impl reference times the reference solver's CPU implementation (built
+from its own sources against the sequential OPS stand-in, OpenMP over all
+host cores) on the same workload instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
+                  ("fp32", 2): 72, ("fp16", 3): 76, ("fp16", 2): 36}
+METRIC = "MLUPS (D3Q19 FP64 3D lid-driven cavity 256^3)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="mplb", choices=["mplb", "reference"])
+    p.add_argument("--size", type=int, default=256)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(n):
+    from mplb_b200 import config
+    case = config.cavity(3, n, 0.05, re=400)
+    return case
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(case, warmup, steps, budget_s, threads=None):
+    """Times the reference's CPU implementation (oracle/_ref); returns
+    (MLUPS, steps timed, threads, seconds)."""
+    from oracle import pyoracle
+    if not pyoracle.reference_available("_omp"):
+        if not pyoracle.build_reference():
+            return None
+    threads = threads or os.cpu_count()
+    kind = "_omp" if threads > 1 else "_fast"
+    secs, cells = pyoracle.time_reference(case, warmup, 1, kind=kind,
+                                          threads=threads)
+    n = max(1, min(steps, int(budget_s / max(secs, 1e-6))))
+    if n > 1:
+        secs, cells = pyoracle.time_reference(case, warmup, n, kind=kind,
+                                              threads=threads)
+    return cells * n / secs / 1e6, n, threads, secs
+
+
+def dist_setup(args):
+    if args.gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, 0
+    import datetime
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    world = int(os.environ["WORLD_SIZE"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference_arm(args, rank, world):
+    case = workload(args.size)
+    if rank != 0:
+        return
+    res = cpu_reference(case, max(1, min(args.warmup, 1)), args.steps,
+                        budget_s=120)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU build (oracle/_ref) not present"}))
+        return
+    mlups, n, threads, secs = res
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mlups,
+        "unit": "MLUPS", "n_gpus": args.gpus, "steps": n,
+        "warmup": 1, "ms_per_step": secs / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
+                               "FP64, lid 0.05, Re 400",
+                   "nodes": case.nodes()},
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{n} StreamCollision steps of the "
+                                   f"{args.size}^3 cavity after 1 warm-up "
+                                   "step (reference sources + sequential "
+                                   "OPS stand-in, OpenMP)"},
+        "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    import numpy as np
+    import torch
+    from mplb_b200 import Solver, abi
+    torch.cuda.set_device(local)
+    case = workload(args.size)
+    nodes = case.nodes()
+    nx, ny, nz = case.size3(0)
+    lib = abi.load_library()
+
+    # --- device-resident timing ------------------------------------------
+    s = Solver(case, lib)
+    s.init_uniform()
+    s.stream_collision(args.warmup)
+    s.synchronize()
+    launches0 = s.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    s.stream_collision(args.steps)     # CUDA events on the library's stream
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = s.last_step_ms()
+    launches = s.launch_count() - launches0
+    ms_max = max_over_ranks(ms, world)
+    value = world * nodes * args.steps / (ms_max * 1e-3) / 1e6
+    kernel_ms = ms / args.steps          # one kernel launch per step
+    bpn = BYTES_PER_NODE[(case.precision, 3)]
+    achieved = bpn * nodes / (kernel_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    s.close()
+    del s
+
+    # --- end to end through the C ABI with host buffers ------------------
+    shp = (nz, ny, nx)
+    pinned = [torch.empty(shp, dtype=torch.float64, pin_memory=True)
+              for _ in range(8)]
+    pinned[0].fill_(1.0)
+    for t in pinned[1:4]:
+        t.zero_()
+    e = Solver(case, lib)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ptr = [t.data_ptr() for t in pinned]
+    rc = lib.mplbgpu_init_macro(e.h, 0, ptr[0], ptr[1], ptr[2], ptr[3])
+    if rc != 0:
+        raise RuntimeError(lib.mplbgpu_last_error(e.h).decode())
+    e.stream_collision(args.steps)
+    e.update_macro_vars()
+    rc = lib.mplbgpu_download_macro(e.h, 0, ptr[4], ptr[5], ptr[6], ptr[7])
+    if rc != 0:
+        raise RuntimeError(lib.mplbgpu_last_error(e.h).decode())
+    t1 = time.perf_counter()
+    barrier(world)
+    e2e_s = max_over_ranks(t1 - t0, world)
+    e2e = world * nodes * args.steps / e2e_s / 1e6
+    rho_sum = float(pinned[4].sum())
+    e.close()
+    if not np.isfinite(rho_sum):
+        raise RuntimeError("non-finite density after the end-to-end run")
+
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        res = cpu_reference(case, 1, 5, budget_s=25)
+        if res is not None:
+            mlups, n, threads, secs = res
+            cpu = {"value": mlups, "unit": "MLUPS", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"{n} StreamCollision steps of the same "
+                             f"{args.size}^3 cavity after 1 warm-up step "
+                             "(reference sources + sequential OPS stand-in, "
+                             "OpenMP)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
+                               "FP64, lid 0.05 (lattice), Re 400",
+                   "nodes_per_gpu": nodes, "parallelism": f"replicas{world}",
+                   "l2": "population arrays 2.7 GB each, larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind,
+                     "bytes_per_node": bpn, "traffic": None},
+        "e2e": {"value": e2e, "unit": "MLUPS",
+                "h2d_bytes_per_step": 4 * 8 * nodes / args.steps,
+                "d2h_bytes_per_step": 4 * 8 * nodes / args.steps},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

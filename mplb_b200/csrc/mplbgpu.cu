@@ -1,0 +1,700 @@
+// C ABI of the B200 stream-collision path (include/mplbgpu.h).
+//
+// A context owns one CUDA stream and, per block, two population arrays in
+// the halo layout of kernels.cuh (ping-pong between steps), the boundary
+// tables produced by plan.cpp, the stale/deferred stores and the dense
+// macroscopic fields used by the residual.  Every entry point validates its
+// arguments and returns a status; CUDA errors are reported with the failing
+// call in mplbgpu_last_error.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mplbgpu.h"
+#include "kernels.cuh"
+#include "plan.h"
+
+using namespace mplb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBlock {
+    BlockDev dev{};
+    double* pop[2] = {nullptr, nullptr};
+    RegionInfo* regions = nullptr;
+    RegionOp* ops = nullptr;
+    double* stale = nullptr;
+    double* fdef = nullptr;
+    int4* dregions = nullptr;
+    double* macro[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* macro_old[4] = {nullptr, nullptr, nullptr, nullptr};
+    struct DOp {
+        DeferredSeg* segs = nullptr;
+        int nseg = 0;
+        long long total = 0;
+    };
+    std::vector<DOp> dops;
+};
+
+struct DevHalo {
+    HaloDev h{};
+    uint8_t* prev = nullptr;
+    int from = 0, to = 0;
+};
+
+}  // namespace
+
+struct mplbgpu_ctx {
+    Plan plan;
+    PhysConst pc{};
+    std::vector<DevBlock> blocks;
+    std::vector<DevHalo> halos;
+    int cur = 0;            // pop[cur] holds the latest g
+    bool initial = true;    // pop[1 - cur] holds f^0 itself
+    bool halos_pending = true;
+    std::vector<bool> initialised;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0;
+    long long launches = 0;
+    double* part = nullptr;     // reduction partials
+    unsigned long long* bad = nullptr;
+    double* scratch = nullptr;  // dense f staging
+    size_t scratch_elems = 0;
+    std::string err;
+};
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kRedBlocks = 1024;
+constexpr int kRedThreads = 256;
+
+int SetErr(mplbgpu_ctx* c, int code, const std::string& m) {
+    if (c) c->err = m; else g_create_error = m;
+    return code;
+}
+
+#define CK(call)                                                            \
+    do {                                                                    \
+        cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess)                                              \
+            return SetErr(ctx, MPLBGPU_ERR_CUDA,                            \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CK_LAUNCH()                                                         \
+    do {                                                                    \
+        ctx->launches++;                                                    \
+        cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess)                                              \
+            return SetErr(ctx, MPLBGPU_ERR_CUDA,                            \
+                          std::string("kernel launch: ") +                  \
+                              cudaGetErrorString(e_));                      \
+    } while (0)
+
+dim3 NodeGrid(const BlockPlan& B, int dim) {
+    return dim3((B.n[0] + kThreads - 1) / kThreads, B.n[1],
+                dim == 3 ? B.n[2] : 1);
+}
+
+DevBlock* FindBlock(mplbgpu_ctx* ctx, int id) {
+    for (size_t i = 0; i < ctx->plan.blocks.size(); i++)
+        if (ctx->plan.blocks[i].id == id) return &ctx->blocks[i];
+    return nullptr;
+}
+
+const BlockPlan* FindPlan(mplbgpu_ctx* ctx, int id) {
+    for (const BlockPlan& B : ctx->plan.blocks)
+        if (B.id == id) return &B;
+    return nullptr;
+}
+
+void FreeAll(mplbgpu_ctx* c) {
+    for (DevBlock& b : c->blocks) {
+        cudaFree(b.pop[0]);
+        cudaFree(b.pop[1]);
+        cudaFree(b.regions);
+        cudaFree(b.ops);
+        cudaFree(b.stale);
+        cudaFree(b.fdef);
+        cudaFree(b.dregions);
+        for (int m = 0; m < 4; m++) {
+            cudaFree(b.macro[m]);
+            cudaFree(b.macro_old[m]);
+        }
+        for (auto& d : b.dops) cudaFree(d.segs);
+    }
+    for (DevHalo& h : c->halos) cudaFree(h.prev);
+    cudaFree(c->part);
+    cudaFree(c->bad);
+    cudaFree(c->scratch);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+int EnsureScratch(mplbgpu_ctx* ctx, size_t elems) {
+    if (ctx->scratch_elems >= elems) return MPLBGPU_OK;
+    cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_elems = 0;
+    CK(cudaMalloc(&ctx->scratch, elems * sizeof(double)));
+    ctx->scratch_elems = elems;
+    return MPLBGPU_OK;
+}
+
+int RunHalos(mplbgpu_ctx* ctx) {
+    const int dim = ctx->plan.dim;
+    for (DevHalo& h : ctx->halos) {
+        DevBlock& fb = ctx->blocks[h.from];
+        DevBlock& tb = ctx->blocks[h.to];
+        const long long cells =
+            (long long)h.h.iter[0] * h.h.iter[1] * h.h.iter[2];
+        const unsigned grid = (unsigned)((cells + 255) / 256);
+        if (dim == 3)
+            HaloKernel<3><<<grid, 256, 0, ctx->stream>>>(
+                h.h, fb.dev, tb.dev, fb.pop[ctx->cur], fb.pop[1 - ctx->cur],
+                tb.pop[ctx->cur]);
+        else
+            HaloKernel<2><<<grid, 256, 0, ctx->stream>>>(
+                h.h, fb.dev, tb.dev, fb.pop[ctx->cur], fb.pop[1 - ctx->cur],
+                tb.pop[ctx->cur]);
+        CK_LAUNCH();
+    }
+    ctx->halos_pending = false;
+    return MPLBGPU_OK;
+}
+
+template <int D>
+int StepOnce(mplbgpu_ctx* ctx) {
+    const int src = ctx->cur, dst = 1 - ctx->cur;
+    for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+        DevBlock& b = ctx->blocks[bi];
+        const BlockPlan& B = ctx->plan.blocks[bi];
+        StepKernel<D, kModeStep><<<NodeGrid(B, D), kThreads, 0, ctx->stream>>>(
+            b.dev, ctx->pc, b.pop[src], b.pop[dst], nullptr, nullptr, nullptr,
+            nullptr);
+        CK_LAUNCH();
+        if (B.ndeferred > 0) {
+            const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
+            DeferredStreamKernel<D><<<g, kThreads, 0, ctx->stream>>>(b.dev,
+                                                                     b.pop[src]);
+            CK_LAUNCH();
+            for (auto& d : b.dops) {
+                const unsigned gd = (unsigned)((d.total + kThreads - 1) / kThreads);
+                DeferredOpKernel<D><<<gd, kThreads, 0, ctx->stream>>>(
+                    b.dev, ctx->pc, b.pop[src], d.segs, d.nseg, d.total);
+                CK_LAUNCH();
+            }
+            DeferredFinishKernel<D, kModeStep><<<g, kThreads, 0, ctx->stream>>>(
+                b.dev, ctx->pc, b.pop[dst], nullptr, nullptr, nullptr, nullptr);
+            CK_LAUNCH();
+        }
+    }
+    ctx->cur = dst;
+    ctx->initial = false;
+    return RunHalos(ctx);
+}
+
+// Current f -> moments (kModeMacro) or point-major f (kModeF) of one block.
+template <int D, int MODE>
+int Observe(mplbgpu_ctx* ctx, size_t bi, double* o0, double* o1, double* o2,
+            double* o3) {
+    DevBlock& b = ctx->blocks[bi];
+    const BlockPlan& B = ctx->plan.blocks[bi];
+    const int prev = 1 - ctx->cur;
+    if (ctx->initial) {
+        DirectObserveKernel<D, MODE><<<NodeGrid(B, D), kThreads, 0,
+                                       ctx->stream>>>(b.dev, ctx->pc,
+                                                      b.pop[prev], o0, o1, o2,
+                                                      o3);
+        CK_LAUNCH();
+        return MPLBGPU_OK;
+    }
+    StepKernel<D, MODE><<<NodeGrid(B, D), kThreads, 0, ctx->stream>>>(
+        b.dev, ctx->pc, b.pop[prev], nullptr, o0, o1, o2, o3);
+    CK_LAUNCH();
+    if (B.ndeferred > 0) {
+        const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
+        DeferredFinishKernel<D, MODE><<<g, kThreads, 0, ctx->stream>>>(
+            b.dev, ctx->pc, nullptr, o0, o1, o2, o3);
+        CK_LAUNCH();
+    }
+    return MPLBGPU_OK;
+}
+
+int UpdateMacro(mplbgpu_ctx* ctx) {
+    for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+        DevBlock& b = ctx->blocks[bi];
+        int rc = ctx->plan.dim == 3
+                     ? Observe<3, kModeMacro>(ctx, bi, b.macro[0], b.macro[1],
+                                              b.macro[2], b.macro[3])
+                     : Observe<2, kModeMacro>(ctx, bi, b.macro[0], b.macro[1],
+                                              b.macro[2], nullptr);
+        if (rc != MPLBGPU_OK) return rc;
+    }
+    return MPLBGPU_OK;
+}
+
+int CheckReady(mplbgpu_ctx* ctx) {
+    for (size_t i = 0; i < ctx->initialised.size(); i++)
+        if (!ctx->initialised[i])
+            return SetErr(ctx, MPLBGPU_ERR_STATE,
+                          "block " + std::to_string(ctx->plan.blocks[i].id) +
+                              " has no initial state (mplbgpu_init_macro or "
+                              "mplbgpu_upload_f)");
+    return MPLBGPU_OK;
+}
+
+template <int D>
+int InitBlock(mplbgpu_ctx* ctx, size_t bi, const double* d_rho,
+              const double* d_u, const double* d_v, const double* d_w,
+              const double* d_f) {
+    DevBlock& b = ctx->blocks[bi];
+    const BlockPlan& B = ctx->plan.blocks[bi];
+    InitKernel<D><<<NodeGrid(B, D), kThreads, 0, ctx->stream>>>(
+        b.dev, ctx->pc, d_rho, d_u, d_v, d_w, d_f, b.pop[1 - ctx->cur],
+        b.pop[ctx->cur]);
+    CK_LAUNCH();
+    return MPLBGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
+    mplbgpu_ctx* ctx = nullptr;
+    if (!desc || !out) return SetErr(nullptr, MPLBGPU_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return SetErr(nullptr, MPLBGPU_ERR_NO_DEVICE, "no CUDA device");
+    std::unique_ptr<mplbgpu_ctx> c(new mplbgpu_ctx);
+    std::string err;
+    int rc = BuildPlan(*desc, &c->plan, &err);
+    if (rc != MPLBGPU_OK) return SetErr(nullptr, rc, err);
+    if (c->plan.precision != MPLBGPU_FP64)
+        return SetErr(nullptr, MPLBGPU_ERR_UNSUPPORTED,
+                      "only the FP64 form is built in this library");
+    ctx = c.get();
+    const Plan& P = c->plan;
+    PhysConst& pc = c->pc;
+    pc.cs = P.cs;
+    pc.omc = P.omc;
+    pc.tw = P.tw;
+    pc.force = P.body_force == MPLBGPU_FORCE_1ST;
+    pc.force_vel = P.force_velocity;
+    for (int a = 0; a < 3; a++) pc.hdta[a] = P.hdta[a];
+    for (int i = 0; i < kMaxQ; i++) {
+        pc.cf[i] = P.cf[i];
+        pc.w[i] = P.w[i];
+    }
+    auto fail_cuda = [&](cudaError_t e, const char* what) {
+        std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+        FreeAll(c.get());
+        c->blocks.clear();
+        c->halos.clear();
+        return SetErr(nullptr, MPLBGPU_ERR_CUDA, m);
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) !=
+        cudaSuccess)
+        return fail_cuda(e, "cudaStreamCreate");
+    if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev1)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+    c->blocks.resize(P.blocks.size());
+    c->initialised.assign(P.blocks.size(), false);
+    const int Q = P.Q;
+    for (size_t bi = 0; bi < P.blocks.size(); bi++) {
+        const BlockPlan& B = P.blocks[bi];
+        DevBlock& b = c->blocks[bi];
+        const size_t popbytes = (size_t)Q * B.popstride * sizeof(double);
+        for (int k = 0; k < 2; k++) {
+            if ((e = cudaMalloc(&b.pop[k], popbytes)) != cudaSuccess)
+                return fail_cuda(e, "cudaMalloc(populations)");
+            if ((e = cudaMemsetAsync(b.pop[k], 0, popbytes, c->stream)) !=
+                cudaSuccess)
+                return fail_cuda(e, "cudaMemset(populations)");
+        }
+        if ((e = cudaMalloc(&b.regions, sizeof(B.region))) != cudaSuccess ||
+            (e = cudaMemcpy(b.regions, B.region, sizeof(B.region),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail_cuda(e, "region table");
+        if (!B.ops.empty()) {
+            const size_t ob = B.ops.size() * sizeof(RegionOp);
+            if ((e = cudaMalloc(&b.ops, ob)) != cudaSuccess ||
+                (e = cudaMemcpy(b.ops, B.ops.data(), ob,
+                                cudaMemcpyHostToDevice)) != cudaSuccess)
+                return fail_cuda(e, "op table");
+        }
+        if (B.nstale > 0 &&
+            (e = cudaMalloc(&b.stale, (size_t)B.nstale * Q * sizeof(double))) !=
+                cudaSuccess)
+            return fail_cuda(e, "stale store");
+        std::vector<int4> dreg;
+        if (B.ndeferred > 0) {
+            if ((e = cudaMalloc(&b.fdef, (size_t)B.ndeferred * Q *
+                                             sizeof(double))) != cudaSuccess)
+                return fail_cuda(e, "deferred store");
+            for (int r = 0; r < kNumRegions; r++) {
+                const RegionInfo& R = B.region[r];
+                if (R.cls == kDeferred)
+                    dreg.push_back(make_int4(
+                        r, (int)R.side_base,
+                        R.ext[0] * R.ext[1] * R.ext[2], 0));
+            }
+            if ((e = cudaMalloc(&b.dregions, dreg.size() * sizeof(int4))) !=
+                    cudaSuccess ||
+                (e = cudaMemcpy(b.dregions, dreg.data(),
+                                dreg.size() * sizeof(int4),
+                                cudaMemcpyHostToDevice)) != cudaSuccess)
+                return fail_cuda(e, "deferred regions");
+            for (const DeferredOp& dop : B.dops) {
+                std::vector<DeferredSeg> segs;
+                long long start = 0;
+                for (const DeferredSegment& s : dop.segments) {
+                    const RegionInfo& R = B.region[s.region];
+                    const long long cnt =
+                        (long long)R.ext[0] * R.ext[1] * R.ext[2];
+                    segs.push_back({s.region, s.op, start, cnt});
+                    start += cnt;
+                }
+                DevBlock::DOp d;
+                d.nseg = (int)segs.size();
+                d.total = start;
+                if ((e = cudaMalloc(&d.segs, segs.size() * sizeof(DeferredSeg))) !=
+                        cudaSuccess ||
+                    (e = cudaMemcpy(d.segs, segs.data(),
+                                    segs.size() * sizeof(DeferredSeg),
+                                    cudaMemcpyHostToDevice)) != cudaSuccess)
+                    return fail_cuda(e, "deferred segments");
+                b.dops.push_back(d);
+            }
+        }
+        const size_t nodes = (size_t)B.nodes();
+        for (int m = 0; m < P.dim + 1; m++) {
+            if ((e = cudaMalloc(&b.macro[m], nodes * sizeof(double))) !=
+                    cudaSuccess ||
+                (e = cudaMalloc(&b.macro_old[m], nodes * sizeof(double))) !=
+                    cudaSuccess)
+                return fail_cuda(e, "macro fields");
+            cudaMemsetAsync(b.macro[m], 0, nodes * sizeof(double), c->stream);
+            cudaMemsetAsync(b.macro_old[m], 0, nodes * sizeof(double),
+                            c->stream);
+        }
+        BlockDev& d = b.dev;
+        for (int a = 0; a < 3; a++) d.n[a] = B.n[a];
+        d.xoff = B.xoff;
+        d.pitch = B.pitch;
+        d.plane = B.plane;
+        d.popstride = B.popstride;
+        d.regions = b.regions;
+        d.ops = b.ops;
+        d.stale = b.stale;
+        d.fdef = b.fdef;
+        d.ndef = B.ndeferred;
+        d.dregions = b.dregions;
+        d.ndregions = (int)dreg.size();
+    }
+    for (const HaloCopy& h : P.halos) {
+        DevHalo dh;
+        dh.from = h.from;
+        dh.to = h.to;
+        for (int a = 0; a < 3; a++) {
+            dh.h.iter[a] = h.iter[a];
+            dh.h.fbase[a] = h.fbase[a];
+            dh.h.tbase[a] = h.tbase[a];
+        }
+        dh.h.pops = h.pops;
+        dh.h.prev = nullptr;
+        if (h.any_prev) {
+            if ((e = cudaMalloc(&dh.prev, h.prev.size())) != cudaSuccess ||
+                (e = cudaMemcpy(dh.prev, h.prev.data(), h.prev.size(),
+                                cudaMemcpyHostToDevice)) != cudaSuccess)
+                return fail_cuda(e, "halo masks");
+            dh.h.prev = dh.prev;
+        }
+        c->halos.push_back(dh);
+    }
+    if ((e = cudaMalloc(&c->part, 2 * kRedBlocks * sizeof(double))) !=
+            cudaSuccess ||
+        (e = cudaMalloc(&c->bad, sizeof(unsigned long long))) != cudaSuccess)
+        return fail_cuda(e, "reduction buffers");
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+        return fail_cuda(e, "cudaStreamSynchronize");
+    *out = c.release();
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_destroy(mplbgpu_ctx* ctx) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    cudaStreamSynchronize(ctx->stream);
+    FreeAll(ctx);
+    delete ctx;
+    return MPLBGPU_OK;
+}
+
+const char* mplbgpu_last_error(const mplbgpu_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
+                                  const double* rho, const double* u,
+                                  const double* v, const double* w) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    DevBlock* b = FindBlock(ctx, block);
+    const BlockPlan* B = FindPlan(ctx, block);
+    if (!b) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    if (!ctx->initial) {
+        // a new initial state after steps: every block starts again
+        std::fill(ctx->initialised.begin(), ctx->initialised.end(), false);
+    }
+    const int dim = ctx->plan.dim;
+    const size_t nodes = (size_t)B->nodes();
+    const double* src[4] = {rho, u, v, w};
+    std::vector<double> fill(nodes);
+    for (int m = 0; m < dim + 1; m++) {
+        if (src[m]) {
+            CK(cudaMemcpyAsync(b->macro[m], src[m], nodes * sizeof(double),
+                               cudaMemcpyHostToDevice, ctx->stream));
+        } else {
+            std::fill(fill.begin(), fill.end(), m == 0 ? 1.0 : 0.0);
+            CK(cudaMemcpyAsync(b->macro[m], fill.data(), nodes * sizeof(double),
+                               cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        // CopyCurrentMacroVar after PreDefinedInitialCondition3D
+        CK(cudaMemcpyAsync(b->macro_old[m], b->macro[m], nodes * sizeof(double),
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    const size_t bi = (size_t)(b - ctx->blocks.data());
+    int rc = dim == 3 ? InitBlock<3>(ctx, bi, b->macro[0], b->macro[1],
+                                     b->macro[2], b->macro[3], nullptr)
+                      : InitBlock<2>(ctx, bi, b->macro[0], b->macro[1],
+                                     b->macro[2], nullptr, nullptr);
+    if (rc != MPLBGPU_OK) return rc;
+    ctx->initial = true;
+    ctx->halos_pending = true;
+    ctx->initialised[bi] = true;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_upload_f(mplbgpu_ctx* ctx, int block, const double* f) {
+    if (!ctx || !f) return ctx ? SetErr(ctx, MPLBGPU_ERR_INVALID, "null f")
+                               : MPLBGPU_ERR_INVALID;
+    DevBlock* b = FindBlock(ctx, block);
+    const BlockPlan* B = FindPlan(ctx, block);
+    if (!b) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    if (!ctx->initial)
+        std::fill(ctx->initialised.begin(), ctx->initialised.end(), false);
+    const size_t elems = (size_t)B->nodes() * ctx->plan.Q;
+    int rc = EnsureScratch(ctx, elems);
+    if (rc != MPLBGPU_OK) return rc;
+    CK(cudaMemcpyAsync(ctx->scratch, f, elems * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    const size_t bi = (size_t)(b - ctx->blocks.data());
+    rc = ctx->plan.dim == 3
+             ? InitBlock<3>(ctx, bi, nullptr, nullptr, nullptr, nullptr,
+                            ctx->scratch)
+             : InitBlock<2>(ctx, bi, nullptr, nullptr, nullptr, nullptr,
+                            ctx->scratch);
+    if (rc != MPLBGPU_OK) return rc;
+    ctx->initial = true;
+    ctx->halos_pending = true;
+    ctx->initialised[bi] = true;
+    // macro fields: moments of the uploaded f, q_old = q
+    rc = ctx->plan.dim == 3
+             ? Observe<3, kModeMacro>(ctx, bi, b->macro[0], b->macro[1],
+                                      b->macro[2], b->macro[3])
+             : Observe<2, kModeMacro>(ctx, bi, b->macro[0], b->macro[1],
+                                      b->macro[2], nullptr);
+    if (rc != MPLBGPU_OK) return rc;
+    for (int m = 0; m < ctx->plan.dim + 1; m++)
+        CK(cudaMemcpyAsync(b->macro_old[m], b->macro[m],
+                           (size_t)B->nodes() * sizeof(double),
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_step(mplbgpu_ctx* ctx, int nsteps) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    if (nsteps < 0) return SetErr(ctx, MPLBGPU_ERR_INVALID, "nsteps < 0");
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    if (ctx->halos_pending) {
+        rc = RunHalos(ctx);
+        if (rc != MPLBGPU_OK) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int s = 0; s < nsteps; s++) {
+        rc = ctx->plan.dim == 3 ? StepOnce<3>(ctx) : StepOnce<2>(ctx);
+        if (rc != MPLBGPU_OK) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_update_macro(mplbgpu_ctx* ctx) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    rc = UpdateMacro(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_residual(mplbgpu_ctx* ctx, int check_period,
+                                double* per_var, double* max_residual) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    if (check_period <= 0)
+        return SetErr(ctx, MPLBGPU_ERR_INVALID, "check_period must be > 0");
+    const int nv = ctx->plan.dim + 1;
+    double diff[4] = {0, 0, 0, 0}, sum[4] = {0, 0, 0, 0};
+    std::vector<double> part(2 * kRedBlocks);
+    for (int m = 0; m < nv; m++) {
+        for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+            DevBlock& b = ctx->blocks[bi];
+            const long long n = ctx->plan.blocks[bi].nodes();
+            ResidualPartialKernel<<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(
+                b.macro[m], b.macro_old[m], n, ctx->part);
+            CK_LAUNCH();
+            CK(cudaMemcpyAsync(part.data(), ctx->part,
+                               part.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            for (int k = 0; k < kRedBlocks; k++) {
+                diff[m] += part[2 * k];
+                sum[m] += part[2 * k + 1];
+            }
+        }
+    }
+    // GetMaximumResidual, Src/flowfield.cpp:148-158
+    double mx = 0;
+    for (int m = 0; m < nv; m++) {
+        const double res = diff[m] / sum[m];
+        if (per_var) per_var[m] = res;
+        const double rel = res / (check_period * ctx->plan.dt);
+        if (mx <= rel) mx = rel;
+    }
+    if (max_residual) *max_residual = mx;
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_download_macro(mplbgpu_ctx* ctx, int block, double* rho,
+                                      double* u, double* v, double* w) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    DevBlock* b = FindBlock(ctx, block);
+    const BlockPlan* B = FindPlan(ctx, block);
+    if (!b) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    double* dst[4] = {rho, u, v, w};
+    const size_t bytes = (size_t)B->nodes() * sizeof(double);
+    for (int m = 0; m < ctx->plan.dim + 1; m++)
+        if (dst[m])
+            CK(cudaMemcpyAsync(dst[m], b->macro[m], bytes,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_download_f(mplbgpu_ctx* ctx, int block, double* f) {
+    if (!ctx || !f) return ctx ? SetErr(ctx, MPLBGPU_ERR_INVALID, "null f")
+                               : MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    DevBlock* b = FindBlock(ctx, block);
+    const BlockPlan* B = FindPlan(ctx, block);
+    if (!b) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    const size_t elems = (size_t)B->nodes() * ctx->plan.Q;
+    rc = EnsureScratch(ctx, elems);
+    if (rc != MPLBGPU_OK) return rc;
+    const size_t bi = (size_t)(b - ctx->blocks.data());
+    rc = ctx->plan.dim == 3
+             ? Observe<3, kModeF>(ctx, bi, ctx->scratch, nullptr, nullptr,
+                                  nullptr)
+             : Observe<2, kModeF>(ctx, bi, ctx->scratch, nullptr, nullptr,
+                                  nullptr);
+    if (rc != MPLBGPU_OK) return rc;
+    CK(cudaMemcpyAsync(f, ctx->scratch, elems * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return MPLBGPU_OK;
+}
+
+static int SumRho(mplbgpu_ctx* ctx, double* total, unsigned long long* nbad) {
+    int rc = UpdateMacro(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    CK(cudaMemsetAsync(ctx->bad, 0, sizeof(unsigned long long), ctx->stream));
+    double s = 0;
+    std::vector<double> part(kRedBlocks);
+    for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+        SumPartialKernel<<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(
+            ctx->blocks[bi].macro[0], ctx->plan.blocks[bi].nodes(), ctx->part,
+            ctx->bad);
+        CK_LAUNCH();
+        CK(cudaMemcpyAsync(part.data(), ctx->part, part.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (double v : part) s += v;
+    }
+    CK(cudaMemcpyAsync(nbad, ctx->bad, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *total = s;
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_mass(mplbgpu_ctx* ctx, double* mass) {
+    if (!ctx || !mass) return MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    unsigned long long nbad = 0;
+    return SumRho(ctx, mass, &nbad);
+}
+
+mplbgpu_status mplbgpu_check_health(mplbgpu_ctx* ctx) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    double s = 0;
+    unsigned long long nbad = 0;
+    rc = SumRho(ctx, &s, &nbad);
+    if (rc != MPLBGPU_OK) return rc;
+    if (nbad)
+        return SetErr(ctx, MPLBGPU_ERR_DIVERGED,
+                      std::to_string(nbad) +
+                          " nodes with non-finite or non-positive density");
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_synchronize(mplbgpu_ctx* ctx) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return MPLBGPU_OK;
+}
+
+long long mplbgpu_launch_count(const mplbgpu_ctx* ctx) {
+    return ctx ? ctx->launches : 0;
+}
+
+mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return MPLBGPU_ERR_INVALID;
+    *ms = ctx->last_ms;
+    return MPLBGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,711 @@
+// Host-side planning of the fused stream-collision step (see plan.h).
+// Compiled with -ffp-contract=off: the FP64 constants below are computed in
+// the reference's operation order so that kernels using them reproduce the
+// reference bit for bit.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "lattice.h"
+
+namespace mplb {
+namespace {
+
+constexpr int kVtFluid = MPLBGPU_VT_FLUID;
+constexpr int kVtMD = MPLBGPU_VT_MDPERIODIC;
+constexpr int kVtVB = MPLBGPU_VT_VIRTUAL_BOUNDARY;
+constexpr int kVtSolid = MPLBGPU_VT_IMMERSED_SOLID;
+
+enum { kDvIncoming = 1, kDvOutgoing = 2, kDvParallel = 3, kDvInvalid = -1 };
+
+struct Lat {
+    int D, Q;
+    int c[kMaxQ][3];
+    int opp[kMaxQ];
+    double w[kMaxQ];
+};
+
+template <int D>
+void FillLat(Lat* L) {
+    using LL = Lattice<D>;
+    L->D = D;
+    L->Q = LL::Q;
+    for (int i = 0; i < LL::Q; i++) {
+        L->c[i][0] = LL::cx(i);
+        L->c[i][1] = LL::cy(i);
+        L->c[i][2] = LL::cz(i);
+        L->opp[i] = LL::opp(i);
+    }
+    // SetupD2Q9Latt / SetupD3Q19Latt, Src/model.cpp:99-131
+    double cls[3];
+    if (D == 2) {
+        cls[0] = 4.0 / 9.0;
+        cls[1] = 1.0 / 9.0;
+        cls[2] = 1.0 / 36.0;
+    } else {
+        cls[0] = 1 / ((double)3);
+        cls[1] = 1 / ((double)18);
+        cls[2] = 1 / ((double)36);
+    }
+    for (int i = 0; i < LL::Q; i++) L->w[i] = cls[LL::wclass(i)];
+}
+
+// CalcBGKFeq(l, rho, u, v[, w], T = 1, polyOrder = 2) / (w_l rho):
+// the bracket "res" of Src/model_host_device.h:34-82, same operation order.
+double FeqRes(const Lat& L, double CS, int l, const double* u) {
+    const double T = 1;
+    const double XI0 = L.c[l][0], XI1 = L.c[l][1], XI2 = L.c[l][2];
+    double cu, c2, u2;
+    if (L.D == 2) {
+        cu = (CS * XI0 * u[0] + CS * XI1 * u[1]);
+        c2 = (CS * XI0 * CS * XI0 + CS * XI1 * CS * XI1);
+        u2 = u[0] * u[0] + u[1] * u[1];
+    } else {
+        cu = (CS * XI0 * u[0] + CS * XI1 * u[1] + CS * XI2 * u[2]);
+        c2 = (CS * XI0 * CS * XI0 + CS * XI1 * CS * XI1 + CS * XI2 * CS * XI2);
+        u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    }
+    const double cu2 = cu * cu;
+    return 1.0 + cu + 0.5 * (cu2 - u2 + (T - 1.0) * (c2 - L.D));
+}
+
+// Block::RangeStart / RangeEnd (Src/block.cpp:14-97), including the
+// TopBack/TopFront y-range left whole by the OP_3D test at Src/block.cpp:35.
+void SurfaceRange(int dim, const int n[3], int s, int r[6]) {
+    for (int a = 0; a < 3; a++) {
+        r[2 * a] = 0;
+        r[2 * a + 1] = n[a];
+    }
+    const bool d3 = dim == 3;
+    if (s == MPLBGPU_RIGHT || s == MPLBGPU_RIGHT_TOP ||
+        s == MPLBGPU_RIGHT_BOTTOM ||
+        (d3 && (s == MPLBGPU_RIGHT_FRONT || s == MPLBGPU_RIGHT_BACK)))
+        r[0] = n[0] - 1;
+    if (s == MPLBGPU_LEFT || s == MPLBGPU_LEFT_BOTTOM || s == MPLBGPU_LEFT_TOP ||
+        (d3 && (s == MPLBGPU_LEFT_FRONT || s == MPLBGPU_LEFT_BACK)))
+        r[1] = 1;
+    if (s == MPLBGPU_TOP || s == MPLBGPU_LEFT_TOP || s == MPLBGPU_RIGHT_TOP)
+        r[2] = n[1] - 1;
+    if (s == MPLBGPU_BOTTOM || s == MPLBGPU_LEFT_BOTTOM ||
+        s == MPLBGPU_RIGHT_BOTTOM ||
+        (d3 && (s == MPLBGPU_BOTTOM_BACK || s == MPLBGPU_BOTTOM_FRONT)))
+        r[3] = 1;
+    if (d3) {
+        if (s == MPLBGPU_FRONT || s == MPLBGPU_LEFT_FRONT ||
+            s == MPLBGPU_RIGHT_FRONT || s == MPLBGPU_TOP_FRONT ||
+            s == MPLBGPU_BOTTOM_FRONT)
+            r[4] = n[2] - 1;
+        if (s == MPLBGPU_BACK || s == MPLBGPU_LEFT_BACK ||
+            s == MPLBGPU_RIGHT_BACK || s == MPLBGPU_TOP_BACK ||
+            s == MPLBGPU_BOTTOM_BACK)
+            r[5] = 1;
+    }
+}
+
+bool ValidSurface(int dim, int s) {
+    switch (s) {
+        case MPLBGPU_LEFT: case MPLBGPU_RIGHT: case MPLBGPU_TOP:
+        case MPLBGPU_BOTTOM: case MPLBGPU_LEFT_TOP: case MPLBGPU_LEFT_BOTTOM:
+        case MPLBGPU_RIGHT_TOP: case MPLBGPU_RIGHT_BOTTOM:
+            return true;
+        case MPLBGPU_FRONT: case MPLBGPU_BACK: case MPLBGPU_LEFT_BACK:
+        case MPLBGPU_LEFT_FRONT: case MPLBGPU_RIGHT_BACK:
+        case MPLBGPU_RIGHT_FRONT: case MPLBGPU_TOP_BACK:
+        case MPLBGPU_TOP_FRONT: case MPLBGPU_BOTTOM_BACK:
+        case MPLBGPU_BOTTOM_FRONT:
+            return dim == 3;
+        default:
+            return false;
+    }
+}
+
+// Faces making up a surface or edge: axis and side (0 min, 1 max).
+int SurfaceFaces(int s, int axis[2], int side[2]) {
+    struct F { int s, a, sd; };
+    static const F tab[] = {
+        {MPLBGPU_LEFT, 0, 0}, {MPLBGPU_RIGHT, 0, 1}, {MPLBGPU_BOTTOM, 1, 0},
+        {MPLBGPU_TOP, 1, 1}, {MPLBGPU_BACK, 2, 0}, {MPLBGPU_FRONT, 2, 1},
+        {MPLBGPU_LEFT_BACK, 0, 0}, {MPLBGPU_LEFT_BACK, 2, 0},
+        {MPLBGPU_LEFT_FRONT, 0, 0}, {MPLBGPU_LEFT_FRONT, 2, 1},
+        {MPLBGPU_RIGHT_BACK, 0, 1}, {MPLBGPU_RIGHT_BACK, 2, 0},
+        {MPLBGPU_RIGHT_FRONT, 0, 1}, {MPLBGPU_RIGHT_FRONT, 2, 1},
+        {MPLBGPU_TOP_BACK, 1, 1}, {MPLBGPU_TOP_BACK, 2, 0},
+        {MPLBGPU_TOP_FRONT, 1, 1}, {MPLBGPU_TOP_FRONT, 2, 1},
+        {MPLBGPU_BOTTOM_BACK, 1, 0}, {MPLBGPU_BOTTOM_BACK, 2, 0},
+        {MPLBGPU_BOTTOM_FRONT, 1, 0}, {MPLBGPU_BOTTOM_FRONT, 2, 1},
+        {MPLBGPU_LEFT_TOP, 0, 0}, {MPLBGPU_LEFT_TOP, 1, 1},
+        {MPLBGPU_LEFT_BOTTOM, 0, 0}, {MPLBGPU_LEFT_BOTTOM, 1, 0},
+        {MPLBGPU_RIGHT_TOP, 0, 1}, {MPLBGPU_RIGHT_TOP, 1, 1},
+        {MPLBGPU_RIGHT_BOTTOM, 0, 1}, {MPLBGPU_RIGHT_BOTTOM, 1, 0},
+    };
+    int n = 0;
+    for (const F& f : tab) {
+        if (f.s == s && n < 2) {
+            axis[n] = f.a;
+            side[n] = f.sd;
+            n++;
+        }
+    }
+    return n;
+}
+
+bool InRange(const int p[3], const int r[6]) {
+    return p[0] >= r[0] && p[0] < r[1] && p[1] >= r[2] && p[1] < r[3] &&
+           p[2] >= r[4] && p[2] < r[5];
+}
+
+// Boundary faces of a node: axes on which it is the first/last node, with
+// the inward sign (+1 on the first node: the "P" codes).
+int NodeFaces(int dim, const int n[3], const int p[3], int axis[3],
+              int sign[3]) {
+    int k = 0;
+    for (int a = 0; a < dim; a++) {
+        if (p[a] == 0) {
+            axis[k] = a;
+            sign[k++] = 1;
+        } else if (p[a] == n[a] - 1) {
+            axis[k] = a;
+            sign[k++] = -1;
+        }
+    }
+    return k;
+}
+
+// VertexGeometryType of a node from its position: the code written last by
+// SetBlockGeometryProperty (Src/flowfield_wrapper.cpp:291-623).
+int GeometryCode(int dim, const int n[3], const int p[3]) {
+    int axis[3], sign[3];
+    const int k = NodeFaces(dim, n, p, axis, sign);
+    auto face = [](int a, int s) { return 10 * (a + 1) + (s > 0 ? 0 : 1); };
+    if (k == 0) return 0;
+    if (k == 1) return face(axis[0], sign[0]);
+    if (k == 2) return face(axis[0], sign[0]) * 1000 + face(axis[1], sign[1]) * 10;
+    return face(axis[0], sign[0]) * 100000 + face(axis[1], sign[1]) * 1000 +
+           face(axis[2], sign[2]) * 10;
+}
+
+// FindBdyDvType / FindBdyDvType3D, Src/boundary_host_device.h:47-706, in
+// inward components; 3D corners keep the reference's labelling.
+int DvType(const Lat& L, int nf, const int axis[3], const int sign[3], int l) {
+    int c[3];
+    for (int q = 0; q < nf; q++) c[q] = sign[q] * L.c[l][axis[q]];
+    if (nf == 1) return c[0] < 0 ? kDvIncoming : (c[0] == 0 ? kDvParallel
+                                                              : kDvOutgoing);
+    if (nf == 2) {
+        if ((c[0] <= 0 && c[1] < 0) || (c[0] < 0 && c[1] == 0))
+            return kDvIncoming;
+        if ((c[0] >= 0 && c[1] > 0) || (c[0] > 0 && c[1] == 0))
+            return kDvOutgoing;
+        return kDvParallel;
+    }
+    if (nf == 3) {
+        if (c[0] == 0 && c[1] == 0 && c[2] == 0) return kDvParallel;
+        if (c[0] <= 0 && c[1] <= 0 && c[2] <= 0) return kDvOutgoing;
+        if (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) return kDvIncoming;
+        return kDvParallel;
+    }
+    return kDvInvalid;
+}
+
+bool FluidLike(int vt) { return vt == kVtFluid || vt == kVtMD; }
+bool PullsAll(int vt) { return vt == kVtFluid || vt == kVtMD || vt == kVtVB; }
+
+// EQMDiffuseRefl constants (KerCutCellEQMDiffuseRefl(3D),
+// Src/boundary_kernel.inc:534-613, 1184-1276).
+RegionOp MakeEqm(const Lat& L, double CS, int nf, const int axis[3],
+                 const int sign[3], const double* given) {
+    RegionOp op{};
+    op.kind = kOpEqm;
+    op.nb_axis = -1;
+    const double u = given[0], v = given[1], w = L.D == 3 ? given[2] : 0.0;
+    const double uw[3] = {u, v, w};
+    double rhoParallel = 0, deltaRho = 0;
+    for (int l = 0; l < L.Q; l++) {
+        const double cx = CS * (double)L.c[l][0];
+        const double cy = CS * (double)L.c[l][1];
+        const double cz = CS * (double)L.c[l][2];
+        const double cu = L.D == 3 ? (cx * u + cy * v + cz * w)
+                                   : (cx * u + cy * v);
+        switch (DvType(L, nf, axis, sign, l)) {
+            case kDvIncoming:
+                op.in_mask |= 1u << l;
+                break;
+            case kDvOutgoing:
+                op.out_mask |= 1u << l;
+                deltaRho += (2 * L.w[l]) * cu;
+                op.b[l] = cu;
+                break;
+            case kDvParallel:
+                op.par_mask |= 1u << l;
+                rhoParallel += L.w[l] * 1 * FeqRes(L, CS, l, uw);
+                op.a[l] = FeqRes(L, CS, l, uw);
+                break;
+            default:
+                break;
+        }
+    }
+    op.denom = 1 - deltaRho - rhoParallel;
+    return op;
+}
+
+// KerCutCellExtrapolPressure1ST(3D), Src/boundary_kernel.inc:404-488,
+// 894-1182: copy mask and source neighbour for the surface being treated.
+RegionOp MakeExtrapol(const Lat& L, int nf, const int axis[3],
+                      const int sign[3], int surface, double rho_given) {
+    RegionOp op{};
+    op.kind = kOpExtrapol;
+    op.rho_given = rho_given;
+    op.nb_axis = -1;
+    int sa[2], ss[2];
+    const int sf = SurfaceFaces(surface, sa, ss);
+    const bool face = sf == 1 && (surface == MPLBGPU_LEFT ||
+                                  surface == MPLBGPU_RIGHT ||
+                                  surface == MPLBGPU_TOP ||
+                                  surface == MPLBGPU_BOTTOM ||
+                                  surface == MPLBGPU_FRONT ||
+                                  surface == MPLBGPU_BACK);
+    if (nf == 1) {
+        op.nb_axis = axis[0];
+        op.nb_sign = sign[0];
+    } else if (face) {
+        const int want = ss[0] == 0 ? 1 : -1;
+        for (int q = 0; q < nf; q++) {
+            if (axis[q] == sa[0] && sign[q] == want) {
+                op.nb_axis = axis[q];
+                op.nb_sign = sign[q];
+            }
+        }
+    }
+    for (int l = 0; l < L.Q; l++) {
+        int c[3] = {0, 0, 0};
+        for (int q = 0; q < nf; q++) c[q] = sign[q] * L.c[l][axis[q]];
+        bool copy = false;
+        if (nf == 1) copy = c[0] > 0;
+        if (nf == 2) copy = (c[0] >= 0 && c[1] > 0) || (c[0] > 0 && c[1] == 0);
+        if (nf == 3)
+            copy = (c[0] >= 0 && c[1] >= 0 && c[2] >= 0) &&
+                   (c[0] != 0 || c[1] != 0 || c[2] != 0);
+        if (copy && op.nb_axis >= 0) op.in_mask |= 1u << l;
+    }
+    return op;
+}
+
+// Halfway bounce-back of this path: populations whose upstream node lies
+// beyond one of the surface's faces.
+RegionOp MakeHbb(const Lat& L, double CS, const int n[3], const int p[3],
+                 int surface, const double* given) {
+    RegionOp op{};
+    op.kind = kOpHbb;
+    op.nb_axis = -1;
+    int sa[2], ss[2];
+    const int sf = SurfaceFaces(surface, sa, ss);
+    for (int l = 0; l < L.Q; l++) {
+        bool beyond = false;
+        for (int q = 0; q < sf; q++) {
+            const int s = p[sa[q]] - L.c[l][sa[q]];
+            beyond = beyond || (ss[q] ? (s > n[sa[q]] - 1) : (s < 0));
+        }
+        if (!beyond) continue;
+        op.out_mask |= 1u << l;
+        double cu = CS * (double)L.c[l][0] * given[0] +
+                    CS * (double)L.c[l][1] * given[1];
+        if (L.D == 3) cu = cu + CS * (double)L.c[l][2] * given[2];
+        op.b[l] = 2.0 * L.w[l] * cu;
+    }
+    return op;
+}
+
+bool Dispatched(int scheme) {
+    return scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL ||
+           scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST ||
+           scheme == MPLBGPU_BC_HALFWAY_BOUNCE_BACK;
+}
+
+}  // namespace
+
+int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
+    auto fail = [&](int code, const std::string& m) {
+        *err = m;
+        return code;
+    };
+    if (d.abi_version != MPLBGPU_ABI_VERSION)
+        return fail(MPLBGPU_ERR_INVALID, "abi_version mismatch");
+    if (!((d.space_dim == 2 && d.lattice == MPLBGPU_D2Q9) ||
+          (d.space_dim == 3 && d.lattice == MPLBGPU_D3Q19)))
+        return fail(MPLBGPU_ERR_UNSUPPORTED,
+                    "only D2Q9 (2D) and D3Q19 (3D) are supported");
+    if (d.precision < MPLBGPU_FP64 || d.precision > MPLBGPU_FP16_SHIFTED)
+        return fail(MPLBGPU_ERR_INVALID, "unknown precision");
+    if (d.nblocks < 1 || !d.blocks)
+        return fail(MPLBGPU_ERR_INVALID, "no blocks");
+    if (!(d.dt > 0) || !(d.cs > 0) || !(d.tau_ref + 0.5 * d.dt > 0))
+        return fail(MPLBGPU_ERR_INVALID, "dt, cs and tau must be positive");
+    if (d.body_force != MPLBGPU_FORCE_NONE && d.body_force != MPLBGPU_FORCE_1ST)
+        return fail(MPLBGPU_ERR_UNSUPPORTED, "unknown body force type");
+
+    Plan& P = *plan;
+    P.dim = d.space_dim;
+    P.Q = d.lattice;
+    P.precision = d.precision;
+    P.elem_bytes = d.precision == MPLBGPU_FP64 ? 8
+                   : d.precision == MPLBGPU_FP32_SHIFTED ? 4 : 2;
+    P.cs = d.cs;
+    P.tau = d.tau_ref;
+    P.dt = d.dt;
+    // KerCollideBGKIsothermal3D, Src/model_kernel.inc:428-438
+    const double tau = d.tau_ref;
+    P.omega = d.dt / (tau + 0.5 * d.dt);
+    P.omc = 1 - P.omega;
+    P.tw = tau * P.omega;
+    P.body_force = d.body_force;
+    P.force_velocity = d.force_velocity ? 1 : 0;
+    Lat L{};
+    if (P.dim == 2) FillLat<2>(&L); else FillLat<3>(&L);
+    for (int a = 0; a < 3; a++) {
+        P.accel[a] = a < P.dim ? d.accel[a] : 0.0;
+        // KerCalcUForce3D: u += dt * a / 2
+        P.hdta[a] = (d.dt * P.accel[a] / 2);
+    }
+    for (int l = 0; l < P.Q; l++) {
+        P.w[l] = L.w[l];
+        // CalcBodyForce, Src/model_host_device.h:25-32
+        double cf = 0;
+        for (int a = 0; a < P.dim; a++)
+            cf += d.cs * (double)L.c[l][a] * P.accel[a];
+        P.cf[l] = cf;
+    }
+
+    // blocks in id order (the reference keeps them in a std::map)
+    std::vector<int> order(d.nblocks);
+    for (int i = 0; i < d.nblocks; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        return d.blocks[x].id < d.blocks[y].id;
+    });
+    for (int i = 1; i < d.nblocks; i++)
+        if (d.blocks[order[i]].id == d.blocks[order[i - 1]].id)
+            return fail(MPLBGPU_ERR_INVALID, "duplicate block id");
+    const int xoff = 32 / P.elem_bytes;
+    P.blocks.resize(d.nblocks);
+    for (int i = 0; i < d.nblocks; i++) {
+        BlockPlan& B = P.blocks[i];
+        const mplbgpu_block& src = d.blocks[order[i]];
+        B.id = src.id;
+        B.index = i;
+        for (int a = 0; a < 3; a++) {
+            B.n[a] = a < P.dim ? src.size[a] : 1;
+            if (a < P.dim && B.n[a] < 2)
+                return fail(MPLBGPU_ERR_INVALID,
+                            "every block needs at least 2 nodes per axis");
+        }
+        B.xoff = xoff;
+        B.pitch = ((xoff + B.n[0] + 1 + xoff - 1) / xoff) * xoff;
+        B.plane = B.pitch * (B.n[1] + 2);
+        const long long zs = P.dim == 3 ? B.n[2] + 2 : 1;
+        const long long ps = B.plane * zs;
+        const long long align = 256 / P.elem_bytes;
+        B.popstride = ((ps + align - 1) / align) * align;
+    }
+    auto blockIndex = [&](int id) {
+        for (const BlockPlan& B : P.blocks)
+            if (B.id == id) return B.index;
+        return -1;
+    };
+
+    // boundaries
+    for (int k = 0; k < d.nboundaries; k++) {
+        const mplbgpu_boundary& bc = d.boundaries[k];
+        if (blockIndex(bc.block) < 0)
+            return fail(MPLBGPU_ERR_INVALID, "boundary on an unknown block");
+        if (!ValidSurface(P.dim, bc.surface))
+            return fail(MPLBGPU_ERR_INVALID, "invalid boundary surface");
+        if (bc.scheme == MPLBGPU_BC_FDPERIODIC)
+            return fail(MPLBGPU_ERR_UNSUPPORTED,
+                        "FDPeriodic copies from a halo of f that the "
+                        "reference never transfers (use MDPeriodic)");
+        if (bc.vertex_type == kVtSolid ||
+            bc.vertex_type == MPLBGPU_VT_IMMERSED_BOUNDARY)
+            return fail(MPLBGPU_ERR_UNSUPPORTED,
+                        "immersed-solid boundary node types are not supported");
+        if (bc.scheme == MPLBGPU_BC_HALFWAY_BOUNCE_BACK) {
+            int sa[2], ss[2];
+            if (SurfaceFaces(bc.surface, sa, ss) < 1)
+                return fail(MPLBGPU_ERR_INVALID, "bad bounce-back surface");
+        }
+    }
+
+    // regions
+    for (BlockPlan& B : P.blocks) {
+        long long stale_nodes = 0, deferred_nodes = 0;
+        for (int r = 0; r < kNumRegions; r++) {
+            RegionInfo& R = B.region[r];
+            R = RegionInfo{};
+            const int rc[3] = {r % 3, (r / 3) % 3, r / 9};
+            bool empty = false;
+            for (int a = 0; a < 3; a++) {
+                if (a >= P.dim) {
+                    R.org[a] = 0;
+                    R.ext[a] = 1;
+                    if (rc[a] != 1) empty = true;
+                    continue;
+                }
+                const int n = B.n[a];
+                if (rc[a] == 0) { R.org[a] = 0; R.ext[a] = 1; }
+                if (rc[a] == 2) { R.org[a] = n - 1; R.ext[a] = 1; }
+                if (rc[a] == 1) { R.org[a] = 1; R.ext[a] = n - 2; }
+                if (R.ext[a] <= 0) empty = true;
+            }
+            if (empty) {
+                R.cls = -1;
+                continue;
+            }
+            const int* p = R.org;
+            // node type: bulk Fluid, faces unset (0), then every boundary in
+            // definition order (SetBulkandHaloNodesType /
+            // SetBoundaryNodeType, Src/flowfield_wrapper.cpp:625-788)
+            bool bulk = true;
+            for (int a = 0; a < P.dim; a++)
+                bulk = bulk && p[a] >= 1 && p[a] < B.n[a] - 1;
+            int vt = bulk ? kVtFluid : 0;
+            for (int k = 0; k < d.nboundaries; k++) {
+                const mplbgpu_boundary& bc = d.boundaries[k];
+                if (bc.block != B.id) continue;
+                int rg[6];
+                SurfaceRange(P.dim, B.n, bc.surface, rg);
+                if (bc.vertex_type == kVtVB) {
+                    const int s = bc.surface;
+                    if (s == MPLBGPU_LEFT || s == MPLBGPU_RIGHT) {
+                        rg[2]++; rg[3]--;
+                        if (P.dim == 3) { rg[4]++; rg[5]--; }
+                    }
+                    if (s == MPLBGPU_TOP || s == MPLBGPU_BOTTOM) {
+                        rg[0]++; rg[1]--;
+                        if (P.dim == 3) { rg[4]++; rg[5]--; }
+                    }
+                    if (P.dim == 3 &&
+                        (s == MPLBGPU_FRONT || s == MPLBGPU_BACK)) {
+                        rg[0]++; rg[1]--; rg[2]++; rg[3]--;
+                    }
+                }
+                if (InRange(p, rg)) vt = bc.vertex_type;
+            }
+            R.vt = vt;
+            R.vg = GeometryCode(P.dim, B.n, p);
+            R.fluidlike = FluidLike(vt) ? 1 : 0;
+            int axis[3], sign[3];
+            const int nf = NodeFaces(P.dim, B.n, p, axis, sign);
+            // KerStream3D selection, Src/scheme_kernel.inc:1400-2051
+            uint32_t pull = 0;
+            for (int l = 0; l < P.Q; l++) {
+                bool take = PullsAll(vt);
+                const bool rest = L.c[l][0] == 0 && L.c[l][1] == 0 &&
+                                  L.c[l][2] == 0;
+                if (!take && (rest || nf > 0)) {
+                    take = true;
+                    if (!rest)
+                        for (int q = 0; q < nf; q++)
+                            if (sign[q] * L.c[l][axis[q]] > 0) take = false;
+                }
+                if (take) pull |= 1u << l;
+            }
+            R.pull = pull;
+            // boundary programme, definition order
+            std::vector<RegionOp> prog;
+            for (int k = 0; k < d.nboundaries; k++) {
+                const mplbgpu_boundary& bc = d.boundaries[k];
+                if (bc.block != B.id || !Dispatched(bc.scheme)) continue;
+                int rg[6];
+                SurfaceRange(P.dim, B.n, bc.surface, rg);
+                if (!InRange(p, rg)) continue;
+                if (bc.scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL)
+                    prog.push_back(MakeEqm(L, P.cs, nf, axis, sign, bc.given));
+                else if (bc.scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST)
+                    prog.push_back(MakeExtrapol(L, nf, axis, sign, bc.surface,
+                                                bc.given[0]));
+                else
+                    prog.push_back(MakeHbb(L, P.cs, B.n, p, bc.surface,
+                                           bc.given));
+            }
+            bool extrapol = false;
+            uint32_t written = 0, readfirst = 0;
+            for (const RegionOp& op : prog) {
+                if (op.kind == kOpExtrapol) extrapol = true;
+                if (op.kind == kOpEqm) {
+                    uint32_t reads = op.in_mask;
+                    for (int l = 0; l < P.Q; l++)
+                        if (op.out_mask >> l & 1u) reads |= 1u << L.opp[l];
+                    readfirst |= reads & ~written;
+                    written |= op.out_mask | op.par_mask;
+                } else if (op.kind == kOpHbb) {
+                    written |= op.out_mask;
+                }
+            }
+            const uint32_t all = (P.Q == 32) ? ~0u : ((1u << P.Q) - 1u);
+            if (prog.empty() && PullsAll(vt)) {
+                R.cls = kPure;
+            } else if (extrapol || (int)prog.size() > kMaxOps ||
+                       (readfirst & ~pull & written) != 0) {
+                R.cls = kDeferred;
+            } else {
+                R.cls = kLocal;
+            }
+            R.stale = all & ~pull & ~written;
+            R.nops = 0;
+            for (const RegionOp& op : prog) {
+                if (R.nops < kMaxOps) R.op[R.nops++] = (int)B.ops.size();
+                B.allops[r].push_back((int)B.ops.size());
+                B.ops.push_back(op);
+            }
+        }
+        // nodes whose post-boundary value an ExtrapolPressure1ST reads must
+        // be materialised too
+        for (int r = 0; r < kNumRegions; r++) {
+            const RegionInfo& R = B.region[r];
+            if (R.cls != kDeferred) continue;
+            for (int oi : B.allops[r]) {
+                const RegionOp& op = B.ops[oi];
+                if (op.kind != kOpExtrapol || op.nb_axis < 0) continue;
+                int q[3] = {R.org[0], R.org[1], R.org[2]};
+                q[op.nb_axis] += op.nb_sign;
+                int rc[3];
+                for (int a = 0; a < 3; a++)
+                    rc[a] = a < P.dim ? RegionCoord(q[a], B.n[a]) : 1;
+                RegionInfo& N = B.region[rc[0] + 3 * rc[1] + 9 * rc[2]];
+                if (N.cls == kLocal) N.cls = kDeferred;
+            }
+        }
+        for (int r = 0; r < kNumRegions; r++) {
+            RegionInfo& R = B.region[r];
+            const long long cnt = (long long)R.ext[0] * R.ext[1] * R.ext[2];
+            R.side_base = -1;
+            if (R.cls == kLocal && R.stale != 0) {
+                R.side_base = stale_nodes;
+                stale_nodes += cnt;
+            } else if (R.cls == kDeferred) {
+                R.side_base = deferred_nodes;
+                deferred_nodes += cnt;
+            }
+        }
+        B.nstale = stale_nodes;
+        B.ndeferred = deferred_nodes;
+        // deferred programme: every boundary, in definition order, on the
+        // deferred regions it covers
+        if (B.ndeferred > 0) {
+            for (int k = 0; k < d.nboundaries; k++) {
+                const mplbgpu_boundary& bc = d.boundaries[k];
+                if (bc.block != B.id || !Dispatched(bc.scheme)) continue;
+                int rg[6];
+                SurfaceRange(P.dim, B.n, bc.surface, rg);
+                DeferredOp dop;
+                for (int r = 0; r < kNumRegions; r++) {
+                    const RegionInfo& R = B.region[r];
+                    if (R.cls != kDeferred || !InRange(R.org, rg)) continue;
+                    int axis[3], sign[3];
+                    const int nf = NodeFaces(P.dim, B.n, R.org, axis, sign);
+                    RegionOp op;
+                    if (bc.scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL)
+                        op = MakeEqm(L, P.cs, nf, axis, sign, bc.given);
+                    else if (bc.scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST)
+                        op = MakeExtrapol(L, nf, axis, sign, bc.surface,
+                                          bc.given[0]);
+                    else
+                        op = MakeHbb(L, P.cs, B.n, R.org, bc.surface,
+                                     bc.given);
+                    dop.segments.push_back({r, (int)B.ops.size()});
+                    B.ops.push_back(op);
+                }
+                if (!dop.segments.empty()) B.dops.push_back(dop);
+            }
+        }
+    }
+
+    // halo transfers: Field::CreateHalos order, Src/field.h:215-395
+    for (const BlockPlan& FB : P.blocks) {
+        for (int s = 0; s <= 5; s++) {
+            for (int c = 0; c < d.nconnections; c++) {
+                const mplbgpu_connection& cn = d.connections[c];
+                if (cn.from_block != FB.id || cn.from_surface != s) continue;
+                const int ti = blockIndex(cn.to_block);
+                if (ti < 0)
+                    return fail(MPLBGPU_ERR_INVALID,
+                                "connection to an unknown block");
+                const BlockPlan& TB = P.blocks[ti];
+                const int axis = s < 2 ? 0 : (s < 4 ? 1 : 2);
+                if (axis >= P.dim)
+                    return fail(MPLBGPU_ERR_INVALID,
+                                "connection surface not in this dimension");
+                HaloCopy h;
+                h.from = FB.index;
+                h.to = ti;
+                h.axis = axis;
+                const bool maxside = s == MPLBGPU_RIGHT || s == MPLBGPU_TOP ||
+                                     s == MPLBGPU_FRONT;
+                const int disp = (cn.type == MPLBGPU_VT_FDPERIODIC ||
+                                  cn.type == kVtMD || cn.type == kVtVB) ? -1
+                                                                        : 0;
+                for (int a = 0; a < 3; a++) {
+                    const int hd = a < P.dim ? 1 : 0;
+                    h.iter[a] = FB.n[a] + 2 * hd;
+                    h.fbase[a] = -hd;
+                    h.tbase[a] = -hd;
+                    if (a != axis && a < P.dim && FB.n[a] != TB.n[a])
+                        return fail(MPLBGPU_ERR_INVALID,
+                                    "connected blocks differ in size");
+                }
+                h.iter[axis] = 1;
+                if (maxside) {
+                    h.fbase[axis] = FB.n[axis] + disp;
+                    h.tbase[axis] = -1;
+                    h.to_low = 1;
+                } else {
+                    h.fbase[axis] = 0;
+                    h.tbase[axis] = TB.n[axis];
+                    h.to_low = 0;
+                }
+                h.pops = 0;
+                for (int l = 0; l < P.Q; l++)
+                    if (L.c[l][axis] == (h.to_low ? 1 : -1)) h.pops |= 1u << l;
+                h.any_prev = false;
+                P.halos.push_back(h);
+            }
+        }
+    }
+    // A source cell that a later transfer of the same step overwrites, and
+    // no earlier one did, still holds last step's value in the reference.
+    for (size_t t = 0; t < P.halos.size(); t++) {
+        HaloCopy& h = P.halos[t];
+        const BlockPlan& FB = P.blocks[h.from];
+        const long long cells = (long long)h.iter[0] * h.iter[1] * h.iter[2];
+        h.prev.assign(cells, 0);
+        for (long long cidx = 0; cidx < cells; cidx++) {
+            const int i = (int)(cidx % h.iter[0]);
+            const int j = (int)((cidx / h.iter[0]) % h.iter[1]);
+            const int k = (int)(cidx / ((long long)h.iter[0] * h.iter[1]));
+            const int sp[3] = {h.fbase[0] + i, h.fbase[1] + j, h.fbase[2] + k};
+            bool inside = true;
+            for (int a = 0; a < P.dim; a++)
+                inside = inside && sp[a] >= 0 && sp[a] < FB.n[a];
+            if (inside) continue;
+            bool before = false, after = false;
+            for (size_t u = 0; u < P.halos.size(); u++) {
+                const HaloCopy& o = P.halos[u];
+                if (u == t || o.to != h.from) continue;
+                bool in = true;
+                for (int a = 0; a < 3; a++)
+                    in = in && sp[a] >= o.tbase[a] &&
+                         sp[a] < o.tbase[a] + o.iter[a];
+                if (!in) continue;
+                if (u < t) before = true; else after = true;
+            }
+            if (!before && after) {
+                h.prev[cidx] = 1;
+                h.any_prev = true;
+            }
+        }
+        if (!h.any_prev) h.prev.clear();
+    }
+    return MPLBGPU_OK;
+}
+
+}  // namespace mplb

@@ -1,0 +1,135 @@
+// Host-side planning of the fused stream-collision step.
+//
+// MPLB assigns every node a VertexType and a VertexGeometryType
+// (PrepareFlowField, Src/flowfield.cpp:224-244) and applies boundary
+// kernels surface by surface in definition order (ImplementBoundary3D,
+// Src/boundary.cpp:379-386).  Every node range the reference uses (bulk,
+// halo shells, faces, edges, corners, the VirtualBoundary-shrunk faces) is
+// a union of the 3^D "regions" of a block - each axis split into
+// {first node, interior, last node} - so all per-node semantics are
+// resolved here once per region:
+//   PURE     : fluid-like node with no boundary kernel: pull all Q
+//              populations, moments, BGK collision.
+//   LOCAL    : boundary node whose boundary kernels only read the node
+//              itself: pulled populations + a short in-register program of
+//              EQMDiffuseRefl / halfway bounce-back operations.
+//   DEFERRED : node whose program reads a neighbour's post-boundary value
+//              (ExtrapolPressure1ST) or is read by one: processed by the
+//              sequential deferred kernels on an explicit f store.
+// The halo transfer plan reproduces Field::CreateHalos order
+// (Src/field.h:215-395), copying only populations that point into the
+// destination block.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mplbgpu.h"
+
+namespace mplb {
+
+constexpr int kMaxQ = 19;
+constexpr int kMaxOps = 4;
+constexpr int kNumRegions = 27;
+
+enum NodeClass : int { kPure = 0, kLocal = 1, kDeferred = 2 };
+enum OpKind : int { kOpEqm = 1, kOpHbb = 2, kOpExtrapol = 3 };
+
+// One boundary operation specialised to one region's geometry.  All FP64
+// constants that depend only on the boundary's given values are computed
+// here in the reference's operation order.
+struct RegionOp {
+    int kind;
+    uint32_t in_mask;   // EQM: incoming;  EXTRAPOL: copied populations
+    uint32_t out_mask;  // EQM: outgoing;  HBB: bounced populations
+    uint32_t par_mask;  // EQM: parallel
+    int nb_axis;        // EXTRAPOL copy source axis (-1: none)
+    int nb_sign;
+    double denom;       // EQM: (1 - deltaRho) - rhoParallel
+    double rho_given;   // EXTRAPOL
+    double a[kMaxQ];    // EQM: feq(1,u_w)/w per parallel population (res)
+    double b[kMaxQ];    // EQM: c.u_w per outgoing; HBB: 2 w (c.u_w)
+};
+
+struct RegionInfo {
+    int cls;            // NodeClass; -1 for an empty region
+    int vt;             // VertexType
+    int vg;             // VertexGeometryType
+    int fluidlike;      // Fluid or MDPeriodic: body force + force velocity
+    uint32_t pull;      // populations taken from the upstream node
+    uint32_t stale;     // LOCAL: populations neither pulled nor written
+    int nops;
+    int op[kMaxOps];    // indices into BlockPlan::ops
+    int ext[3];         // node extent of the region per axis
+    int org[3];         // first node of the region per axis
+    long long side_base;  // first index in the stale or deferred store
+};
+
+struct DeferredSegment {
+    int region;
+    int op;             // index into BlockPlan::ops
+};
+
+struct DeferredOp {     // one boundary (definition order) on deferred nodes
+    std::vector<DeferredSegment> segments;
+};
+
+struct BlockPlan {
+    int id;
+    int index;          // position in id order
+    int n[3];
+    int xoff;           // element index of x = 0 inside a row
+    long long pitch;    // elements per row
+    long long plane;    // elements per z plane (with y halo)
+    long long popstride;// elements per population (with halos)
+    RegionInfo region[kNumRegions];
+    std::vector<RegionOp> ops;
+    long long nstale;   // nodes with a stale store
+    long long ndeferred;
+    std::vector<DeferredOp> dops;
+    std::vector<int> allops[kNumRegions];  // every op of a region (host)
+    bool any_deferred() const { return ndeferred > 0; }
+    long long nodes() const { return (long long)n[0] * n[1] * n[2]; }
+};
+
+struct HaloCopy {
+    int from, to;       // block indices (id order)
+    int axis;
+    int to_low;         // 1: destination layer is -1 (from Right/Top/Front)
+    int iter[3];
+    int fbase[3];
+    int tbase[3];
+    uint32_t pops;      // populations copied
+    std::vector<uint8_t> prev;  // per box cell: read the previous array
+    bool any_prev;
+};
+
+struct Plan {
+    int dim = 3;
+    int Q = 19;
+    int precision = MPLBGPU_FP64;
+    int elem_bytes = 8;
+    double cs = 0, tau = 0, dt = 0;
+    double omega = 0;   // dt / (tau + dt/2)
+    double omc = 0;     // 1 - omega
+    double tw = 0;      // tau * omega
+    int body_force = 0;
+    int force_velocity = 0;
+    double accel[3] = {0, 0, 0};
+    double hdta[3] = {0, 0, 0};  // dt * a / 2
+    double cf[kMaxQ] = {};       // CS c_i . a  (CalcBodyForce sum)
+    double w[kMaxQ] = {};
+    std::vector<BlockPlan> blocks;  // sorted by id
+    std::vector<HaloCopy> halos;
+};
+
+// Builds the plan; returns MPLBGPU_OK or an error code with a message.
+int BuildPlan(const mplbgpu_desc& desc, Plan* plan, std::string* err);
+
+// Region of coordinate v on an axis of n nodes: 0 first, 2 last, 1 inside.
+inline int RegionCoord(int v, int n) {
+    return v == 0 ? 0 : (v == n - 1 ? 2 : 1);
+}
+
+}  // namespace mplb

@@ -1,0 +1,28 @@
+"""Loads the golden fixtures made by tests/golden/make_golden.py."""
+import json
+import os
+
+import numpy as np
+
+from mplb_b200.config import CaseConfig
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    case = CaseConfig.from_json(json.loads(str(z["case_json"])))
+    case.check_period = int(z["check_period"])
+    out = {"case": case, "steps": int(z["steps"]), "macro": {}, "f": {},
+           "residual_steps": z["residual_steps"],
+           "residual_max": z["residual_max"],
+           "residual_per_var": z["residual_per_var"]}
+    vars_ = ["rho", "u", "v", "w"][:case.space_dim + 1]
+    for b in case.block_ids:
+        out["macro"][b] = [z[f"{n}_b{b}"] for n in vars_]
+        out["f"][b] = z[f"f_b{b}"]
+    return out

@@ -1,0 +1,109 @@
+"""CPU checks of the oracle (the C restatement of the reference step):
+bitwise against the golden fixtures made by the reference itself, and -
+where the reference build is present - against the reference on more
+cases."""
+import numpy as np
+import pytest
+
+import golden_cases
+from mplb_b200 import config
+
+
+def run_oracle(pyoracle, case, steps):
+    o = pyoracle.Oracle(case)
+    o.init_uniform()
+    cp = case.check_period
+    hist = []
+    for _ in range(steps // cp):
+        o.step(cp)
+        o.update_macro()
+        hist.append(o.residual(cp))
+    o.step(steps % cp)
+    o.update_macro()
+    return o, hist
+
+
+@pytest.mark.parametrize("name", golden_cases.names())
+def test_oracle_matches_reference_golden(oracle_mod, name):
+    g = golden_cases.load(name)
+    o, hist = run_oracle(oracle_mod, g["case"], g["steps"])
+    for b in g["case"].block_ids:
+        for got, want in zip(o.macro(b), g["macro"][b]):
+            assert np.array_equal(got, want)
+        assert np.array_equal(o.f(b), g["f"][b])
+    assert np.array_equal(np.array([h[0] for h in hist]), g["residual_max"])
+
+
+REF_CASES = {
+    "cavity3d_13": (lambda: config.cavity(3, 13, 0.05, re=400), 40, 20),
+    "cavity2d_lid_first": (lambda: config.cavity(
+        2, 15, 0.1, re=30, order=("Top", "Left", "Right", "Bottom")), 120, 40),
+    "lchannel_app_9": (lambda: config.lchannel_app(9), 50, 25),
+    "poiseuille3d": (lambda: config.poiseuille(3, 7, 9, 6, g_lattice=1e-4),
+                     60, 30),
+}
+
+
+@pytest.mark.parametrize("name", sorted(REF_CASES))
+def test_oracle_matches_reference_built_here(oracle_mod, name):
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    build, steps, cp = REF_CASES[name]
+    case = build()
+    case.check_period = cp
+    ref = oracle_mod.run_reference(case, steps)
+    o, hist = run_oracle(oracle_mod, case, steps)
+    for b in case.block_ids:
+        for got, want in zip(o.macro(b), ref["macro"][b]):
+            assert np.array_equal(got, want)
+        assert np.array_equal(o.f(b), ref["f"][b])
+    assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
+
+
+def test_oracle_corner_populations_are_stale(oracle_mod):
+    """3D corners: the six populations with all components pointing away
+    from the corner's walls are neither streamed nor rewritten
+    (Src/boundary_host_device.h:486-693 labels), so they keep f^0."""
+    case = config.cavity(3, 8, 0.05, re=100)
+    o = oracle_mod.Oracle(case)
+    o.init_uniform()
+    f0 = o.f(0)[0, 0, 0].copy()
+    o.step(25)
+    f = o.f(0)[0, 0, 0]
+    from mplb_b200.csrc_tables import D3Q19_C
+    stale = [i for i, c in enumerate(D3Q19_C) if c != (0, 0, 0)
+             and all(v >= 0 for v in c)]
+    assert len(stale) == 6
+    assert np.array_equal(f[stale], f0[stale])
+
+
+def test_oracle_mass_conserved_in_periodic_box(oracle_mod):
+    """Fully periodic box (MDPeriodic on every face): total mass is
+    conserved to round-off."""
+    case = config.poiseuille(3, 6, 6, 6, g_lattice=0.0)
+    case.boundaries = [b for b in case.boundaries
+                       if b.surface not in ("Top", "Bottom")]
+    case.boundaries += [config._bc(0, "Top", "MDPeriodic", "MDPeriodic"),
+                        config._bc(0, "Bottom", "MDPeriodic", "MDPeriodic")]
+    case.connections += [config.ConnectionDef(0, "Top", 0, "Bottom",
+                                              "MDPeriodic"),
+                         config.ConnectionDef(0, "Bottom", 0, "Top",
+                                              "MDPeriodic")]
+    o = oracle_mod.Oracle(case)
+    rng = np.random.default_rng(7)
+    shp = (6, 6, 6)
+    o.init_macro(0, 1 + 0.01 * rng.standard_normal(shp),
+                 0.01 * rng.standard_normal(shp),
+                 0.01 * rng.standard_normal(shp),
+                 0.01 * rng.standard_normal(shp))
+    o.update_macro()
+    m0 = o.macro(0)[0].sum()
+    o.step(50)
+    o.update_macro()
+    assert abs(o.macro(0)[0].sum() - m0) < 1e-12 * m0
+
+
+def test_json_round_trip():
+    case = config.lchannel(leg=12, side=8, depth=6)
+    back = config.CaseConfig.from_json(case.to_json())
+    assert back.to_json() == case.to_json()
