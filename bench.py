@@ -44,7 +44,7 @@ METRIC = "MLUPS (D3Q19 FP64 3D lid-driven cavity 256^3)"
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="mplb", choices=["mplb", "reference"])
     p.add_argument("--size", type=int, default=256)

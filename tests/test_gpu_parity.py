@@ -130,7 +130,7 @@ def test_divergence_is_detected(gpu_lib):
     s = Solver(case)
     s.init_uniform()
     f = s.f(0)
-    f[5, 5, :] = np.nan
+    f[0, 5, 5, :] = np.nan
     s.upload_f(0, f)
     s.stream_collision(2)
     assert s.check_health() == abi.ERR_DIVERGED
