@@ -198,6 +198,27 @@ long long mplbgpu_launch_count(const mplbgpu_ctx* ctx);
 /* Device time of the most recent mplbgpu_step call's kernels (ms). */
 mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms);
 
+/* Residual sums that allocate nothing (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc where they need the reduction -
+ * programs that give all device memory to their own pool at start-up, or
+ * loops that cannot take the device-wide synchronisation that allocating
+ * and freeing cause.  The caller owns every buffer: q[v] and q_old[v]
+ * (v < nvars <= 4) are device arrays of n doubles, sums a device array of
+ * 2 * nvars doubles that receives sum((q - q_old)^2) and sum(q^2) per
+ * variable; q_old is overwritten with q.  Per-CTA partial sums go to a
+ * fixed 512 KiB device array inside the library (held on every GPU that
+ * loads it until exit), which limits n to MPLBGPU_NOALLOC_MAX_NODES; larger
+ * n is rejected with MPLBGPU_ERR_INVALID.  The first call on a device looks
+ * up that array's address for the current device; make it before any
+ * stream capture.  Work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream).  All calls share the array: calls that overlap on the
+ * GPU race. */
+#define MPLBGPU_NOALLOC_MAX_NODES 16777216LL
+mplbgpu_status mplbgpu_residual_sums_noalloc(const double* const* q,
+                                             double* const* q_old, int nvars,
+                                             long long n, double* sums,
+                                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,7 +119,11 @@ _SIGNATURES = {
     "mplbgpu_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
     "mplbgpu_last_step_ms": (ctypes.c_int, [ctypes.c_void_p,
                                             ctypes.c_void_p]),
+    "mplbgpu_residual_sums_noalloc": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong,
+        ctypes.c_void_p, ctypes.c_void_p]),
 }
+NOALLOC_MAX_NODES = 16777216
 
 
 def exported_symbols():

@@ -13,7 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmplbgpu.so")
-SOURCES = [os.path.join(CSRC, "mplbgpu.cu"), os.path.join(CSRC, "plan.cpp")]
+SOURCES = [os.path.join(CSRC, "mplbgpu.cu"), os.path.join(CSRC, "noalloc.cu"),
+           os.path.join(CSRC, "plan.cpp")]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "lattice.h",
                                             "plan.h")] + [
     os.path.join(HERE, "..", "include", "mplbgpu.h")]
