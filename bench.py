@@ -38,7 +38,9 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
                   ("fp32", 2): 72, ("fp16", 3): 76, ("fp16", 2): 36}
-METRIC = "MLUPS (D3Q19 FP64 3D lid-driven cavity 256^3)"
+METRIC = "MLUPS (D3Q19 3D lid-driven cavity 256^3)"
+DTYPES = {"fp64": "f64", "fp32": "f32 (shifted f - w)",
+          "fp16": "f16 storage of (f - w)/w, f32 arithmetic"}
 
 
 def parse():
@@ -48,13 +50,15 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="mplb", choices=["mplb", "reference"])
     p.add_argument("--size", type=int, default=256)
+    p.add_argument("--precision", default="fp64",
+                   choices=["fp64", "fp32", "fp16"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
 
-def workload(n):
+def workload(n, precision="fp64"):
     from mplb_b200 import config
-    case = config.cavity(3, n, 0.05, re=400)
+    case = config.cavity(3, n, 0.05, re=400, precision=precision)
     return case
 
 
@@ -211,7 +215,7 @@ def main():
     import torch
     from mplb_b200 import Solver, abi
     torch.cuda.set_device(local)
-    case = workload(args.size)
+    case = workload(args.size, args.precision)
     nodes = case.nodes()
     nx, ny, nz = case.size3(0)
     lib = abi.load_library()
@@ -287,12 +291,14 @@ def main():
         "metric": METRIC, "value": value, "unit": "MLUPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPES[args.precision], "data": "synthetic",
         "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
-                               "FP64, lid 0.05 (lattice), Re 400",
+                               f"{args.precision.upper()}, lid 0.05 "
+                               "(lattice), Re 400",
                    "nodes_per_gpu": nodes, "parallelism": f"replicas{world}",
-                   "l2": "population arrays 2.7 GB each, larger than L2"},
+                   "l2": "population arrays of 0.7-2.7 GB each, larger "
+                         "than L2"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,

@@ -13,18 +13,40 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmplbgpu.so")
-SOURCES = [os.path.join(CSRC, "mplbgpu.cu"), os.path.join(CSRC, "noalloc.cu"),
-           os.path.join(CSRC, "plan.cpp")]
+# (source, extra nvcc flags): the FP64 kernels and the host code that
+# computes their constants must not contract multiply-adds; the shifted
+# low-precision kernels may.
+UNITS = [("mplbgpu.cu", ["-fmad=false"]), ("kernels_f64.cu", ["-fmad=false"]),
+         ("kernels_lp.cu", ["-fmad=true"]), ("noalloc.cu", ["-fmad=false"]),
+         ("plan.cpp", [])]
+SOURCES = [os.path.join(CSRC, u) for u, _ in UNITS]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "lattice.h",
-                                            "plan.h")] + [
+                                            "plan.h", "launch.h",
+                                            "launch_impl.cuh")] + [
     os.path.join(HERE, "..", "include", "mplbgpu.h")]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 
-def nvcc_command(out=OUT, extra=()):
-    return ["nvcc", "-O3", "-std=c++17", ARCH, "-lineinfo", "-fmad=false",
-            "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-shared",
-            "-o", out] + list(extra) + SOURCES
+BUILD_DIR = os.path.join(HERE, "_build")
+
+
+def compile_commands():
+    """One nvcc command per translation unit (objects in _build/)."""
+    cmds = []
+    for unit, flags in UNITS:
+        obj = os.path.join(BUILD_DIR, unit + ".o")
+        cmds.append((obj, ["nvcc", "-O3", "-std=c++17", ARCH, "-lineinfo"] +
+                     flags + ["-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+                              "-c", os.path.join(CSRC, unit), "-o", obj]))
+    return cmds
+
+
+def nvcc_command(out=OUT):
+    """All flags used for the library (for inspection and tests)."""
+    cmd = []
+    for _, c in compile_commands():
+        cmd += c
+    return cmd
 
 
 def up_to_date(out=OUT):
@@ -37,10 +59,20 @@ def up_to_date(out=OUT):
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return OUT
-    cmd = nvcc_command()
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    cmds = compile_commands()
+    procs = []
+    for obj, cmd in cmds:
+        if verbose:
+            print(" ".join(cmd))
+        procs.append(subprocess.Popen(cmd))
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
+    link = ["nvcc", "-shared", ARCH, "-o", OUT] + [o for o, _ in cmds]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return OUT
 
 

@@ -10,13 +10,24 @@
 // takes moments (UpdateMacroVars3D) and collides (KerCollideBGKIsothermal3D)
 // - 2 Q values of memory traffic per node.
 //
-// FP64 arithmetic follows the reference's operation order exactly; the
-// translation unit is compiled with -fmad=false so no product is fused into
-// an add, and terms the reference multiplies by a zero lattice component
-// are skipped (adding a signed zero never changes a non-zero sum).
+// Storage forms (template parameter T):
+//   double : the reference's arithmetic.  Every FP64 expression follows the
+//            reference's operation order; the translation unit is compiled
+//            with -fmad=false so no product is fused into an add, and terms
+//            the reference multiplies by a zero lattice component are skipped
+//            (adding a signed zero never changes a non-zero sum).  Results
+//            are bit-identical to the reference.
+//   float  : the shifted deviation h_i = f_i - w_i in FP32 with FP32
+//            arithmetic (rho = 1 + sum h, feq - w computed directly).
+//   __half : the same deviation normalised by its weight, h_i / w_i, in
+//            FP16 storage; arithmetic in FP32.
+// Moments, residuals and the side stores are FP64 in every form.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include <cstdint>
+#include <type_traits>
 
 #include "lattice.h"
 #include "plan.h"
@@ -32,6 +43,13 @@ struct PhysConst {
     double hdta[3];    // dt * a / 2
     double cf[kMaxQ];  // CS c_i . a
     double w[kMaxQ];
+    // single-precision copies for the shifted forms
+    float csf, omcf, twf;
+    float hdtaf[3];
+    float cff[kMaxQ];
+    float wf[kMaxQ];
+    float winvf[kMaxQ];  // 1 / w_i
+    uint32_t seed;       // per launch (FP16 stochastic rounding)
 };
 
 struct BlockDev {
@@ -45,10 +63,122 @@ struct BlockDev {
     long long ndef;
     const int4* dregions;  // deferred regions: (region, base, count, -)
     int ndregions;
+    // per population: element offset of the upstream value (i * popstride -
+    // c_i . strides) and of the own value (i * popstride)
+    long long pull_off[kMaxQ];
+    long long pop_off[kMaxQ];
+    // per region: class (bits 0-1) and fluid-like flag (bit 2)
+    uint8_t rflags[kNumRegions];
 };
 
 enum StepMode : int { kModeStep = 0, kModeMacro = 1, kModeF = 2 };
 
+// ---------------------------------------------------------------------------
+// storage forms
+struct Rng;
+template <typename T>
+struct Prec;
+
+template <>
+struct Prec<double> {
+    using C = double;
+    static constexpr bool kShifted = false;
+    __device__ static __forceinline__ C Load(const double* p, long long k, int,
+                                             const PhysConst&) {
+        return p[k];
+    }
+    __device__ static __forceinline__ void Store(double* p, long long k, int,
+                                                 C v, const PhysConst&, Rng&) {
+        p[k] = v;
+    }
+};
+
+template <>
+struct Prec<float> {
+    using C = float;
+    static constexpr bool kShifted = true;
+    __device__ static __forceinline__ C Load(const float* p, long long k, int,
+                                             const PhysConst&) {
+        return p[k];
+    }
+    __device__ static __forceinline__ void Store(float* p, long long k, int,
+                                                 C v, const PhysConst&, Rng&) {
+        p[k] = v;
+    }
+};
+
+// FP16 stores round stochastically: the 13 float mantissa bits that FP16
+// drops are compared with a random draw, so increments far below one FP16
+// unit - a small body force per step - survive in expectation instead of
+// being rounded away every step.  Draws come from a per-thread xorshift32
+// generator seeded by hashing the node index with the step number.
+struct Rng {
+    uint32_t s;
+    uint32_t word;
+};
+
+__device__ __forceinline__ Rng SeedRng(uint32_t seed, long long node) {
+    uint32_t k = (uint32_t)node * 0x9e3779b9u ^ (uint32_t)(node >> 32) ^
+                 seed * 0x85ebca6bu;
+    k ^= k >> 16;
+    k *= 0x7feb352du;
+    k ^= k >> 15;
+    k *= 0x846ca68bu;
+    k ^= k >> 16;
+    return Rng{k | 1u, 0u};
+}
+
+// 13 random bits for population i, aligned with the 13 mantissa bits that
+// FP16 drops (one xorshift32 step serves two populations).
+__device__ __forceinline__ uint32_t SrDraw(Rng& g, int i) {
+    if ((i & 1) == 0) {
+        g.s ^= g.s << 13;
+        g.s ^= g.s >> 17;
+        g.s ^= g.s << 5;
+        g.word = g.s;
+    }
+    return (i & 1) ? (g.word >> 19) : (g.word & 0x1fffu);
+}
+
+__device__ __forceinline__ __half StochasticHalf(float v, uint32_t r) {
+    const uint32_t bits = __float_as_uint(v);
+    // normal FP16 range (|v| >= 2^-14; stored values stay far below 65504);
+    // smaller values round to nearest
+    if (((bits >> 23) & 0xffu) < 113u) return __float2half_rn(v);
+    return __float2half_rz(__uint_as_float(bits + r));
+}
+
+template <>
+struct Prec<__half> {
+    using C = float;
+    static constexpr bool kShifted = true;
+    __device__ static __forceinline__ C Load(const __half* p, long long k,
+                                             int i, const PhysConst& pc) {
+        return __half2float(p[k]) * pc.wf[i];
+    }
+    __device__ static __forceinline__ void Store(__half* p, long long k, int i,
+                                                 C v, const PhysConst& pc,
+                                                 Rng& rng) {
+        p[k] = StochasticHalf(v * pc.winvf[i], SrDraw(rng, i));
+    }
+};
+
+// Value of the reference's f_i from a value of form T (for FP64 outputs).
+template <typename T>
+__device__ __forceinline__ double ToF(typename Prec<T>::C v, int i,
+                                      const PhysConst& pc) {
+    if constexpr (Prec<T>::kShifted) return (double)v + pc.w[i];
+    else return v;
+}
+template <typename T>
+__device__ __forceinline__ typename Prec<T>::C FromF(double f, int i,
+                                                     const PhysConst& pc) {
+    if constexpr (Prec<T>::kShifted)
+        return (typename Prec<T>::C)(f - pc.w[i]);
+    else return f;
+}
+
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ int RegionOf(int x, int y, int z, const int n[3],
                                         int D) {
     const int rx = x == 0 ? 0 : (x == n[0] - 1 ? 2 : 1);
@@ -71,18 +201,44 @@ __device__ __forceinline__ long long UpOffset(const BlockDev& b, int i) {
              (long long)L::cz(i) * b.plane);
 }
 
+// Element index of population i at the upstream node / at the node itself:
+// mode 1 adds per-population offsets precomputed on the host (fewer integer
+// instructions per node), mode 0 computes them from the strides.
+#ifndef MPLB_ADDR_MODE
+#define MPLB_ADDR_MODE 1
+#endif
+template <typename L>
+__device__ __forceinline__ long long PullIndex(const BlockDev& b,
+                                               long long node, int i) {
+#if MPLB_ADDR_MODE == 1
+    return node + b.pull_off[i];
+#else
+    return i * b.popstride + node + UpOffset<L>(b, i);
+#endif
+}
+
+__device__ __forceinline__ long long OwnIndex(const BlockDev& b,
+                                              long long node, int i) {
+#if MPLB_ADDR_MODE == 1
+    return node + b.pop_off[i];
+#else
+    return i * b.popstride + node;
+#endif
+}
+
 __device__ __forceinline__ long long LocalIndex(const RegionInfo& R, int x,
                                                 int y, int z) {
     return ((long long)(z - R.org[2]) * R.ext[1] + (y - R.org[1])) * R.ext[0] +
            (x - R.org[0]);
 }
 
-// Moments of f (KerCalcDensity3D, KerCalcU3D/V3D/W3D and the _Force
+// ---------------------------------------------------------------------------
+// FP64 form: moments (KerCalcDensity3D, KerCalcU3D/V3D/W3D and the _Force
 // variants, Src/model_kernel.inc:570-759).
 template <typename L>
-__device__ __forceinline__ void Moments(const double* f, const PhysConst& pc,
-                                        bool fluidlike, double& rho,
-                                        double u[3]) {
+__device__ __forceinline__ void MomentsF64(const double* f, const PhysConst& pc,
+                                           bool fluidlike, double& rho,
+                                           double u[3]) {
     constexpr int Q = L::Q;
     rho = 0.0;
 #pragma unroll
@@ -103,12 +259,12 @@ __device__ __forceinline__ void Moments(const double* f, const PhysConst& pc,
     if (L::D == 2) u[2] = 0.0;
 }
 
-// BGK collision (KerCollideBGKIsothermal3D with CalcBGKFeq and
+// FP64 form: BGK collision (KerCollideBGKIsothermal3D with CalcBGKFeq and
 // CalcBodyForce, Src/model_kernel.inc:410-455, model_host_device.h:25-82).
 template <typename L>
-__device__ __forceinline__ void Collide(double* f, const PhysConst& pc,
-                                        bool fluidlike, double rho,
-                                        const double u[3]) {
+__device__ __forceinline__ void CollideF64(double* f, const PhysConst& pc,
+                                           bool fluidlike, double rho,
+                                           const double u[3]) {
     constexpr int Q = L::Q;
     const double cu0 = pc.cs * u[0], cu1 = pc.cs * u[1], cu2 = pc.cs * u[2];
     const double u2 = L::D == 3 ? (u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]
@@ -138,89 +294,218 @@ __device__ __forceinline__ void Collide(double* f, const PhysConst& pc,
     }
 }
 
-// EQMDiffuseRefl (KerCutCellEQMDiffuseRefl3D, Src/boundary_kernel.inc:
-// 1184-1276) with the wall constants precomputed per region.
+// Shifted forms: h = f - w.  rho = 1 + sum h, j = sum CS c h (sum c w = 0).
 template <typename L>
-__device__ __forceinline__ void ApplyEqm(double* f, const RegionOp& op,
+__device__ __forceinline__ void MomentsShifted(const float* h,
+                                               const PhysConst& pc,
+                                               bool fluidlike, float& drho,
+                                               float u[3]) {
+    constexpr int Q = L::Q;
+    drho = 0.0f;
+#pragma unroll
+    for (int i = 0; i < Q; i++) drho += h[i];
+    const float rinv = 1.0f / (1.0f + drho);
+#pragma unroll
+    for (int a = 0; a < L::D; a++) {
+        float s = 0.0f;
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const int c = comp<L>(i, a);
+            if (c > 0) s += h[i];
+            if (c < 0) s -= h[i];
+        }
+        s = pc.csf * s * rinv;
+        if (pc.force_vel && fluidlike) s += pc.hdtaf[a];
+        u[a] = s;
+    }
+    if (L::D == 2) u[2] = 0.0f;
+}
+
+// feq_i - w_i = w_i [(rho - 1) + rho (cu + (cu^2 - u^2) / 2)].
+template <typename L>
+__device__ __forceinline__ void CollideShifted(float* h, const PhysConst& pc,
+                                               bool fluidlike, float drho,
+                                               const float u[3]) {
+    constexpr int Q = L::Q;
+    const float rho = 1.0f + drho;
+    const float cu0 = pc.csf * u[0], cu1 = pc.csf * u[1], cu2 = pc.csf * u[2];
+    const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const bool force = pc.force && fluidlike;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        const float cu = (float)L::cx(i) * cu0 + (float)L::cy(i) * cu1 +
+                         (float)L::cz(i) * cu2;
+        const float heq = pc.wf[i] * (drho + rho * (cu + 0.5f * (cu * cu - u2)));
+        float g = heq + pc.omcf * (h[i] - heq);
+        if (force) g += pc.twf * (pc.wf[i] * rho * pc.cff[i]);
+        h[i] = g;
+    }
+}
+
+template <typename L, typename T>
+__device__ __forceinline__ void MomentsT(const typename Prec<T>::C* f,
+                                         const PhysConst& pc, bool fluidlike,
+                                         double& rho, double u[3]) {
+    if constexpr (Prec<T>::kShifted) {
+        float drho, uf[3];
+        MomentsShifted<L>(f, pc, fluidlike, drho, uf);
+        rho = 1.0 + (double)drho;
+        u[0] = uf[0];
+        u[1] = uf[1];
+        u[2] = uf[2];
+    } else {
+        MomentsF64<L>(f, pc, fluidlike, rho, u);
+    }
+}
+
+template <typename L, typename T>
+__device__ __forceinline__ void MomentsCollideT(typename Prec<T>::C* f,
+                                                const PhysConst& pc,
+                                                bool fluidlike) {
+    if constexpr (Prec<T>::kShifted) {
+        float drho, u[3];
+        MomentsShifted<L>(f, pc, fluidlike, drho, u);
+        CollideShifted<L>(f, pc, fluidlike, drho, u);
+    } else {
+        double rho, u[3];
+        MomentsF64<L>(f, pc, fluidlike, rho, u);
+        CollideF64<L>(f, pc, fluidlike, rho, u);
+    }
+}
+
+// EQMDiffuseRefl (KerCutCellEQMDiffuseRefl3D, Src/boundary_kernel.inc:
+// 1184-1276) with the wall constants precomputed per region.  Shifted
+// forms use sum_in f = sum_in h + sum_in w and w_opp(i) = w_i.
+template <typename L, typename T>
+__device__ __forceinline__ void ApplyEqm(typename Prec<T>::C* f,
+                                         const RegionOp& op,
                                          const PhysConst& pc) {
     constexpr int Q = L::Q;
-    double rhoIn = 0.0;
+    if constexpr (Prec<T>::kShifted) {
+        // rhoWall - 1 and w_i (rhoWall a_i - 1) without cancellation
+        float sin = 0.0f;
 #pragma unroll
-    for (int i = 0; i < Q; i++)
-        if (op.in_mask >> i & 1u) rhoIn = rhoIn + f[i];
-    const double rhoWall = (2.0 * rhoIn) / op.denom;
+        for (int i = 0; i < Q; i++)
+            if (op.in_mask >> i & 1u) sin += f[i];
+        const float inv = 1.0f / (float)op.denom;
+        const float drw = ((float)op.c0 + 2.0f * sin) * inv;
+        const float rhoWall = 1.0f + drw;
 #pragma unroll
-    for (int i = 0; i < Q; i++)
-        if (op.par_mask >> i & 1u) f[i] = (pc.w[i] * rhoWall) * op.a[i];
+        for (int i = 0; i < Q; i++)
+            if (op.par_mask >> i & 1u)
+                f[i] = pc.wf[i] * ((float)op.am1[i] + drw * (float)op.a[i]);
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.out_mask >> i & 1u)
+                f[i] = f[L::opp(i)] +
+                       2.0f * rhoWall * pc.wf[i] * (float)op.b[i];
+    } else {
+        double rhoIn = 0.0;
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.in_mask >> i & 1u) rhoIn = rhoIn + f[i];
+        const double rhoWall = (2.0 * rhoIn) / op.denom;
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.par_mask >> i & 1u) f[i] = (pc.w[i] * rhoWall) * op.a[i];
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.out_mask >> i & 1u)
+                f[i] = f[L::opp(i)] + ((2.0 * rhoWall) * pc.w[i]) * op.b[i];
+    }
+}
+
+// Halfway bounce-back: f_i = g_opp(i)(x) + 2 w_i (c_i . u_wall); the same
+// for the deviation because w_opp(i) = w_i.
+template <typename L, typename T>
+__device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
+                                         const RegionOp& op,
+                                         const PhysConst& pc,
+                                         const T* __restrict__ src,
+                                         const BlockDev& b, long long node) {
+    constexpr int Q = L::Q;
+    using P = Prec<T>;
 #pragma unroll
     for (int i = 0; i < Q; i++)
         if (op.out_mask >> i & 1u)
-            f[i] = f[L::opp(i)] + ((2.0 * rhoWall) * pc.w[i]) * op.b[i];
+            f[i] = P::Load(src, L::opp(i) * b.popstride + node, L::opp(i), pc) +
+                   (typename P::C)op.b[i];
 }
 
+// ---------------------------------------------------------------------------
 // Fused step over one block.  kModeStep writes g^{n+1}; kModeMacro and
 // kModeF recompute the current f = post-boundary populations from the
-// previous g and write moments or f instead (no collision).
-template <int D, int MODE>
-__global__ void __launch_bounds__(128)
-    StepKernel(BlockDev b, PhysConst pc, const double* __restrict__ src,
-               double* __restrict__ dst, double* __restrict__ out0,
+// previous g and write moments or f (FP64, dense) instead.
+// The shifted forms are instruction-issue bound: holding them to 64
+// registers (8 CTAs of 128 threads per SM) keeps enough warps to issue from.
+#ifndef MPLB_LP_MIN_BLOCKS
+#define MPLB_LP_MIN_BLOCKS 8
+#endif
+// The FP64 form holds 19 doubles per node; 5 CTAs per SM (<= 102 registers)
+// keeps it spill-free with 20 warps of loads in flight.
+#ifndef MPLB_F64_MIN_BLOCKS
+#define MPLB_F64_MIN_BLOCKS 5
+#endif
+template <int D, typename T, int MODE>
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value
+                                           ? MPLB_F64_MIN_BLOCKS
+                                           : MPLB_LP_MIN_BLOCKS)
+    StepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
+               T* __restrict__ dst, double* __restrict__ out0,
                double* __restrict__ out1, double* __restrict__ out2,
                double* __restrict__ out3) {
     using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
     constexpr int Q = L::Q;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = D == 3 ? (int)blockIdx.z : 0;
     if (x >= b.n[0]) return;
     const int r = RegionOf(x, y, z, b.n, D);
-    const RegionInfo& R = b.regions[r];
-    const int cls = R.cls;
+    const int rf = b.rflags[r];
+    const int cls = rf & 3;
     if (cls == kDeferred) return;
     const long long node = NodeIndex<D>(b, x, y, z);
-    double f[Q];
+    C f[Q];
     if (cls == kPure) {
 #pragma unroll
         for (int i = 0; i < Q; i++)
-            f[i] = src[i * b.popstride + node + UpOffset<L>(b, i)];
+            f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
     } else {
+        const RegionInfo& R = b.regions[r];
         const uint32_t pull = R.pull;
         const uint32_t stale = R.stale;
-        const double* st = b.stale + (R.side_base >= 0
-                                          ? (R.side_base + LocalIndex(R, x, y, z)) * Q
-                                          : 0);
+        const double* st =
+            b.stale + (R.side_base >= 0
+                           ? (R.side_base + LocalIndex(R, x, y, z)) * Q
+                           : 0);
 #pragma unroll
         for (int i = 0; i < Q; i++) {
             if (pull >> i & 1u)
-                f[i] = src[i * b.popstride + node + UpOffset<L>(b, i)];
+                f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
             else if (stale >> i & 1u)
-                f[i] = st[i];
+                f[i] = (C)st[i];
             else
-                f[i] = 0.0;
+                f[i] = (C)0;
         }
         for (int k = 0; k < R.nops; k++) {
             const RegionOp& op = b.ops[R.op[k]];
-            if (op.kind == kOpEqm) {
-                ApplyEqm<L>(f, op, pc);
-            } else if (op.kind == kOpHbb) {
-#pragma unroll
-                for (int i = 0; i < Q; i++)
-                    if (op.out_mask >> i & 1u)
-                        f[i] = src[L::opp(i) * b.popstride + node] + op.b[i];
-            }
+            if (op.kind == kOpEqm) ApplyEqm<L, T>(f, op, pc);
+            else if (op.kind == kOpHbb) ApplyHbb<L, T>(f, op, pc, src, b, node);
         }
     }
-    const bool fl = R.fluidlike != 0;
+    const bool fl = (rf & 4) != 0;
     if (MODE == kModeF) {
         const long long dn =
             ((long long)z * b.n[1] + y) * (long long)b.n[0] + x;
 #pragma unroll
-        for (int i = 0; i < Q; i++) out0[dn * Q + i] = f[i];
+        for (int i = 0; i < Q; i++) out0[dn * Q + i] = ToF<T>(f[i], i, pc);
         return;
     }
-    double rho, u[3];
-    Moments<L>(f, pc, fl, rho, u);
     if (MODE == kModeMacro) {
+        double rho, u[3];
+        MomentsT<L, T>(f, pc, fl, rho, u);
         const long long dn =
             ((long long)z * b.n[1] + y) * (long long)b.n[0] + x;
         out0[dn] = rho;
@@ -229,9 +514,11 @@ __global__ void __launch_bounds__(128)
         if (D == 3) out3[dn] = u[2];
         return;
     }
-    Collide<L>(f, pc, fl, rho, u);
+    MomentsCollideT<L, T>(f, pc, fl);
+    Rng rng = SeedRng(pc.seed, node);
 #pragma unroll
-    for (int i = 0; i < Q; i++) dst[i * b.popstride + node] = f[i];
+    for (int i = 0; i < Q; i++)
+        P::Store(dst, OwnIndex(b, node, i), i, f[i], pc, rng);
 }
 
 // Deferred nodes: thread t -> (region, node).
@@ -255,9 +542,11 @@ __device__ __forceinline__ bool DeferredNode(const BlockDev& b, long long t,
 }
 
 // Deferred nodes, part 1: streaming into the explicit f store (populations
-// not pulled keep their previous value, as in KerStream3D).
-template <int D>
-__global__ void DeferredStreamKernel(BlockDev b, const double* __restrict__ src) {
+// not pulled keep their previous value, as in KerStream3D).  The store holds
+// f (FP64 form) or the deviation h (shifted forms) in FP64.
+template <int D, typename T>
+__global__ void DeferredStreamKernel(BlockDev b, PhysConst pc,
+                                     const T* __restrict__ src) {
     using L = Lattice<D>;
     constexpr int Q = L::Q;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -270,8 +559,8 @@ __global__ void DeferredStreamKernel(BlockDev b, const double* __restrict__ src)
 #pragma unroll
     for (int i = 0; i < Q; i++)
         if (R.pull >> i & 1u)
-            b.fdef[i * b.ndef + k] =
-                src[i * b.popstride + node + UpOffset<L>(b, i)];
+            b.fdef[i * b.ndef + k] = Prec<T>::Load(
+                src, i * b.popstride + node + UpOffset<L>(b, i), i, pc);
 }
 
 struct DeferredSeg {
@@ -285,12 +574,14 @@ struct DeferredSeg {
 // (EQMDiffuseRefl, ExtrapolPressure1ST or halfway bounce-back).  The
 // extrapolation reads the inner neighbour's current f: from the store when
 // it is deferred, otherwise (a pure node) straight from its upstream g.
-template <int D>
+template <int D, typename T>
 __global__ void DeferredOpKernel(BlockDev b, PhysConst pc,
-                                 const double* __restrict__ src,
+                                 const T* __restrict__ src,
                                  const DeferredSeg* __restrict__ segs,
                                  int nseg, long long total) {
     using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
     constexpr int Q = L::Q;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= total) return;
@@ -304,52 +595,66 @@ __global__ void DeferredOpKernel(BlockDev b, PhysConst pc,
     const int z = R.org[2] + (int)(loc / ((long long)R.ext[0] * R.ext[1]));
     const long long k = R.side_base + loc;
     const RegionOp& op = b.ops[sg.op];
-    double f[Q];
+    C f[Q];
 #pragma unroll
-    for (int i = 0; i < Q; i++) f[i] = b.fdef[i * b.ndef + k];
+    for (int i = 0; i < Q; i++) f[i] = (C)b.fdef[i * b.ndef + k];
     if (op.kind == kOpEqm) {
-        ApplyEqm<L>(f, op, pc);
+        ApplyEqm<L, T>(f, op, pc);
     } else if (op.kind == kOpHbb) {
-        const long long node = NodeIndex<D>(b, x, y, z);
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.out_mask >> i & 1u)
-                f[i] = src[L::opp(i) * b.popstride + node] + op.b[i];
+        ApplyHbb<L, T>(f, op, pc, src, b, NodeIndex<D>(b, x, y, z));
     } else if (op.kind == kOpExtrapol) {
         int q[3] = {x, y, z};
         if (op.nb_axis >= 0) q[op.nb_axis] += op.nb_sign;
         const int nr = RegionOf(q[0], q[1], q[2], b.n, D);
         const RegionInfo& N = b.regions[nr];
         const bool nbdef = N.cls == kDeferred;
-        const long long nk = nbdef ? N.side_base + LocalIndex(N, q[0], q[1], q[2])
-                                   : 0;
+        const long long nk =
+            nbdef ? N.side_base + LocalIndex(N, q[0], q[1], q[2]) : 0;
         const long long nnode = NodeIndex<D>(b, q[0], q[1], q[2]);
-        double rho = 0.0;
+        if constexpr (P::kShifted) {
+            // f_i = (h_i + w_i) rho_given / rho for all but the last
+            float drho = 0.0f;
 #pragma unroll
-        for (int i = 0; i < Q; i++) {
-            if (op.in_mask >> i & 1u) {
-                f[i] = nbdef ? b.fdef[i * b.ndef + nk]
-                             : src[i * b.popstride + nnode + UpOffset<L>(b, i)];
+            for (int i = 0; i < Q; i++) {
+                if (op.in_mask >> i & 1u)
+                    f[i] = nbdef ? (C)b.fdef[i * b.ndef + nk]
+                                 : P::Load(src, i * b.popstride + nnode +
+                                                    UpOffset<L>(b, i), i, pc);
+                drho += f[i];
             }
-            rho = rho + f[i];
-        }
-        const double ratio = op.rho_given / rho;
+            const float rm1 = ((float)(op.rho_given - 1.0) - drho) / (1.0f + drho);
 #pragma unroll
-        for (int i = 0; i < Q - 1; i++) f[i] = f[i] * ratio;
+            for (int i = 0; i < Q - 1; i++) f[i] += (f[i] + pc.wf[i]) * rm1;
+        } else {
+            double rho = 0.0;
+#pragma unroll
+            for (int i = 0; i < Q; i++) {
+                if (op.in_mask >> i & 1u)
+                    f[i] = nbdef ? b.fdef[i * b.ndef + nk]
+                                 : P::Load(src, i * b.popstride + nnode +
+                                                    UpOffset<L>(b, i), i, pc);
+                rho = rho + f[i];
+            }
+            const double ratio = op.rho_given / rho;
+#pragma unroll
+            for (int i = 0; i < Q - 1; i++) f[i] = f[i] * ratio;
+        }
     }
 #pragma unroll
-    for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = f[i];
+    for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = (double)f[i];
 }
 
 // Deferred nodes, part 3: moments and collision (or observation).
-template <int D, int MODE>
+template <int D, typename T, int MODE>
 __global__ void DeferredFinishKernel(BlockDev b, PhysConst pc,
-                                     double* __restrict__ dst,
+                                     T* __restrict__ dst,
                                      double* __restrict__ out0,
                                      double* __restrict__ out1,
                                      double* __restrict__ out2,
                                      double* __restrict__ out3) {
     using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
     constexpr int Q = L::Q;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= b.ndef) return;
@@ -357,52 +662,69 @@ __global__ void DeferredFinishKernel(BlockDev b, PhysConst pc,
     long long k;
     if (!DeferredNode(b, t, r, x, y, z, k)) return;
     const RegionInfo& R = b.regions[r];
-    double f[Q];
+    C f[Q];
 #pragma unroll
-    for (int i = 0; i < Q; i++) f[i] = b.fdef[i * b.ndef + k];
+    for (int i = 0; i < Q; i++) f[i] = (C)b.fdef[i * b.ndef + k];
     const long long dn = ((long long)z * b.n[1] + y) * (long long)b.n[0] + x;
     if (MODE == kModeF) {
 #pragma unroll
-        for (int i = 0; i < Q; i++) out0[dn * Q + i] = f[i];
+        for (int i = 0; i < Q; i++) out0[dn * Q + i] = ToF<T>(f[i], i, pc);
         return;
     }
-    double rho, u[3];
-    Moments<L>(f, pc, R.fluidlike != 0, rho, u);
     if (MODE == kModeMacro) {
+        double rho, u[3];
+        MomentsT<L, T>(f, pc, R.fluidlike != 0, rho, u);
         out0[dn] = rho;
         out1[dn] = u[0];
         out2[dn] = u[1];
         if (D == 3) out3[dn] = u[2];
         return;
     }
-    Collide<L>(f, pc, R.fluidlike != 0, rho, u);
+    MomentsCollideT<L, T>(f, pc, R.fluidlike != 0);
     const long long node = NodeIndex<D>(b, x, y, z);
+    Rng rng = SeedRng(pc.seed, node);
 #pragma unroll
-    for (int i = 0; i < Q; i++) dst[i * b.popstride + node] = f[i];
+    for (int i = 0; i < Q; i++)
+        P::Store(dst, i * b.popstride + node, i, f[i], pc, rng);
 }
 
 // Initial state of one block from per-node macroscopic values
 // (KerInitialiseBGK2nd3D: f = feq(rho, u), Src/model_kernel.inc:352-380) or
-// from uploaded f (fin != nullptr, point-major).  Writes f^0 to `fdirect`
-// (same layout as g), the stale and deferred stores, and g^0 = collision of
-// f^0 with its own moments to `g`.
-template <int D>
+// from uploaded f (fin != nullptr, point-major, FP64).  Writes f^0 to
+// `fdirect` (form T, same layout as g), the stale and deferred stores, and
+// g^0 = collision of f^0 with its own moments to `g`.
+template <int D, typename T>
 __global__ void __launch_bounds__(128)
     InitKernel(BlockDev b, PhysConst pc, const double* __restrict__ rho0,
                const double* __restrict__ u0, const double* __restrict__ v0,
                const double* __restrict__ w0, const double* __restrict__ fin,
-               double* __restrict__ fdirect, double* __restrict__ g) {
+               T* __restrict__ fdirect, T* __restrict__ g) {
     using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
     constexpr int Q = L::Q;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = D == 3 ? (int)blockIdx.z : 0;
     if (x >= b.n[0]) return;
     const long long dn = ((long long)z * b.n[1] + y) * (long long)b.n[0] + x;
-    double f[Q];
+    C f[Q];
     if (fin != nullptr) {
 #pragma unroll
-        for (int i = 0; i < Q; i++) f[i] = fin[dn * Q + i];
+        for (int i = 0; i < Q; i++) f[i] = FromF<T>(fin[dn * Q + i], i, pc);
+    } else if constexpr (P::kShifted) {
+        const float drho = (float)(rho0[dn] - 1.0);
+        const float rho = 1.0f + drho;
+        const float u[3] = {(float)u0[dn], (float)v0[dn],
+                            D == 3 ? (float)w0[dn] : 0.0f};
+        const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const float cu = pc.csf * ((float)L::cx(i) * u[0] +
+                                       (float)L::cy(i) * u[1] +
+                                       (float)L::cz(i) * u[2]);
+            f[i] = pc.wf[i] * (drho + rho * (cu + 0.5f * (cu * cu - u2)));
+        }
     } else {
         // CalcBGKFeq(l, rho, u, v, w, 1, 2), Src/model_host_device.h:58-82
         const double rho = rho0[dn];
@@ -432,34 +754,37 @@ __global__ void __launch_bounds__(128)
     const int r = RegionOf(x, y, z, b.n, D);
     const RegionInfo& R = b.regions[r];
     const long long node = NodeIndex<D>(b, x, y, z);
+    Rng rng = SeedRng(pc.seed, node);
 #pragma unroll
-    for (int i = 0; i < Q; i++) fdirect[i * b.popstride + node] = f[i];
+    for (int i = 0; i < Q; i++)
+        P::Store(fdirect, i * b.popstride + node, i, f[i], pc, rng);
     if (R.side_base >= 0) {
         const long long k = R.side_base + LocalIndex(R, x, y, z);
         if (R.cls == kLocal) {
 #pragma unroll
-            for (int i = 0; i < Q; i++) b.stale[k * Q + i] = f[i];
+            for (int i = 0; i < Q; i++) b.stale[k * Q + i] = (double)f[i];
         } else if (R.cls == kDeferred) {
 #pragma unroll
-            for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = f[i];
+            for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = (double)f[i];
         }
     }
-    double rho, u[3];
-    Moments<L>(f, pc, R.fluidlike != 0, rho, u);
-    Collide<L>(f, pc, R.fluidlike != 0, rho, u);
+    MomentsCollideT<L, T>(f, pc, R.fluidlike != 0);
 #pragma unroll
-    for (int i = 0; i < Q; i++) g[i * b.popstride + node] = f[i];
+    for (int i = 0; i < Q; i++)
+        P::Store(g, i * b.popstride + node, i, f[i], pc, rng);
 }
 
 // Observation straight from f^0 stored by InitKernel (before any step).
-template <int D, int MODE>
+template <int D, typename T, int MODE>
 __global__ void DirectObserveKernel(BlockDev b, PhysConst pc,
-                                    const double* __restrict__ fdirect,
+                                    const T* __restrict__ fdirect,
                                     double* __restrict__ out0,
                                     double* __restrict__ out1,
                                     double* __restrict__ out2,
                                     double* __restrict__ out3) {
     using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
     constexpr int Q = L::Q;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -467,17 +792,24 @@ __global__ void DirectObserveKernel(BlockDev b, PhysConst pc,
     if (x >= b.n[0]) return;
     const long long dn = ((long long)z * b.n[1] + y) * (long long)b.n[0] + x;
     const long long node = NodeIndex<D>(b, x, y, z);
-    double f[Q];
+    const RegionInfo& R = b.regions[RegionOf(x, y, z, b.n, D)];
+    C f[Q];
+    if (R.cls == kDeferred && R.side_base >= 0) {
+        const long long k = R.side_base + LocalIndex(R, x, y, z);
 #pragma unroll
-    for (int i = 0; i < Q; i++) f[i] = fdirect[i * b.popstride + node];
+        for (int i = 0; i < Q; i++) f[i] = (C)b.fdef[i * b.ndef + k];
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            f[i] = P::Load(fdirect, i * b.popstride + node, i, pc);
+    }
     if (MODE == kModeF) {
 #pragma unroll
-        for (int i = 0; i < Q; i++) out0[dn * Q + i] = f[i];
+        for (int i = 0; i < Q; i++) out0[dn * Q + i] = ToF<T>(f[i], i, pc);
         return;
     }
-    const RegionInfo& R = b.regions[RegionOf(x, y, z, b.n, D)];
     double rho, u[3];
-    Moments<L>(f, pc, R.fluidlike != 0, rho, u);
+    MomentsT<L, T>(f, pc, R.fluidlike != 0, rho, u);
     out0[dn] = rho;
     out1[dn] = u[0];
     out2[dn] = u[1];
@@ -495,11 +827,11 @@ struct HaloDev {
 // One connection's halo copy (Field::TransferHalos / ops_halo_transfer):
 // the face layer of the source block into the destination block's halo,
 // only the populations that point into the destination.
-template <int D>
+template <int D, typename T>
 __global__ void HaloKernel(HaloDev h, BlockDev fb, BlockDev tb,
-                           const double* __restrict__ cur_from,
-                           const double* __restrict__ prev_from,
-                           double* __restrict__ cur_to) {
+                           const T* __restrict__ cur_from,
+                           const T* __restrict__ prev_from,
+                           T* __restrict__ cur_to) {
     using L = Lattice<D>;
     constexpr int Q = L::Q;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -512,7 +844,7 @@ __global__ void HaloKernel(HaloDev h, BlockDev fb, BlockDev tb,
                                      h.fbase[2] + k);
     const long long d = NodeIndex<D>(tb, h.tbase[0] + i, h.tbase[1] + j,
                                      h.tbase[2] + k);
-    const double* from = (h.prev != nullptr && h.prev[t]) ? prev_from : cur_from;
+    const T* from = (h.prev != nullptr && h.prev[t]) ? prev_from : cur_from;
 #pragma unroll
     for (int q = 0; q < Q; q++)
         if (h.pops >> q & 1u)
@@ -524,56 +856,12 @@ __global__ void HaloKernel(HaloDev h, BlockDev fb, BlockDev tb,
 // KerCalcMacroVarSquare, Src/flowfield_kernel.inc:131-153); q_old <- q.
 __global__ void ResidualPartialKernel(const double* __restrict__ q,
                                       double* __restrict__ qold, long long n,
-                                      double* __restrict__ part) {
-    __shared__ double sd[256];
-    __shared__ double ss[256];
-    double d = 0.0, s = 0.0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const double v = q[t];
-        const double dv = v - qold[t];
-        d = d + dv * dv;
-        s = s + v * v;
-        qold[t] = v;
-    }
-    sd[threadIdx.x] = d;
-    ss[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            sd[threadIdx.x] = sd[threadIdx.x] + sd[threadIdx.x + w];
-            ss[threadIdx.x] = ss[threadIdx.x] + ss[threadIdx.x + w];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = sd[0];
-        part[2 * blockIdx.x + 1] = ss[0];
-    }
-}
+                                      double* __restrict__ part);
 
 // Sum of a field over n values, per CTA (mass), and a count of
 // non-finite or non-positive values (health word).
 __global__ void SumPartialKernel(const double* __restrict__ q, long long n,
                                  double* __restrict__ part,
-                                 unsigned long long* __restrict__ bad) {
-    __shared__ double ss[256];
-    double s = 0.0;
-    unsigned long long nb = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const double v = q[t];
-        s = s + v;
-        if (!(v > 0.0) || !isfinite(v)) nb++;
-    }
-    ss[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) ss[threadIdx.x] = ss[threadIdx.x] + ss[threadIdx.x + w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) part[blockIdx.x] = ss[0];
-    if (nb) atomicAdd(bad, nb);
-}
+                                 unsigned long long* __restrict__ bad);
 
 }  // namespace mplb

@@ -1,0 +1,45 @@
+// Host-side launchers of the step kernels, one instantiation per lattice
+// dimension and storage form.  The FP64 form is compiled in
+// kernels_f64.cu with -fmad=false (bitwise reference arithmetic), the
+// shifted FP32/FP16 forms in kernels_lp.cu with fused multiply-adds.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace mplb {
+
+template <int D, typename T>
+struct Launch {
+    static cudaError_t Step(int mode, dim3 grid, cudaStream_t s,
+                            const BlockDev& b, const PhysConst& pc,
+                            const T* src, T* dst, double* o0, double* o1,
+                            double* o2, double* o3);
+    static cudaError_t DeferredStream(unsigned grid, cudaStream_t s,
+                                      const BlockDev& b, const PhysConst& pc,
+                                      const T* src);
+    static cudaError_t DeferredOp(unsigned grid, cudaStream_t s,
+                                  const BlockDev& b, const PhysConst& pc,
+                                  const T* src, const DeferredSeg* segs,
+                                  int nseg, long long total);
+    static cudaError_t DeferredFinish(int mode, unsigned grid, cudaStream_t s,
+                                      const BlockDev& b, const PhysConst& pc,
+                                      T* dst, double* o0, double* o1,
+                                      double* o2, double* o3);
+    static cudaError_t Init(dim3 grid, cudaStream_t s, const BlockDev& b,
+                            const PhysConst& pc, const double* rho,
+                            const double* u, const double* v, const double* w,
+                            const double* fin, T* fdirect, T* g);
+    static cudaError_t DirectObserve(int mode, dim3 grid, cudaStream_t s,
+                                     const BlockDev& b, const PhysConst& pc,
+                                     const T* fdirect, double* o0, double* o1,
+                                     double* o2, double* o3);
+    static cudaError_t Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
+                            const BlockDev& fb, const BlockDev& tb,
+                            const T* cur_from, const T* prev_from, T* cur_to);
+};
+
+constexpr int kStepThreads = 128;
+
+}  // namespace mplb

@@ -1,0 +1,98 @@
+// Definitions of the launchers declared in launch.h (included by the
+// translation units that instantiate them).
+#pragma once
+
+#include "launch.h"
+
+namespace mplb {
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
+                               const BlockDev& b, const PhysConst& pc,
+                               const T* src, T* dst, double* o0, double* o1,
+                               double* o2, double* o3) {
+    if (mode == kModeStep)
+        StepKernel<D, T, kModeStep><<<grid, kStepThreads, 0, s>>>(
+            b, pc, src, dst, o0, o1, o2, o3);
+    else if (mode == kModeMacro)
+        StepKernel<D, T, kModeMacro><<<grid, kStepThreads, 0, s>>>(
+            b, pc, src, dst, o0, o1, o2, o3);
+    else
+        StepKernel<D, T, kModeF><<<grid, kStepThreads, 0, s>>>(
+            b, pc, src, dst, o0, o1, o2, o3);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::DeferredStream(unsigned grid, cudaStream_t s,
+                                         const BlockDev& b,
+                                         const PhysConst& pc, const T* src) {
+    DeferredStreamKernel<D, T><<<grid, kStepThreads, 0, s>>>(b, pc, src);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::DeferredOp(unsigned grid, cudaStream_t s,
+                                     const BlockDev& b, const PhysConst& pc,
+                                     const T* src, const DeferredSeg* segs,
+                                     int nseg, long long total) {
+    DeferredOpKernel<D, T><<<grid, kStepThreads, 0, s>>>(b, pc, src, segs,
+                                                         nseg, total);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::DeferredFinish(int mode, unsigned grid,
+                                         cudaStream_t s, const BlockDev& b,
+                                         const PhysConst& pc, T* dst,
+                                         double* o0, double* o1, double* o2,
+                                         double* o3) {
+    if (mode == kModeStep)
+        DeferredFinishKernel<D, T, kModeStep><<<grid, kStepThreads, 0, s>>>(
+            b, pc, dst, o0, o1, o2, o3);
+    else if (mode == kModeMacro)
+        DeferredFinishKernel<D, T, kModeMacro><<<grid, kStepThreads, 0, s>>>(
+            b, pc, dst, o0, o1, o2, o3);
+    else
+        DeferredFinishKernel<D, T, kModeF><<<grid, kStepThreads, 0, s>>>(
+            b, pc, dst, o0, o1, o2, o3);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::Init(dim3 grid, cudaStream_t s, const BlockDev& b,
+                               const PhysConst& pc, const double* rho,
+                               const double* u, const double* v,
+                               const double* w, const double* fin, T* fdirect,
+                               T* g) {
+    InitKernel<D, T><<<grid, kStepThreads, 0, s>>>(b, pc, rho, u, v, w, fin,
+                                                   fdirect, g);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::DirectObserve(int mode, dim3 grid, cudaStream_t s,
+                                        const BlockDev& b,
+                                        const PhysConst& pc, const T* fdirect,
+                                        double* o0, double* o1, double* o2,
+                                        double* o3) {
+    if (mode == kModeMacro)
+        DirectObserveKernel<D, T, kModeMacro><<<grid, kStepThreads, 0, s>>>(
+            b, pc, fdirect, o0, o1, o2, o3);
+    else
+        DirectObserveKernel<D, T, kModeF><<<grid, kStepThreads, 0, s>>>(
+            b, pc, fdirect, o0, o1, o2, o3);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
+                               const BlockDev& fb, const BlockDev& tb,
+                               const T* cur_from, const T* prev_from,
+                               T* cur_to) {
+    HaloKernel<D, T><<<grid, 256, 0, s>>>(h, fb, tb, cur_from, prev_from,
+                                          cur_to);
+    return cudaGetLastError();
+}
+
+}  // namespace mplb

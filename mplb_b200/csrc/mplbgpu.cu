@@ -16,7 +16,7 @@
 #include <vector>
 
 #include "../../include/mplbgpu.h"
-#include "kernels.cuh"
+#include "launch.h"
 #include "plan.h"
 
 using namespace mplb;
@@ -27,7 +27,7 @@ thread_local std::string g_create_error;
 
 struct DevBlock {
     BlockDev dev{};
-    double* pop[2] = {nullptr, nullptr};
+    void* pop[2] = {nullptr, nullptr};   // form T of the context
     RegionInfo* regions = nullptr;
     RegionOp* ops = nullptr;
     double* stale = nullptr;
@@ -64,6 +64,7 @@ struct mplbgpu_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0;
     long long launches = 0;
+    unsigned long long step_count = 0;
     double* part = nullptr;     // reduction partials
     unsigned long long* bad = nullptr;
     double* scratch = nullptr;  // dense f staging
@@ -73,8 +74,22 @@ struct mplbgpu_ctx {
 
 namespace {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = kStepThreads;
 constexpr int kRedBlocks = 1024;
+
+// Calls FN<D, T>(args...) for the context's dimension and storage form.
+#define MPLB_DISPATCH(ctx, FN, ...)                                          \
+    ((ctx)->plan.dim == 3                                                   \
+         ? ((ctx)->plan.precision == MPLBGPU_FP64                           \
+                ? FN<3, double>(__VA_ARGS__)                                \
+                : (ctx)->plan.precision == MPLBGPU_FP32_SHIFTED             \
+                      ? FN<3, float>(__VA_ARGS__)                           \
+                      : FN<3, __half>(__VA_ARGS__))                         \
+         : ((ctx)->plan.precision == MPLBGPU_FP64                           \
+                ? FN<2, double>(__VA_ARGS__)                                \
+                : (ctx)->plan.precision == MPLBGPU_FP32_SHIFTED             \
+                      ? FN<2, float>(__VA_ARGS__)                           \
+                      : FN<2, __half>(__VA_ARGS__)))
 constexpr int kRedThreads = 256;
 
 int SetErr(mplbgpu_ctx* c, int code, const std::string& m) {
@@ -90,15 +105,16 @@ int SetErr(mplbgpu_ctx* c, int code, const std::string& m) {
                           std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-#define CK_LAUNCH()                                                         \
+#define CK_LAUNCH_E(...)                                                    \
     do {                                                                    \
         ctx->launches++;                                                    \
-        cudaError_t e_ = cudaGetLastError();                                \
+        cudaError_t e_ = (__VA_ARGS__);                                     \
         if (e_ != cudaSuccess)                                              \
             return SetErr(ctx, MPLBGPU_ERR_CUDA,                            \
                           std::string("kernel launch: ") +                  \
                               cudaGetErrorString(e_));                      \
     } while (0)
+#define CK_LAUNCH() CK_LAUNCH_E(cudaGetLastError())
 
 dim3 NodeGrid(const BlockPlan& B, int dim) {
     return dim3((B.n[0] + kThreads - 1) / kThreads, B.n[1],
@@ -151,82 +167,80 @@ int EnsureScratch(mplbgpu_ctx* ctx, size_t elems) {
     return MPLBGPU_OK;
 }
 
-int RunHalos(mplbgpu_ctx* ctx) {
-    const int dim = ctx->plan.dim;
+template <int D, typename T>
+int RunHalosT(mplbgpu_ctx* ctx) {
     for (DevHalo& h : ctx->halos) {
         DevBlock& fb = ctx->blocks[h.from];
         DevBlock& tb = ctx->blocks[h.to];
         const long long cells =
             (long long)h.h.iter[0] * h.h.iter[1] * h.h.iter[2];
         const unsigned grid = (unsigned)((cells + 255) / 256);
-        if (dim == 3)
-            HaloKernel<3><<<grid, 256, 0, ctx->stream>>>(
-                h.h, fb.dev, tb.dev, fb.pop[ctx->cur], fb.pop[1 - ctx->cur],
-                tb.pop[ctx->cur]);
-        else
-            HaloKernel<2><<<grid, 256, 0, ctx->stream>>>(
-                h.h, fb.dev, tb.dev, fb.pop[ctx->cur], fb.pop[1 - ctx->cur],
-                tb.pop[ctx->cur]);
-        CK_LAUNCH();
+        CK_LAUNCH_E(Launch<D, T>::Halo(
+            grid, ctx->stream, h.h, fb.dev, tb.dev,
+            static_cast<const T*>(fb.pop[ctx->cur]),
+            static_cast<const T*>(fb.pop[1 - ctx->cur]),
+            static_cast<T*>(tb.pop[ctx->cur])));
     }
     ctx->halos_pending = false;
     return MPLBGPU_OK;
 }
 
-template <int D>
+int RunHalos(mplbgpu_ctx* ctx) { return MPLB_DISPATCH(ctx, RunHalosT, ctx); }
+
+template <int D, typename T>
 int StepOnce(mplbgpu_ctx* ctx) {
     const int src = ctx->cur, dst = 1 - ctx->cur;
+    ctx->pc.seed = (uint32_t)(++ctx->step_count);
     for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
         DevBlock& b = ctx->blocks[bi];
         const BlockPlan& B = ctx->plan.blocks[bi];
-        StepKernel<D, kModeStep><<<NodeGrid(B, D), kThreads, 0, ctx->stream>>>(
-            b.dev, ctx->pc, b.pop[src], b.pop[dst], nullptr, nullptr, nullptr,
-            nullptr);
-        CK_LAUNCH();
+        const T* s = static_cast<const T*>(b.pop[src]);
+        T* d = static_cast<T*>(b.pop[dst]);
+        CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D), ctx->stream,
+                                       b.dev, ctx->pc, s, d, nullptr, nullptr,
+                                       nullptr, nullptr));
         if (B.ndeferred > 0) {
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
-            DeferredStreamKernel<D><<<g, kThreads, 0, ctx->stream>>>(b.dev,
-                                                                     b.pop[src]);
-            CK_LAUNCH();
-            for (auto& d : b.dops) {
-                const unsigned gd = (unsigned)((d.total + kThreads - 1) / kThreads);
-                DeferredOpKernel<D><<<gd, kThreads, 0, ctx->stream>>>(
-                    b.dev, ctx->pc, b.pop[src], d.segs, d.nseg, d.total);
-                CK_LAUNCH();
+            CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, ctx->stream, b.dev,
+                                                     ctx->pc, s));
+            for (auto& dop : b.dops) {
+                const unsigned gd =
+                    (unsigned)((dop.total + kThreads - 1) / kThreads);
+                CK_LAUNCH_E(Launch<D, T>::DeferredOp(gd, ctx->stream, b.dev,
+                                                     ctx->pc, s, dop.segs,
+                                                     dop.nseg, dop.total));
             }
-            DeferredFinishKernel<D, kModeStep><<<g, kThreads, 0, ctx->stream>>>(
-                b.dev, ctx->pc, b.pop[dst], nullptr, nullptr, nullptr, nullptr);
-            CK_LAUNCH();
+            CK_LAUNCH_E(Launch<D, T>::DeferredFinish(
+                kModeStep, g, ctx->stream, b.dev, ctx->pc, d, nullptr, nullptr,
+                nullptr, nullptr));
         }
     }
     ctx->cur = dst;
     ctx->initial = false;
-    return RunHalos(ctx);
+    return RunHalosT<D, T>(ctx);
 }
 
 // Current f -> moments (kModeMacro) or point-major f (kModeF) of one block.
-template <int D, int MODE>
-int Observe(mplbgpu_ctx* ctx, size_t bi, double* o0, double* o1, double* o2,
-            double* o3) {
+template <int D, typename T>
+int Observe(mplbgpu_ctx* ctx, int mode, size_t bi, double* o0, double* o1,
+            double* o2, double* o3) {
     DevBlock& b = ctx->blocks[bi];
     const BlockPlan& B = ctx->plan.blocks[bi];
     const int prev = 1 - ctx->cur;
+    const T* pv = static_cast<const T*>(b.pop[prev]);
     if (ctx->initial) {
-        DirectObserveKernel<D, MODE><<<NodeGrid(B, D), kThreads, 0,
-                                       ctx->stream>>>(b.dev, ctx->pc,
-                                                      b.pop[prev], o0, o1, o2,
-                                                      o3);
-        CK_LAUNCH();
+        CK_LAUNCH_E(Launch<D, T>::DirectObserve(mode, NodeGrid(B, D),
+                                                ctx->stream, b.dev, ctx->pc,
+                                                pv, o0, o1, o2, o3));
         return MPLBGPU_OK;
     }
-    StepKernel<D, MODE><<<NodeGrid(B, D), kThreads, 0, ctx->stream>>>(
-        b.dev, ctx->pc, b.pop[prev], nullptr, o0, o1, o2, o3);
-    CK_LAUNCH();
+    CK_LAUNCH_E(Launch<D, T>::Step(mode, NodeGrid(B, D), ctx->stream, b.dev,
+                                   ctx->pc, pv, nullptr, o0, o1, o2, o3));
     if (B.ndeferred > 0) {
         const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
-        DeferredFinishKernel<D, MODE><<<g, kThreads, 0, ctx->stream>>>(
-            b.dev, ctx->pc, nullptr, o0, o1, o2, o3);
-        CK_LAUNCH();
+        CK_LAUNCH_E(Launch<D, T>::DeferredFinish(mode, g, ctx->stream, b.dev,
+                                                 ctx->pc, nullptr, o0, o1, o2,
+                                                 o3));
     }
     return MPLBGPU_OK;
 }
@@ -234,11 +248,9 @@ int Observe(mplbgpu_ctx* ctx, size_t bi, double* o0, double* o1, double* o2,
 int UpdateMacro(mplbgpu_ctx* ctx) {
     for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
         DevBlock& b = ctx->blocks[bi];
-        int rc = ctx->plan.dim == 3
-                     ? Observe<3, kModeMacro>(ctx, bi, b.macro[0], b.macro[1],
-                                              b.macro[2], b.macro[3])
-                     : Observe<2, kModeMacro>(ctx, bi, b.macro[0], b.macro[1],
-                                              b.macro[2], nullptr);
+        int rc = MPLB_DISPATCH(ctx, Observe, ctx, (int)kModeMacro, bi,
+                               b.macro[0], b.macro[1], b.macro[2],
+                               ctx->plan.dim == 3 ? b.macro[3] : nullptr);
         if (rc != MPLBGPU_OK) return rc;
     }
     return MPLBGPU_OK;
@@ -254,16 +266,16 @@ int CheckReady(mplbgpu_ctx* ctx) {
     return MPLBGPU_OK;
 }
 
-template <int D>
+template <int D, typename T>
 int InitBlock(mplbgpu_ctx* ctx, size_t bi, const double* d_rho,
               const double* d_u, const double* d_v, const double* d_w,
               const double* d_f) {
     DevBlock& b = ctx->blocks[bi];
     const BlockPlan& B = ctx->plan.blocks[bi];
-    InitKernel<D><<<NodeGrid(B, D), kThreads, 0, ctx->stream>>>(
-        b.dev, ctx->pc, d_rho, d_u, d_v, d_w, d_f, b.pop[1 - ctx->cur],
-        b.pop[ctx->cur]);
-    CK_LAUNCH();
+    CK_LAUNCH_E(Launch<D, T>::Init(NodeGrid(B, D), ctx->stream, b.dev,
+                                   ctx->pc, d_rho, d_u, d_v, d_w, d_f,
+                                   static_cast<T*>(b.pop[1 - ctx->cur]),
+                                   static_cast<T*>(b.pop[ctx->cur])));
     return MPLBGPU_OK;
 }
 
@@ -282,9 +294,6 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     std::string err;
     int rc = BuildPlan(*desc, &c->plan, &err);
     if (rc != MPLBGPU_OK) return SetErr(nullptr, rc, err);
-    if (c->plan.precision != MPLBGPU_FP64)
-        return SetErr(nullptr, MPLBGPU_ERR_UNSUPPORTED,
-                      "only the FP64 form is built in this library");
     ctx = c.get();
     const Plan& P = c->plan;
     PhysConst& pc = c->pc;
@@ -297,7 +306,14 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     for (int i = 0; i < kMaxQ; i++) {
         pc.cf[i] = P.cf[i];
         pc.w[i] = P.w[i];
+        pc.cff[i] = (float)P.cf[i];
+        pc.wf[i] = (float)P.w[i];
+        pc.winvf[i] = P.w[i] > 0 ? (float)(1.0 / P.w[i]) : 0.0f;
     }
+    pc.csf = (float)P.cs;
+    pc.omcf = (float)P.omc;
+    pc.twf = (float)P.tw;
+    for (int a = 0; a < 3; a++) pc.hdtaf[a] = (float)P.hdta[a];
     auto fail_cuda = [&](cudaError_t e, const char* what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         FreeAll(c.get());
@@ -318,7 +334,7 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     for (size_t bi = 0; bi < P.blocks.size(); bi++) {
         const BlockPlan& B = P.blocks[bi];
         DevBlock& b = c->blocks[bi];
-        const size_t popbytes = (size_t)Q * B.popstride * sizeof(double);
+        const size_t popbytes = (size_t)Q * B.popstride * P.elem_bytes;
         for (int k = 0; k < 2; k++) {
             if ((e = cudaMalloc(&b.pop[k], popbytes)) != cudaSuccess)
                 return fail_cuda(e, "cudaMalloc(populations)");
@@ -405,6 +421,22 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
         d.ndef = B.ndeferred;
         d.dregions = b.dregions;
         d.ndregions = (int)dreg.size();
+        for (int i = 0; i < kMaxQ; i++) {
+            d.pop_off[i] = i < Q ? (long long)i * B.popstride : 0;
+            d.pull_off[i] = 0;
+        }
+        for (int i = 0; i < Q; i++) {
+            const int cx = P.dim == 3 ? Lattice<3>::cx(i) : Lattice<2>::cx(i);
+            const int cy = P.dim == 3 ? Lattice<3>::cy(i) : Lattice<2>::cy(i);
+            const int cz = P.dim == 3 ? Lattice<3>::cz(i) : 0;
+            d.pull_off[i] = (long long)i * B.popstride -
+                            (cx + cy * B.pitch + cz * B.plane);
+        }
+        for (int r = 0; r < kNumRegions; r++) {
+            const RegionInfo& R = B.region[r];
+            d.rflags[r] = (uint8_t)((R.cls < 0 ? kPure : R.cls) |
+                                    (R.fluidlike ? 4 : 0));
+        }
     }
     for (const HaloCopy& h : P.halos) {
         DevHalo dh;
@@ -478,10 +510,9 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
                            cudaMemcpyDeviceToDevice, ctx->stream));
     }
     const size_t bi = (size_t)(b - ctx->blocks.data());
-    int rc = dim == 3 ? InitBlock<3>(ctx, bi, b->macro[0], b->macro[1],
-                                     b->macro[2], b->macro[3], nullptr)
-                      : InitBlock<2>(ctx, bi, b->macro[0], b->macro[1],
-                                     b->macro[2], nullptr, nullptr);
+    int rc = MPLB_DISPATCH(ctx, InitBlock, ctx, bi, b->macro[0], b->macro[1],
+                           b->macro[2], dim == 3 ? b->macro[3] : nullptr,
+                           nullptr);
     if (rc != MPLBGPU_OK) return rc;
     ctx->initial = true;
     ctx->halos_pending = true;
@@ -504,21 +535,16 @@ mplbgpu_status mplbgpu_upload_f(mplbgpu_ctx* ctx, int block, const double* f) {
     CK(cudaMemcpyAsync(ctx->scratch, f, elems * sizeof(double),
                        cudaMemcpyHostToDevice, ctx->stream));
     const size_t bi = (size_t)(b - ctx->blocks.data());
-    rc = ctx->plan.dim == 3
-             ? InitBlock<3>(ctx, bi, nullptr, nullptr, nullptr, nullptr,
-                            ctx->scratch)
-             : InitBlock<2>(ctx, bi, nullptr, nullptr, nullptr, nullptr,
-                            ctx->scratch);
+    rc = MPLB_DISPATCH(ctx, InitBlock, ctx, bi, nullptr, nullptr, nullptr,
+                       nullptr, ctx->scratch);
     if (rc != MPLBGPU_OK) return rc;
     ctx->initial = true;
     ctx->halos_pending = true;
     ctx->initialised[bi] = true;
     // macro fields: moments of the uploaded f, q_old = q
-    rc = ctx->plan.dim == 3
-             ? Observe<3, kModeMacro>(ctx, bi, b->macro[0], b->macro[1],
-                                      b->macro[2], b->macro[3])
-             : Observe<2, kModeMacro>(ctx, bi, b->macro[0], b->macro[1],
-                                      b->macro[2], nullptr);
+    rc = MPLB_DISPATCH(ctx, Observe, ctx, (int)kModeMacro, bi, b->macro[0],
+                       b->macro[1], b->macro[2],
+                       ctx->plan.dim == 3 ? b->macro[3] : nullptr);
     if (rc != MPLBGPU_OK) return rc;
     for (int m = 0; m < ctx->plan.dim + 1; m++)
         CK(cudaMemcpyAsync(b->macro_old[m], b->macro[m],
@@ -539,7 +565,7 @@ mplbgpu_status mplbgpu_step(mplbgpu_ctx* ctx, int nsteps) {
     }
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int s = 0; s < nsteps; s++) {
-        rc = ctx->plan.dim == 3 ? StepOnce<3>(ctx) : StepOnce<2>(ctx);
+        rc = MPLB_DISPATCH(ctx, StepOnce, ctx);
         if (rc != MPLBGPU_OK) return rc;
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -623,11 +649,8 @@ mplbgpu_status mplbgpu_download_f(mplbgpu_ctx* ctx, int block, double* f) {
     rc = EnsureScratch(ctx, elems);
     if (rc != MPLBGPU_OK) return rc;
     const size_t bi = (size_t)(b - ctx->blocks.data());
-    rc = ctx->plan.dim == 3
-             ? Observe<3, kModeF>(ctx, bi, ctx->scratch, nullptr, nullptr,
-                                  nullptr)
-             : Observe<2, kModeF>(ctx, bi, ctx->scratch, nullptr, nullptr,
-                                  nullptr);
+    rc = MPLB_DISPATCH(ctx, Observe, ctx, (int)kModeF, bi, ctx->scratch,
+                       nullptr, nullptr, nullptr);
     if (rc != MPLBGPU_OK) return rc;
     CK(cudaMemcpyAsync(f, ctx->scratch, elems * sizeof(double),
                        cudaMemcpyDeviceToHost, ctx->stream));

@@ -231,6 +231,7 @@ RegionOp MakeEqm(const Lat& L, double CS, int nf, const int axis[3],
         switch (DvType(L, nf, axis, sign, l)) {
             case kDvIncoming:
                 op.in_mask |= 1u << l;
+                op.win += L.w[l];
                 break;
             case kDvOutgoing:
                 op.out_mask |= 1u << l;
@@ -247,6 +248,9 @@ RegionOp MakeEqm(const Lat& L, double CS, int nf, const int axis[3],
         }
     }
     op.denom = 1 - deltaRho - rhoParallel;
+    op.c0 = 2 * op.win - op.denom;
+    for (int l = 0; l < L.Q; l++)
+        if (op.par_mask >> l & 1u) op.am1[l] = op.a[l] - 1.0;
     return op;
 }
 

@@ -47,6 +47,10 @@ struct RegionOp {
     int nb_axis;        // EXTRAPOL copy source axis (-1: none)
     int nb_sign;
     double denom;       // EQM: (1 - deltaRho) - rhoParallel
+    double win;         // EQM: sum of the incoming weights (shifted forms)
+    double c0;          // EQM: 2 win - denom, so rhoWall - 1 =
+                        //      (c0 + 2 sum_in h) / denom (shifted forms)
+    double am1[kMaxQ];  // EQM: a - 1 per parallel population (shifted)
     double rho_given;   // EXTRAPOL
     double a[kMaxQ];    // EQM: feq(1,u_w)/w per parallel population (res)
     double b[kMaxQ];    // EQM: c.u_w per outgoing; HBB: 2 w (c.u_w)

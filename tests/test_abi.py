@@ -31,10 +31,11 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_build_targets_sm100a_only():
-    cmd = build.nvcc_command()
-    archs = [c for c in cmd if c.startswith("-gencode")]
-    assert archs == ["-gencode=arch=compute_100a,code=sm_100a"]
-    assert "-fmad=false" in cmd
+    for obj, cmd in build.compile_commands():
+        archs = [c for c in cmd if c.startswith("-gencode")]
+        assert archs == ["-gencode=arch=compute_100a,code=sm_100a"]
+        if obj.endswith(("mplbgpu.cu.o", "kernels_f64.cu.o")):
+            assert "-fmad=false" in cmd
 
 
 def test_descriptor_round_trip():

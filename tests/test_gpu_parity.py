@@ -28,7 +28,7 @@ def run_gpu(case, steps):
     return s, hist
 
 
-@pytest.mark.parametrize("name", golden_cases.names())
+@pytest.mark.parametrize("name", golden_cases.names(include_long=True))
 def test_gpu_matches_reference_golden(gpu_lib, name):
     g = golden_cases.load(name)
     s, hist = run_gpu(g["case"], g["steps"])

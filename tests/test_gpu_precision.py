@@ -1,0 +1,60 @@
+"""Shifted FP32 and FP16-storage forms against the FP64 form (which is
+bit-identical to the reference), and against the analytic Poiseuille
+profile.  Tolerances are relative L2 errors of the velocity."""
+import numpy as np
+import pytest
+
+from mplb_b200 import Solver, config
+
+pytestmark = pytest.mark.gpu
+
+
+def run(case, steps):
+    with Solver(case) as s:
+        s.init_uniform()
+        s.stream_collision(steps)
+        s.update_macro_vars()
+        return [a.copy() for b in case.block_ids for a in s.macro(b)]
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-5), ("fp16", 2e-3)])
+def test_poiseuille_shifted_vs_fp64(gpu_lib, prec, tol):
+    """The precision workload: body-force channel, halfway bounce-back walls
+    (relative L2 of u against the FP64 form)."""
+    mk = lambda p: config.poiseuille(2, 8, 64, g_lattice=1e-6,
+                                     wall="HalfwayBounceBack", precision=p)
+    ref = run(mk("fp64"), 20000)
+    got = run(mk(prec), 20000)
+    assert rel_l2(got[1], ref[1]) < tol
+    assert rel_l2(got[0], ref[0]) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 5e-5), ("fp16", 5e-3)])
+def test_cavity3d_shifted_vs_fp64(gpu_lib, prec, tol):
+    mk = lambda p: config.cavity(3, 48, 0.05, re=400, precision=p)
+    ref = run(mk("fp64"), 1500)
+    got = run(mk(prec), 1500)
+    speed = np.sqrt(ref[1] ** 2 + ref[2] ** 2 + ref[3] ** 2)
+    speed_p = np.sqrt(got[1] ** 2 + got[2] ** 2 + got[3] ** 2)
+    assert rel_l2(speed_p, speed) < tol
+    assert rel_l2(got[0], ref[0]) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 2e-3), ("fp32", 2e-3),
+                                      ("fp16", 5e-3)])
+def test_poiseuille_halfway_bounce_back_analytic(gpu_lib, prec, tol):
+    """u(y) = g / (2 nu) y (H - y) with the walls half a spacing outside the
+    first and last nodes (H = ny), lattice units."""
+    ny, tau, g = 32, 0.8, 1e-5
+    case = config.poiseuille(2, 4, ny, g_lattice=g, wall="HalfwayBounceBack",
+                             precision=prec)
+    m = run(case, 12000)
+    u = m[1][0, :, 2] / np.sqrt(3.0)
+    y = np.arange(ny) + 0.5
+    nu = (tau - 0.5) / 3
+    ua = g / (2 * nu) * y * (ny - y)
+    assert rel_l2(u, ua) < tol
