@@ -198,6 +198,62 @@ long long mplbgpu_launch_count(const mplbgpu_ctx* ctx);
 /* Device time of the most recent mplbgpu_step call's kernels (ms). */
 mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms);
 
+/* ---------------------------------------------------------------------
+ * Batched cavities (no counterpart in the reference, which runs one case
+ * per process): many independent square D2Q9 lid-driven cavities of
+ * different sizes advanced together.  Each cavity is the single-block
+ * case with halfway bounce-back on its four walls and a lid moving along
+ * +x; its residual is the reference's CalcResidualError +
+ * GetMaximumResidual on that cavity, with dt = 1 / ((n - 1) sqrt(3)).
+ * ------------------------------------------------------------------- */
+typedef struct {
+    int n;           /* nodes per side */
+    double lid_u;    /* lid speed in MPLB units (sqrt(3) x lattice units) */
+    double tau_ref;  /* MPLB tauRef (tau_L = tauRef / dt + 1/2) */
+} mplbgpu_cavity;
+
+typedef struct {
+    int tile_nodes;  /* nodes per tile = threads per CTA: 64, 128 or 256 */
+    int persistent;  /* 1: one cooperative launch per chunk of steps with a
+                        bounded grid barrier between steps; 0: one launch
+                        per step, a chunk replayed from a CUDA graph */
+    int chunk;       /* steps per chunk (even) */
+    int ctas_per_sm; /* CTAs per SM of the grid-stride launches */
+} mplbgpu_batch_tuning;
+
+typedef struct mplbgpu_batch mplbgpu_batch;
+
+/* precision: MPLBGPU_FP64 or MPLBGPU_FP32_SHIFTED. */
+mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
+                                    int precision, mplbgpu_batch** out);
+mplbgpu_status mplbgpu_batch_destroy(mplbgpu_batch* b);
+const char* mplbgpu_batch_last_error(const mplbgpu_batch* b);
+mplbgpu_status mplbgpu_batch_set_tuning(mplbgpu_batch* b,
+                                        const mplbgpu_batch_tuning* t);
+mplbgpu_status mplbgpu_batch_get_tuning(mplbgpu_batch* b,
+                                        mplbgpu_batch_tuning* t);
+/* Initial macroscopic fields of every cavity, packed cavity after cavity
+ * (n*n values each, y slowest); NULL means rho = 1 / u = v = 0.  f = feq,
+ * every cavity active again. */
+mplbgpu_status mplbgpu_batch_init(mplbgpu_batch* b, const double* rho,
+                                  const double* u, const double* v);
+/* nsteps steps of every active cavity; moments of the last step are kept. */
+mplbgpu_status mplbgpu_batch_step(mplbgpu_batch* b, int nsteps);
+/* Steps every active cavity, check_period at a time, until its residual is
+ * below criterion or max_steps have passed.  Per cavity (arrays of ncav,
+ * each may be NULL): steps taken, last residual, 1 if converged. */
+mplbgpu_status mplbgpu_batch_run(mplbgpu_batch* b, long long max_steps,
+                                 int check_period, double criterion,
+                                 long long* steps, double* residual,
+                                 int* converged);
+/* Moments of the last step or check, packed like mplbgpu_batch_init. */
+mplbgpu_status mplbgpu_batch_download_macro(mplbgpu_batch* b, double* rho,
+                                            double* u, double* v);
+/* Device time, node updates and kernel launches since the last init. */
+mplbgpu_status mplbgpu_batch_stats(mplbgpu_batch* b, double* device_ms,
+                                   long long* node_updates,
+                                   long long* launches);
+
 /* Residual sums that allocate nothing (no counterpart in the reference).
  * For callers that cannot call cudaMalloc where they need the reduction -
  * programs that give all device memory to their own pool at start-up, or

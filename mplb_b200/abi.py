@@ -87,6 +87,16 @@ class Desc(ctypes.Structure):
     ]
 
 
+class Cavity(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("lid_u", ctypes.c_double),
+                ("tau_ref", ctypes.c_double)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("tile_nodes", ctypes.c_int), ("persistent", ctypes.c_int),
+                ("chunk", ctypes.c_int), ("ctas_per_sm", ctypes.c_int)]
+
+
 class NativeLibraryError(RuntimeError):
     """The CUDA library is missing or failed to load."""
 
@@ -119,6 +129,25 @@ _SIGNATURES = {
     "mplbgpu_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
     "mplbgpu_last_step_ms": (ctypes.c_int, [ctypes.c_void_p,
                                             ctypes.c_void_p]),
+    "mplbgpu_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "mplbgpu_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "mplbgpu_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p,
+                                                ctypes.c_void_p]),
+    "mplbgpu_batch_get_tuning": (ctypes.c_int, [ctypes.c_void_p,
+                                                ctypes.c_void_p]),
+    "mplbgpu_batch_init": (ctypes.c_int, [ctypes.c_void_p] +
+                           [ctypes.c_void_p] * 3),
+    "mplbgpu_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mplbgpu_batch_run": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "mplbgpu_batch_download_macro": (ctypes.c_int, [ctypes.c_void_p] +
+                                     [ctypes.c_void_p] * 3),
+    "mplbgpu_batch_stats": (ctypes.c_int, [ctypes.c_void_p] +
+                            [ctypes.c_void_p] * 3),
     "mplbgpu_residual_sums_noalloc": (ctypes.c_int, [
         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong,
         ctypes.c_void_p, ctypes.c_void_p]),

@@ -18,11 +18,13 @@ OUT = os.path.join(HERE, "libmplbgpu.so")
 # low-precision kernels may.
 UNITS = [("mplbgpu.cu", ["-fmad=false"]), ("kernels_f64.cu", ["-fmad=false"]),
          ("kernels_lp.cu", ["-fmad=true"]), ("noalloc.cu", ["-fmad=false"]),
+         ("batch.cu", ["-fmad=false"]),
          ("plan.cpp", [])]
 SOURCES = [os.path.join(CSRC, u) for u, _ in UNITS]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "lattice.h",
                                             "plan.h", "launch.h",
-                                            "launch_impl.cuh")] + [
+                                            "launch_impl.cuh",
+                                            "batch_kernels.cuh")] + [
     os.path.join(HERE, "..", "include", "mplbgpu.h")]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 

@@ -1,0 +1,270 @@
+// Batched lid-driven cavities: many independent square D2Q9 blocks of
+// different sizes advanced together.
+//
+// Every cavity is the single-block case of the fused step (kernels.cuh)
+// with halfway bounce-back on its four walls, the top one moving: a
+// population whose upstream node lies beyond a wall takes the node's own
+// post-collision opposite population plus 2 w_i (c_i . u_wall) (the top
+// wall wins at the two top corners, as when the top boundary is defined
+// after the side walls).  Cavities are cut into tiles of consecutive nodes;
+// a CTA advances one tile per iteration of a grid-stride loop over the
+// active tiles (tiles of converged cavities are dropped between check
+// periods).  Population p of node k (= y n + x) of a cavity sits at
+// base + p n^2 + k, structure of arrays per cavity, no halo.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace mplb {
+
+struct BatchCav {
+    long long base;    // element offset of the cavity in a population array
+    long long mbase;   // offset of its nodes in the macro arrays
+    int n;             // nodes per side
+    int pad;
+    double omc;        // 1 - omega of this cavity
+    double dt;         // MPLB time step (residual normalisation)
+    float omcf;
+    float pad2;
+    double lidb[9];    // 2 w_i (c_i . u_lid) for populations bounced at the lid
+    float lidbf[9];
+};
+
+struct BatchDev {
+    const BatchCav* cavs;
+    const int2* tiles;      // active tiles: (cavity, first node)
+    const int* ntiles;      // number of active tiles (device word)
+    int tile_nodes;         // nodes per tile = threads per CTA
+    double* macro[3];       // rho, u, v of every cavity, packed
+    double* macro_old[3];
+};
+
+struct GridSync {           // bounded grid-wide barrier state
+    unsigned* count;
+    unsigned* gen;
+    int* err;               // set to 1 when a wait gives up
+    long long limit;        // polls before giving up
+};
+
+// One node of one cavity: pull with bounce-back, moments, collision.
+template <typename T, bool MACRO>
+__device__ __forceinline__ void BatchNode(const BatchDev& bd,
+                                          const PhysConst& pc,
+                                          const BatchCav& cv, int k,
+                                          const T* __restrict__ src,
+                                          T* __restrict__ dst) {
+    using L = Lattice<2>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int Q = 9;
+    const int n = cv.n;
+    const long long nn = (long long)n * n;
+    const int x = k % n, y = k / n;
+    const T* s = src + cv.base;
+    T* d = dst + cv.base;
+    C f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        const int sx = x - L::cx(i), sy = y - L::cy(i);
+        if (sx >= 0 && sx < n && sy >= 0 && sy < n) {
+            f[i] = P::Load(s, i * nn + (long long)sy * n + sx, i, pc);
+        } else {
+            C b = (C)0;
+            if (sy > n - 1) {
+                if constexpr (P::kShifted) b = cv.lidbf[i];
+                else b = cv.lidb[i];
+            }
+            f[i] = P::Load(s, L::opp(i) * nn + k, L::opp(i), pc) + b;
+        }
+    }
+    double rho, u[3];
+    MomentsCollideT<L, T>(f, pc, false, cv.omc, cv.omcf, rho, u);
+    Rng rng = SeedRng(pc.seed, cv.base + k);
+#pragma unroll
+    for (int i = 0; i < Q; i++) P::Store(d, i * nn + k, i, f[i], pc, rng);
+    if (MACRO) {
+        bd.macro[0][cv.mbase + k] = rho;
+        bd.macro[1][cv.mbase + k] = u[0];
+        bd.macro[2][cv.mbase + k] = u[1];
+    }
+}
+
+template <typename T, bool MACRO>
+__device__ __forceinline__ void BatchSweep(const BatchDev& bd,
+                                           const PhysConst& pc,
+                                           const T* __restrict__ src,
+                                           T* __restrict__ dst) {
+    const int nt = *bd.ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 tile = bd.tiles[t];
+        const BatchCav& cv = bd.cavs[tile.x];
+        const int k = tile.y + threadIdx.x;
+        if (k < cv.n * cv.n) BatchNode<T, MACRO>(bd, pc, cv, k, src, dst);
+    }
+}
+
+// One step over every active tile (a CUDA graph replays a chunk of these).
+template <typename T, bool MACRO>
+__global__ void __launch_bounds__(256)
+    BatchStepKernel(BatchDev bd, PhysConst pc, const T* __restrict__ src,
+                    T* __restrict__ dst) {
+    BatchSweep<T, MACRO>(bd, pc, src, dst);
+}
+
+// Grid-wide barrier with a bounded wait: thread 0 of each CTA arrives and
+// polls the generation word; after `limit` polls it records an error and
+// the kernel returns instead of waiting on.
+__device__ __forceinline__ bool GridBarrier(const GridSync& g,
+                                            unsigned& my_gen) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        const unsigned target = my_gen + 1;
+        __threadfence();
+        if (atomicAdd(g.count, 1u) == gridDim.x - 1) {
+            atomicExch(g.count, 0u);
+            __threadfence();
+            atomicExch(g.gen, target);
+        } else {
+            long long polls = 0;
+            while (atomicAdd(g.gen, 0u) != target) {
+                if (++polls > g.limit || atomicAdd(g.err, 0) != 0) {
+                    atomicExch(g.err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        my_gen = target;
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// `nsteps` steps in one launch (all CTAs co-resident, cooperative launch),
+// ping-ponging between a and b; moments are written on the last step when
+// `macro_last` is set.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    BatchPersistentKernel(BatchDev bd, PhysConst pc, T* a, T* b, int nsteps,
+                          int macro_last, GridSync gs) {
+    unsigned my_gen = 0;
+    if (threadIdx.x == 0) my_gen = atomicAdd(gs.gen, 0u);
+    for (int s = 0; s < nsteps; s++) {
+        const T* src = (s & 1) ? b : a;
+        T* dst = (s & 1) ? a : b;
+        if (macro_last && s == nsteps - 1)
+            BatchSweep<T, true>(bd, pc, src, dst);
+        else
+            BatchSweep<T, false>(bd, pc, src, dst);
+        if (s + 1 < nsteps && !GridBarrier(gs, my_gen)) return;
+        pc.seed += 1;
+    }
+}
+
+// Per active tile: sum (q - q_old)^2 and sum q^2 of rho, u, v; q_old <- q.
+__global__ void BatchResidualPartialKernel(BatchDev bd,
+                                           double* __restrict__ part);
+
+// Per active cavity c (CTA c): sums its tiles' partials in order and writes
+// max_q [sum (q - q_old)^2 / sum q^2] / (check_period dt) (the reference's
+// CalcResidualError + GetMaximumResidual on one cavity).
+__global__ void BatchResidualFinalKernel(BatchDev bd,
+                                         const double* __restrict__ part,
+                                         const int4* __restrict__ ranges,
+                                         int ncav, int check_period,
+                                         double* __restrict__ res);
+
+// Initial state: f^0 = feq(rho, u, v) from the packed macro fields
+// (KerInitialiseBGK2nd), then g^0 = collision of f^0 with its own moments,
+// as the first StreamCollision would do, into `a`.
+template <typename T>
+__global__ void BatchInitKernel(BatchDev bd, PhysConst pc,
+                                const int2* __restrict__ alltiles, int ntiles,
+                                T* __restrict__ a) {
+    using L = Lattice<2>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int2 tile = alltiles[t];
+        const BatchCav& cv = bd.cavs[tile.x];
+        const int k = tile.y + threadIdx.x;
+        if (k >= cv.n * cv.n) continue;
+        const long long nn = (long long)cv.n * cv.n;
+        const double rho = bd.macro[0][cv.mbase + k];
+        const double ux = bd.macro[1][cv.mbase + k];
+        const double uy = bd.macro[2][cv.mbase + k];
+        const double u2 = ux * ux + uy * uy;
+        C f[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            double cu = 0.0;
+            bool first = true;
+            const int c0 = L::cx(i), c1 = L::cy(i);
+            if (c0 != 0) {
+                cu = c0 > 0 ? pc.cs * ux : -(pc.cs * ux);
+                first = false;
+            }
+            if (c1 != 0) {
+                const double t1 = c1 > 0 ? pc.cs * uy : -(pc.cs * uy);
+                cu = first ? t1 : cu + t1;
+            }
+            if constexpr (P::kShifted)
+                f[i] = (C)(pc.w[i] *
+                           ((rho - 1.0) + rho * (cu + 0.5 * (cu * cu - u2))));
+            else
+                f[i] = (pc.w[i] * rho) * ((1.0 + cu) + 0.5 * (cu * cu - u2));
+        }
+        double r, u[3];
+        MomentsCollideT<L, T>(f, pc, false, cv.omc, cv.omcf, r, u);
+        Rng rng = SeedRng(0x5eedu, cv.base + k);
+#pragma unroll
+        for (int i = 0; i < 9; i++) P::Store(a + cv.base, i * nn + k, i, f[i], pc, rng);
+    }
+}
+
+}  // namespace mplb
+
+namespace mplb {
+
+// Host launchers, instantiated with the FP64 and the FP32 forms.
+template <typename T>
+struct BatchLaunch {
+    static cudaError_t Step(bool macro, int grid, int threads, cudaStream_t s,
+                            const BatchDev& bd, const PhysConst& pc,
+                            const T* src, T* dst) {
+        if (macro)
+            BatchStepKernel<T, true><<<grid, threads, 0, s>>>(bd, pc, src, dst);
+        else
+            BatchStepKernel<T, false><<<grid, threads, 0, s>>>(bd, pc, src, dst);
+        return cudaGetLastError();
+    }
+    static cudaError_t Persistent(int grid, int threads, cudaStream_t s,
+                                  const BatchDev& bd, const PhysConst& pc,
+                                  T* a, T* b, int nsteps, int macro_last,
+                                  const GridSync& gs) {
+        BatchDev bdv = bd;
+        PhysConst pcv = pc;
+        GridSync gsv = gs;
+        void* args[] = {&bdv, &pcv, &a, &b, &nsteps, &macro_last, &gsv};
+        return cudaLaunchCooperativeKernel(
+            (const void*)BatchPersistentKernel<T>, dim3(grid), dim3(threads),
+            args, 0, s);
+    }
+    static cudaError_t MaxCoResident(int threads, int* per_sm) {
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            per_sm, (const void*)BatchPersistentKernel<T>, threads, 0);
+    }
+    static cudaError_t Init(int grid, int threads, cudaStream_t s,
+                            const BatchDev& bd, const PhysConst& pc,
+                            const int2* alltiles, int ntiles, T* a) {
+        BatchInitKernel<T><<<grid, threads, 0, s>>>(bd, pc, alltiles, ntiles,
+                                                    a);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace mplb

@@ -264,7 +264,7 @@ __device__ __forceinline__ void MomentsF64(const double* f, const PhysConst& pc,
 template <typename L>
 __device__ __forceinline__ void CollideF64(double* f, const PhysConst& pc,
                                            bool fluidlike, double rho,
-                                           const double u[3]) {
+                                           const double u[3], double omc) {
     constexpr int Q = L::Q;
     const double cu0 = pc.cs * u[0], cu1 = pc.cs * u[1], cu2 = pc.cs * u[2];
     const double u2 = L::D == 3 ? (u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]
@@ -288,7 +288,7 @@ __device__ __forceinline__ void CollideF64(double* f, const PhysConst& pc,
         const double res = (1.0 + cu) + 0.5 * (cu * cu - u2);
         const double wr = pc.w[i] * rho;
         const double feq = wr * res;
-        double g = feq + pc.omc * (f[i] - feq);
+        double g = feq + omc * (f[i] - feq);
         if (force) g = g + pc.tw * (wr * pc.cf[i]);
         f[i] = g;
     }
@@ -321,61 +321,29 @@ __device__ __forceinline__ void MomentsShifted(const float* h,
     if (L::D == 2) u[2] = 0.0f;
 }
 
-// feq_i - w_i = w_i [(rho - 1) + rho (cu + (cu^2 - u^2) / 2)], written as
-// an even part A (shared by i and its opposite) and an odd part +-B; the
-// collision h' = omc h + omega heq (+ tau omega F_i, odd in c) then costs
-// about seven operations per population.
-// The paired even/odd form below saves arithmetic but rounds the even part
-// (which carries the mass) against the much larger odd part in
-// (ga + gb) and (ga - gb); measured on a forced channel it loses 15x more
-// accuracy than the direct form, so the direct form is the default.
-#ifndef MPLB_PAIRED_COLLISION
-#define MPLB_PAIRED_COLLISION 0
-#endif
+// feq_i - w_i = w_i [(rho - 1) + rho (cu + (cu^2 - u^2) / 2)], computed
+// directly so that no term is rounded against 1.  (Splitting it into the
+// parts even and odd in c_i saves arithmetic but rounds the even part, which
+// carries the mass, against the odd part; on a forced channel that was 15x
+// less accurate, so the direct form is used.)
 template <typename L>
 __device__ __forceinline__ void CollideShifted(float* h, const PhysConst& pc,
                                                bool fluidlike, float drho,
-                                               const float u[3]) {
+                                               const float u[3], float omc) {
     constexpr int Q = L::Q;
-#if !MPLB_PAIRED_COLLISION
-    {
-        const float rho = 1.0f + drho;
-        const float cu0 = pc.csf * u[0], cu1 = pc.csf * u[1],
-                    cu2 = pc.csf * u[2];
-        const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-        const bool force = pc.force && fluidlike;
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const float cu = (float)L::cx(i) * cu0 + (float)L::cy(i) * cu1 +
-                             (float)L::cz(i) * cu2;
-            const float heq =
-                pc.wf[i] * (drho + rho * (cu + 0.5f * (cu * cu - u2)));
-            float g = heq + pc.omcf * (h[i] - heq);
-            if (force) g += pc.twf * (pc.wf[i] * rho * pc.cff[i]);
-            h[i] = g;
-        }
-        return;
-    }
-#endif
-    constexpr int H = (Q - 1) / 2;  // opp(i) = i + H for 1 <= i <= H
     const float rho = 1.0f + drho;
     const float cu0 = pc.csf * u[0], cu1 = pc.csf * u[1], cu2 = pc.csf * u[2];
-    const float u2h = 0.5f * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-    const float om = 1.0f - pc.omcf;
-    const float omc = pc.omcf;
+    const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
     const bool force = pc.force && fluidlike;
-    h[0] = omc * h[0] + om * (pc.wf[0] * (drho - rho * u2h));
 #pragma unroll
-    for (int i = 1; i <= H; i++) {
-        const int j = i + H;
+    for (int i = 0; i < Q; i++) {
         const float cu = (float)L::cx(i) * cu0 + (float)L::cy(i) * cu1 +
                          (float)L::cz(i) * cu2;
-        const float wr = pc.wf[i] * rho;
-        const float ga = om * (pc.wf[i] * drho + wr * (0.5f * cu * cu - u2h));
-        float gb = om * (wr * cu);
-        if (force) gb += pc.twf * (wr * pc.cff[i]);
-        h[i] = omc * h[i] + (ga + gb);
-        h[j] = omc * h[j] + (ga - gb);
+        const float heq =
+            pc.wf[i] * (drho + rho * (cu + 0.5f * (cu * cu - u2)));
+        float g = heq + omc * (h[i] - heq);
+        if (force) g += pc.twf * (pc.wf[i] * rho * pc.cff[i]);
+        h[i] = g;
     }
 }
 
@@ -395,19 +363,39 @@ __device__ __forceinline__ void MomentsT(const typename Prec<T>::C* f,
     }
 }
 
+// Moments then collision with relaxation 1 - omega = omc (per cavity in
+// the batched solver); returns the moments in FP64.
+template <typename L, typename T>
+__device__ __forceinline__ void MomentsCollideT(typename Prec<T>::C* f,
+                                                const PhysConst& pc,
+                                                bool fluidlike, double omc,
+                                                float omcf, double& rho_out,
+                                                double u_out[3]) {
+    if constexpr (Prec<T>::kShifted) {
+        float drho, u[3];
+        MomentsShifted<L>(f, pc, fluidlike, drho, u);
+        rho_out = 1.0 + (double)drho;
+        u_out[0] = u[0];
+        u_out[1] = u[1];
+        u_out[2] = u[2];
+        CollideShifted<L>(f, pc, fluidlike, drho, u, omcf);
+    } else {
+        double rho, u[3];
+        MomentsF64<L>(f, pc, fluidlike, rho, u);
+        rho_out = rho;
+        u_out[0] = u[0];
+        u_out[1] = u[1];
+        u_out[2] = u[2];
+        CollideF64<L>(f, pc, fluidlike, rho, u, omc);
+    }
+}
+
 template <typename L, typename T>
 __device__ __forceinline__ void MomentsCollideT(typename Prec<T>::C* f,
                                                 const PhysConst& pc,
                                                 bool fluidlike) {
-    if constexpr (Prec<T>::kShifted) {
-        float drho, u[3];
-        MomentsShifted<L>(f, pc, fluidlike, drho, u);
-        CollideShifted<L>(f, pc, fluidlike, drho, u);
-    } else {
-        double rho, u[3];
-        MomentsF64<L>(f, pc, fluidlike, rho, u);
-        CollideF64<L>(f, pc, fluidlike, rho, u);
-    }
+    double rho, u[3];
+    MomentsCollideT<L, T>(f, pc, fluidlike, pc.omc, pc.omcf, rho, u);
 }
 
 // EQMDiffuseRefl (KerCutCellEQMDiffuseRefl3D, Src/boundary_kernel.inc:

@@ -60,3 +60,63 @@ __global__ void SumPartialKernel(const double* __restrict__ q, long long n,
 }
 
 }  // namespace mplb
+
+#include "batch_kernels.cuh"
+
+namespace mplb {
+
+template struct BatchLaunch<double>;
+
+__global__ void BatchResidualPartialKernel(BatchDev bd,
+                                           double* __restrict__ part) {
+    __shared__ double sh[6][256];
+    const int nt = *bd.ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 tile = bd.tiles[t];
+        const BatchCav& cv = bd.cavs[tile.x];
+        const int k = tile.y + threadIdx.x;
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        if (k < cv.n * cv.n) {
+            for (int m = 0; m < 3; m++) {
+                const double q = bd.macro[m][cv.mbase + k];
+                const double dq = q - bd.macro_old[m][cv.mbase + k];
+                v[2 * m] = dq * dq;
+                v[2 * m + 1] = q * q;
+                bd.macro_old[m][cv.mbase + k] = q;
+            }
+        }
+        for (int j = 0; j < 6; j++) sh[j][threadIdx.x] = v[j];
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w)
+                for (int j = 0; j < 6; j++)
+                    sh[j][threadIdx.x] = sh[j][threadIdx.x] + sh[j][threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x < 6) part[(long long)t * 6 + threadIdx.x] = sh[threadIdx.x][0];
+        __syncthreads();
+    }
+}
+
+__global__ void BatchResidualFinalKernel(BatchDev bd,
+                                         const double* __restrict__ part,
+                                         const int4* __restrict__ ranges,
+                                         int ncav, int check_period,
+                                         double* __restrict__ res) {
+    // ranges[c] = (cavity, first active tile, tile count, -)
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncav) return;
+    const int4 r = ranges[c];
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = r.y; t < r.y + r.z; t++)
+        for (int j = 0; j < 6; j++) s[j] = s[j] + part[(long long)t * 6 + j];
+    const BatchCav& cv = bd.cavs[r.x];
+    double mx = 0.0;
+    for (int m = 0; m < 3; m++) {
+        const double rel = (s[2 * m] / s[2 * m + 1]) / (check_period * cv.dt);
+        if (mx <= rel) mx = rel;
+    }
+    res[c] = mx;
+}
+
+}  // namespace mplb

@@ -10,3 +10,11 @@ template struct Launch<2, __half>;
 template struct Launch<3, __half>;
 
 }  // namespace mplb
+
+#include "batch_kernels.cuh"
+
+namespace mplb {
+
+template struct BatchLaunch<float>;
+
+}  // namespace mplb
