@@ -1,0 +1,38 @@
+// Drop-in glue: MPLB's StreamCollision / UpdateMacroVars(3D) /
+// CalcResidualError on the B200 path.  Compiled into the reference's own
+// build (with its headers and OPS); see INTEGRATION.md for the three early
+// returns that route the reference's functions here.
+//
+// On the first StreamCollision the glue reads what the setup API holds
+// (g_Block() and each Block::Neighbors(), BlockBoundaries(), g_Components(),
+// TimeStep(), SoundSpeed(), g_MacroBodyforce(), g_f()), creates an
+// mplbgpu context and uploads f; from then on the distributions stay on the
+// GPU.  UpdateMacroVars copies the moments (and, unless MPLB_B200_SYNC_F=0,
+// the distributions) back into the reference's dats so that Iterate's HDF5
+// writers see current data.  MPLB_B200_PRECISION=fp32|fp16 selects a
+// shifted storage form (default fp64, bit-identical to the reference).
+#ifndef MPLBGPU_DROPIN_H
+#define MPLBGPU_DROPIN_H
+
+#include "type.h"
+
+namespace mplbgpu_dropin {
+
+// True once the GPU context exists (after the first StreamCollision).
+bool Active();
+
+// Replaces the body of StreamCollision(time) (Src/evolution.cpp:137-193).
+void StreamCollision(const Real time);
+
+// Replaces UpdateMacroVars3D / UpdateMacroVars when Active().
+void UpdateMacroVars();
+
+// Replaces CalcResidualError (Src/flowfield_wrapper.cpp:31-89) when Active().
+void CalcResidualError();
+
+// Frees the GPU context.
+void Release();
+
+}  // namespace mplbgpu_dropin
+
+#endif

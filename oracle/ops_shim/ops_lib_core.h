@@ -193,6 +193,10 @@ ops_arg ops_arg_reduce(ops_reduction handle, int dim, const char* type,
  * ops_dat_get_raw_pointer): pointer to component 0 of point (0,0[,0]) plus
  * the element strides of the three axes. */
 char* ops_shim_point_ptr(ops_dat dat, int i, int j, int k);
+/* OPS's copies of a dat's interior points (no halo) to / from a user
+ * buffer, point-major with all components of a point together. */
+void ops_dat_fetch_data(ops_dat dat, int part, char* data);
+void ops_dat_set_data(ops_dat dat, int part, char* data);
 long ops_shim_stride(ops_dat dat, int axis);
 
 #endif  // OPS_LIB_CORE_H

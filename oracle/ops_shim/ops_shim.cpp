@@ -199,3 +199,23 @@ ops_arg ops_arg_reduce(ops_reduction handle, int dim, const char* /*type*/,
     a.red = handle;
     return a;
 }
+
+void ops_dat_fetch_data(ops_dat d, int /*part*/, char* data) {
+    const size_t bytes = (size_t)d->dim * (size_t)d->elem_size;
+    for (int k = 0; k < d->size[2]; k++)
+        for (int j = 0; j < d->size[1]; j++)
+            for (int i = 0; i < d->size[0]; i++) {
+                std::memcpy(data, ops_shim_point_ptr(d, i, j, k), bytes);
+                data += bytes;
+            }
+}
+
+void ops_dat_set_data(ops_dat d, int /*part*/, char* data) {
+    const size_t bytes = (size_t)d->dim * (size_t)d->elem_size;
+    for (int k = 0; k < d->size[2]; k++)
+        for (int j = 0; j < d->size[1]; j++)
+            for (int i = 0; i < d->size[0]; i++) {
+                std::memcpy(ops_shim_point_ptr(d, i, j, k), data, bytes);
+                data += bytes;
+            }
+}

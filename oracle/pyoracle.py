@@ -133,10 +133,12 @@ class Oracle:
         return vt, vg
 
 
-def run_reference(case, steps, kind="", workdir=None):
-    """Runs oracle/_ref/ref_case_{2d,3d}{kind}; returns dict with macro
-    arrays per block, f per block and the residual history."""
-    exe = os.path.join(REF_DIR, f"ref_case_{case.space_dim}d{kind}")
+def run_reference(case, steps, kind="", workdir=None, program="ref_case"):
+    """Runs oracle/_ref/{program}_{2d,3d}{kind}; returns dict with macro
+    arrays per block, f per block and the residual history.  program
+    "dropin_case" is the same driver with the B200 drop-in glue in place of
+    the reference's step."""
+    exe = os.path.join(REF_DIR, f"{program}_{case.space_dim}d{kind}")
     tmp = workdir or tempfile.mkdtemp(prefix="mplbref_")
     cfg = os.path.join(tmp, "case.json")
     with open(cfg, "w") as fh:

@@ -30,6 +30,12 @@
 
 #include "mplb.h"
 #include "ops_seq_v2.h"
+#ifdef MPLB_DROPIN
+// Built with MPLB_DROPIN the same driver runs the B200 path through the
+// drop-in glue (mplb_b200/dropin) in place of the reference's
+// StreamCollision / UpdateMacroVars / CalcResidualError.
+#include "mplbgpu_dropin.h"
+#endif
 
 namespace {
 Real g_rho0{1}, g_u0{0}, g_v0{0}, g_w0{0};
@@ -108,11 +114,35 @@ void UpdateMacroscopicBodyForce(const Real /*time*/) {
 }
 
 static void UpdateMacro() {
+#ifdef MPLB_DROPIN
+    if (mplbgpu_dropin::Active()) {
+        mplbgpu_dropin::UpdateMacroVars();
+        return;
+    }
+#endif
 #ifdef OPS_3D
     UpdateMacroVars3D();
 #else
     UpdateMacroVars();
 #endif
+}
+
+static void Step(Real time) {
+#ifdef MPLB_DROPIN
+    mplbgpu_dropin::StreamCollision(time);
+#else
+    StreamCollision(time);
+#endif
+}
+
+static void Residual() {
+#ifdef MPLB_DROPIN
+    if (mplbgpu_dropin::Active()) {
+        mplbgpu_dropin::CalcResidualError();
+        return;
+    }
+#endif
+    CalcResidualError();
 }
 
 static void DumpDat(ops_dat dat, const Block& block, const std::string& path) {
@@ -198,10 +228,10 @@ int main(int argc, const char** argv) {
     UpdateMacroscopicBodyForce(0);
 
     if (timingSteps > 0) {
-        for (long it = 0; it < steps; it++) StreamCollision(it * TimeStep());
+        for (long it = 0; it < steps; it++) Step(it * TimeStep());
         const auto t0 = std::chrono::steady_clock::now();
         for (long it = 0; it < timingSteps; it++) {
-            StreamCollision((steps + it) * TimeStep());
+            Step((steps + it) * TimeStep());
         }
         const auto t1 = std::chrono::steady_clock::now();
         long cells{0};
@@ -219,11 +249,11 @@ int main(int argc, const char** argv) {
     std::ofstream res(outDir + "/residual.txt");
     res.precision(17);
     for (long it = 0; it < steps; it++) {
-        StreamCollision(it * TimeStep());
+        Step(it * TimeStep());
         const long done{it + 1};
         if (!config.transient && done % (long)config.checkPeriod == 0) {
             UpdateMacro();
-            CalcResidualError();
+            Residual();
             const Real maxRes{GetMaximumResidual(config.checkPeriod)};
             res << done << " " << maxRes;
             for (auto& e : g_ResidualError()) res << " " << e.second;
