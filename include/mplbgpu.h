@@ -233,20 +233,24 @@ mplbgpu_status mplbgpu_batch_set_tuning(mplbgpu_batch* b,
 mplbgpu_status mplbgpu_batch_get_tuning(mplbgpu_batch* b,
                                         mplbgpu_batch_tuning* t);
 /* Initial macroscopic fields of every cavity, packed cavity after cavity
- * (n*n values each, y slowest); NULL means rho = 1 / u = v = 0.  f = feq,
- * every cavity active again. */
+ * (n*n values each, y slowest), in host or device memory; NULL means
+ * rho = 1 / u = v = 0.  f = feq, every cavity active again. */
 mplbgpu_status mplbgpu_batch_init(mplbgpu_batch* b, const double* rho,
                                   const double* u, const double* v);
 /* nsteps steps of every active cavity; moments of the last step are kept. */
 mplbgpu_status mplbgpu_batch_step(mplbgpu_batch* b, int nsteps);
 /* Steps every active cavity, check_period at a time, until its residual is
  * below criterion or max_steps have passed.  Per cavity (arrays of ncav,
- * each may be NULL): steps taken, last residual, 1 if converged. */
+ * each may be NULL): steps taken, last residual, and 1 if converged, 0 if
+ * not within max_steps, -1 if it diverged (NaN residual; the cavity is
+ * dropped at that check; unlike the reference's GetMaximumResidual, which
+ * skips NaN ratios and so reports a diverged run as converged). */
 mplbgpu_status mplbgpu_batch_run(mplbgpu_batch* b, long long max_steps,
                                  int check_period, double criterion,
                                  long long* steps, double* residual,
                                  int* converged);
-/* Moments of the last step or check, packed like mplbgpu_batch_init. */
+/* Moments of the last step or check, packed like mplbgpu_batch_init, into
+ * host or device memory. */
 mplbgpu_status mplbgpu_batch_download_macro(mplbgpu_batch* b, double* rho,
                                             double* u, double* v);
 /* Device time, node updates and kernel launches since the last init. */

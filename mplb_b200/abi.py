@@ -155,8 +155,51 @@ _SIGNATURES = {
 NOALLOC_MAX_NODES = 16777216
 
 
+# ---- include/mplbnn.h (warm-start network) ----
+NN_GRID = 128
+
+
+class NNView(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("nimg", ctypes.c_int),
+                ("h", ctypes.c_int), ("w", ctypes.c_int), ("c", ctypes.c_int),
+                ("ps", ctypes.c_longlong)]
+
+
+_vp, _ip, _fp, _dp = (ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
+                      ctypes.c_double)
+_llp = ctypes.POINTER(ctypes.c_longlong)
+_SIGNATURES.update({
+    "mplbnn_conv_forward": (_ip, [ctypes.POINTER(NNView), _vp, _ip, _vp, _ip,
+                                  ctypes.POINTER(NNView), _ip,
+                                  ctypes.POINTER(NNView), _vp]),
+    "mplbnn_conv_wgrad": (_ip, [ctypes.POINTER(NNView),
+                                ctypes.POINTER(NNView), _ip, _vp, _vp]),
+    "mplbnn_error": (ctypes.c_char_p, []),
+    "mplbnn_create": (_ip, [_ip, ctypes.POINTER(_vp)]),
+    "mplbnn_destroy": (_ip, [_vp]),
+    "mplbnn_last_error": (ctypes.c_char_p, [_vp]),
+    "mplbnn_synchronize": (_ip, [_vp]),
+    "mplbnn_param_count": (ctypes.c_longlong, [_vp]),
+    "mplbnn_layer_count": (_ip, []),
+    "mplbnn_layer_info": (_ip, [_ip, ctypes.POINTER(_ip), ctypes.POINTER(_ip),
+                                ctypes.POINTER(_ip), _llp, _llp]),
+    "mplbnn_init_params": (_ip, [_vp, ctypes.c_ulonglong]),
+    "mplbnn_set_params": (_ip, [_vp, _vp]),
+    "mplbnn_get_params": (_ip, [_vp, _vp]),
+    "mplbnn_get_grads": (_ip, [_vp, _vp]),
+    "mplbnn_forward": (_ip, [_vp, _vp, _ip, _vp]),
+    "mplbnn_loss_grad": (_ip, [_vp, _vp, _vp, _vp, _ip, ctypes.POINTER(_dp)]),
+    "mplbnn_adam_step": (_ip, [_vp, _fp, _fp, _fp, _fp]),
+    "mplbnn_fields_to_grid": (_ip, [_vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp,
+                                    _vp, _vp]),
+    "mplbnn_grid_to_fields": (_ip, [_vp, _vp, _ip, _vp, _vp, _vp, _vp, _vp,
+                                    _vp, _vp]),
+})
+
+
 def exported_symbols():
-    """Names every build of the library must export (from mplbgpu.h)."""
+    """Names every build of the library must export (from mplbgpu.h and
+    mplbnn.h)."""
     return sorted(_SIGNATURES)
 
 

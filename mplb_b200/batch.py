@@ -169,6 +169,8 @@ class Batch:
         self._check(self.lib.mplbgpu_batch_step(self.h, int(n)))
 
     def run(self, max_steps, check_period=1000, criterion=1e-8):
+        """Per cavity: steps, last residual, converged (bool); cavities whose
+        residual turned NaN are in `self.diverged` afterwards."""
         k = len(self.specs)
         steps = np.zeros(k, np.int64)
         res = np.zeros(k)
@@ -176,7 +178,8 @@ class Batch:
         self._check(self.lib.mplbgpu_batch_run(
             self.h, int(max_steps), int(check_period), float(criterion),
             steps.ctypes.data, res.ctypes.data, conv.ctypes.data))
-        return steps, res, conv.astype(bool)
+        self.diverged = conv == -1
+        return steps, res, conv == 1
 
     def macro(self):
         """[(rho, u, v)] per cavity, n x n arrays (MPLB units)."""

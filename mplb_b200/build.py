@@ -19,13 +19,16 @@ OUT = os.path.join(HERE, "libmplbgpu.so")
 UNITS = [("mplbgpu.cu", ["-fmad=false"]), ("kernels_f64.cu", ["-fmad=false"]),
          ("kernels_lp.cu", ["-fmad=true"]), ("noalloc.cu", ["-fmad=false"]),
          ("batch.cu", ["-fmad=false"]),
+         ("nn/conv.cu", ["-fmad=true"]), ("nn/warmstart.cu", ["-fmad=true"]),
          ("plan.cpp", [])]
 SOURCES = [os.path.join(CSRC, u) for u, _ in UNITS]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "lattice.h",
                                             "plan.h", "launch.h",
                                             "launch_impl.cuh",
-                                            "batch_kernels.cuh")] + [
-    os.path.join(HERE, "..", "include", "mplbgpu.h")]
+                                            "batch_kernels.cuh",
+                                            "nn/umma.cuh", "nn/conv.cuh",
+                                            "nn/conv_host.h")] + [
+    os.path.join(HERE, "..", "include", h) for h in ("mplbgpu.h", "mplbnn.h")]
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 
@@ -36,7 +39,7 @@ def compile_commands():
     """One nvcc command per translation unit (objects in _build/)."""
     cmds = []
     for unit, flags in UNITS:
-        obj = os.path.join(BUILD_DIR, unit + ".o")
+        obj = os.path.join(BUILD_DIR, unit.replace("/", "_") + ".o")
         cmds.append((obj, ["nvcc", "-O3", "-std=c++17", ARCH, "-lineinfo"] +
                      flags + ["-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                               "-c", os.path.join(CSRC, unit), "-o", obj]))

@@ -467,7 +467,7 @@ mplbgpu_status mplbgpu_batch_init(mplbgpu_batch* b, const double* rho,
     for (int m = 0; m < 3; m++) {
         if (src[m]) {
             BCK(cudaMemcpyAsync(b->macro[m], src[m], b->total_nodes * sizeof(double),
-                                cudaMemcpyHostToDevice, b->stream));
+                                cudaMemcpyDefault, b->stream));
         } else {
             fill.assign(b->total_nodes, m == 0 ? 1.0 : 0.0);
             BCK(cudaMemcpyAsync(b->macro[m], fill.data(),
@@ -557,7 +557,8 @@ mplbgpu_status mplbgpu_batch_run(mplbgpu_batch* b, long long max_steps,
             const int c = b->active[k];
             st[c] += n;
             rs[c] = hres[k];
-            if (n == check_period && hres[k] < criterion) cv[c] = 1;
+            if (std::isnan(hres[k])) cv[c] = -1;   // diverged: dropped
+            else if (n == check_period && hres[k] < criterion) cv[c] = 1;
             else still.push_back(c);
         }
         if (still.size() != b->active.size()) {
@@ -581,7 +582,7 @@ mplbgpu_status mplbgpu_batch_download_macro(mplbgpu_batch* b, double* rho,
     for (int m = 0; m < 3; m++)
         if (dst[m])
             BCK(cudaMemcpyAsync(dst[m], b->macro[m], b->total_nodes * sizeof(double),
-                                cudaMemcpyDeviceToHost, b->stream));
+                                cudaMemcpyDefault, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
     return MPLBGPU_OK;
 }

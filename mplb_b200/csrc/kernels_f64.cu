@@ -114,6 +114,12 @@ __global__ void BatchResidualFinalKernel(BatchDev bd,
     double mx = 0.0;
     for (int m = 0; m < 3; m++) {
         const double rel = (s[2 * m] / s[2 * m + 1]) / (check_period * cv.dt);
+        // A NaN ratio (a diverged cavity) is kept, not skipped: the host
+        // reports the cavity as diverged instead of converged.
+        if (isnan(rel)) {
+            mx = rel;
+            break;
+        }
         if (mx <= rel) mx = rel;
     }
     res[c] = mx;

@@ -1,5 +1,6 @@
 """The C-ABI library: builds for sm_100a, loads, exports every entry point
-include/mplbgpu.h declares; descriptor validation that needs no device."""
+include/mplbgpu.h and include/mplbnn.h declare; descriptor validation that
+needs no device."""
 import os
 import re
 import subprocess
@@ -12,8 +13,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def header_functions():
-    text = open(os.path.join(ROOT, "include", "mplbgpu.h")).read()
-    return sorted(set(re.findall(r"\b(mplbgpu_[a-z_]+)\s*\(", text)))
+    names = set()
+    for h in ("mplbgpu.h", "mplbnn.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"\b(mplb(?:gpu|nn)_[a-z_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_header_and_binding_agree():
@@ -24,7 +28,7 @@ def test_library_exports_every_declared_symbol():
     build.build()
     out = subprocess.run(["nm", "-D", "--defined-only", build.OUT],
                          capture_output=True, text=True, check=True).stdout
-    exported = set(re.findall(r"\bT (mplbgpu_[a-z_]+)", out))
+    exported = set(re.findall(r"\bT (mplb(?:gpu|nn)_[a-z_]+)", out))
     missing = [f for f in header_functions() if f not in exported]
     assert not missing, missing
     abi.load_library()  # loads without a device

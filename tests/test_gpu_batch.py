@@ -85,3 +85,16 @@ def test_batch_fp32_vs_fp64(gpu_lib):
         speed = np.hypot(a[1], a[2])
         ref = np.hypot(w[1], w[2])
         assert np.linalg.norm(speed - ref) / np.linalg.norm(ref) < 1e-4
+
+
+def test_diverged_cavity_is_reported_not_converged(gpu_lib):
+    """tau_L = 0.50015 with a fast lid: BGK blows up; the batch reports the
+    cavity as diverged (NaN residual) and keeps solving the healthy one."""
+    specs = [CavitySpec(64, 1.0e5, 0.08), CavitySpec(64, 100.0, 0.05)]
+    b = Batch(specs, "fp32", lib=gpu_lib)
+    b.init()
+    steps, res, conv = b.run(max_steps=100000, check_period=1000,
+                             criterion=1e-8)
+    assert b.diverged.tolist() == [True, False]
+    assert not conv[0] and np.isnan(res[0]) and steps[0] < 100000
+    assert conv[1] and res[1] < 1e-8
