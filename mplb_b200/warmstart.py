@@ -299,10 +299,12 @@ def rel_l2_per_cavity(specs, a, b):
 
 def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
              check_period=1000, criterion=1e-8, epochs=60, batch=32,
-             sizes=None, log=print, tuning=None):
+             log=print, tuning=None, lr_max=2e-3, details=None, **cavity_kw):
+    """The warm-start experiment; cavity_kw goes to cavity_set (sizes,
+    re_range, lid_range).  Returns (summary dict, trained network); per-
+    cavity arrays of the held-out set are added to `details` if given."""
     torch = _torch()
-    kw = {} if sizes is None else {"sizes": sizes}
-    specs = cavity_set(count, seed, **kw)
+    specs = cavity_set(count, seed, **cavity_kw)
     train_specs, held = specs[:n_train], specs[n_train:]
     res = {"count": count, "n_train": n_train, "held_out": len(held),
            "criterion": criterion, "check_period": check_period,
@@ -318,7 +320,8 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
         f"{twall:.1f}s")
     cond_all = torch.from_numpy(conditioning(train_specs)[keep]).cuda()
     net.init(seed)
-    hist, train_s = train(net, cond_all, targets, epochs, log=log)
+    hist, train_s = train(net, cond_all, targets, epochs, lr_max=lr_max,
+                          log=log)
     res["train_s"] = train_s
     res["loss_first"] = hist[0][1]
     res["loss_last"] = hist[-1][1]
@@ -360,6 +363,14 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
         if both.any() else None,
         "total_s": time.perf_counter() - t0,
     })
+    if details is not None:
+        details.update({
+            "n": [s.n for s in held], "re": [s.re for s in held],
+            "lid": [s.lid for s in held], "cold_steps": csteps.tolist(),
+            "warm_steps": wsteps.tolist(), "cold_conv": cconv.tolist(),
+            "warm_conv": wconv.tolist(), "init_u_error": init_err.tolist(),
+            "final_u_difference": final_diff.tolist(),
+            "loss_history": hist})
     return res, net
 
 
@@ -370,19 +381,25 @@ def main(argv=None):
                     help="256 cavities of side 64/96, 20 epochs")
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--max-steps", type=int, default=2_000_000)
+    ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--details-out", default=None)
     ap.add_argument("--params-out", default=None)
     a = ap.parse_args(argv)
-    kw = dict(epochs=a.epochs, max_steps=a.max_steps)
+    kw = dict(epochs=a.epochs, max_steps=a.max_steps, lr_max=a.lr)
     if a.quick:
         kw.update(count=256, n_train=192, sizes=(64, 96), epochs=20)
     log = lambda m: print(m, file=sys.stderr, flush=True)
-    res, net = pipeline(log=log, **kw)
+    details = {}
+    res, net = pipeline(log=log, details=details, **kw)
     line = json.dumps(res)
     print(line, flush=True)
     if a.out:
         with open(a.out, "a") as fh:
             fh.write(line + "\n")
+    if a.details_out:
+        with open(a.details_out, "w") as fh:
+            json.dump(details, fh)
     if a.params_out:
         np.save(a.params_out, net.params())
 
