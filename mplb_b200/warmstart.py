@@ -16,7 +16,11 @@ on them is a kernel of libmplbgpu.so.  There is no CPU path.
 
 runs the whole experiment: steady states of the training cavities, training,
 then the held-out cavities cold-started and warm-started to the same
-criterion, and prints one JSON line.
+criterion, and prints one JSON line;
+
+    python -m mplb_b200.warmstart trainbench [--steps K]
+
+times training steps on a fixed synthetic batch of 32.
 """
 import argparse
 import ctypes
@@ -374,9 +378,40 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
     return res, net
 
 
+def train_bench(steps=50, warmup=3, batch=32, seed=0):
+    """Time `steps` training steps (loss, gradients, Adam) on a fixed
+    synthetic batch; returns (ms per step, convolution FLOPs per step)."""
+    torch = _torch()
+    net = Network(batch)
+    net.init(1)
+    rng = np.random.default_rng(seed)
+    cond = torch.from_numpy(rng.uniform(0, 1, (batch, 3)).astype(
+        np.float32)).cuda()
+    tgt = torch.from_numpy((rng.standard_normal((batch, GRID, GRID, 3)) *
+                            0.1).astype(np.float32)).cuda()
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        net.loss_grad(cond, tgt)
+        net.adam(1e-4)
+    net.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.loss_grad(cond, tgt)
+        net.adam(1e-4)
+    net.synchronize()
+    ms = (time.perf_counter() - t0) / steps * 1e3
+    side = [128, 128, 64, 64, 32, 32, 16, 16, 32, 32, 64, 64, 128, 128, 128]
+    flops = 0.0
+    for l, (ci, co, t, _, _) in enumerate(net.layers()):
+        f = 2.0 * batch * side[l] ** 2 * co * t * ci
+        flops += f * (2 if l == 0 else 3)   # no data gradient of layer 0
+    return ms, flops
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["pipeline"])
+    ap.add_argument("cmd", choices=["pipeline", "trainbench"])
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--quick", action="store_true",
                     help="256 cavities of side 64/96, 20 epochs")
     ap.add_argument("--epochs", type=int, default=60)
@@ -386,6 +421,11 @@ def main(argv=None):
     ap.add_argument("--details-out", default=None)
     ap.add_argument("--params-out", default=None)
     a = ap.parse_args(argv)
+    if a.cmd == "trainbench":
+        ms, flops = train_bench(a.steps)
+        print(json.dumps({"train_step_ms": ms, "conv_flops_per_step": flops,
+                          "tflops": flops / ms / 1e9}))
+        return
     kw = dict(epochs=a.epochs, max_steps=a.max_steps, lr_max=a.lr)
     if a.quick:
         kw.update(count=256, n_train=192, sizes=(64, 96), epochs=20)
