@@ -46,7 +46,12 @@ struct PhysConst {
     // single-precision copies for the shifted forms
     float csf, omcf, twf;
     float hdtaf[3];
+    float hdta_csf[3];   // dt a / (2 CS): momentum the equilibrium's
+                         // half-step velocity shift adds, per unit density
     float cff[kMaxQ];
+    float wcff[kMaxQ];   // w_i CS c_i . a (body force per unit density)
+    float tw_omf;        // tau omega / omega: the force term relative to
+                         // the relaxation rate
     float wf[kMaxQ];
     float winvf[kMaxQ];  // 1 / w_i
     uint32_t seed;       // per launch (FP16 stochastic rounding)
@@ -67,6 +72,16 @@ struct BlockDev {
     // c_i . strides) and of the own value (i * popstride)
     long long pull_off[kMaxQ];
     long long pop_off[kMaxQ];
+    // the same offsets in 32 bits, valid when off32 (every offset and the
+    // whole population array fit in an int): one IMAD per access instead of
+    // 64-bit index arithmetic
+    int pull_off32[kMaxQ];
+    int pop_off32[kMaxQ];
+    int off32;
+    // the step runs as SplitStepKernel (every extent >= 3 and the interior
+    // region PURE); center_fluid: the interior is fluid-like
+    int split;
+    int center_fluid;
     // per region: class (bits 0-1) and fluid-like flag (bit 2)
     uint8_t rflags[kNumRegions];
 };
@@ -301,19 +316,24 @@ __device__ __forceinline__ void MomentsShifted(const float* h,
                                                bool fluidlike, float& drho,
                                                float u[3]) {
     constexpr int Q = L::Q;
-    drho = 0.0f;
+    // Opposite populations are combined first: h_i + h_opp(i) cancels the
+    // large odd parts (exactly, by Sterbenz's lemma, when they dominate) and
+    // h_i - h_opp(i) the even parts, so the partial sums stay at the size of
+    // the result instead of the size of the populations.  Summed in index
+    // order, the partial sums of rho - 1 reach the odd parts' size and their
+    // rounding breaks mass and momentum conservation coherently from step to
+    // step (30x larger velocity error on a forced channel).
+    drho = h[0];
 #pragma unroll
-    for (int i = 0; i < Q; i++) drho += h[i];
-    const float rinv = 1.0f / (1.0f + drho);
+    for (int i = 1; i < Q; i++)
+        if (i < L::opp(i)) drho += h[i] + h[L::opp(i)];
+    const float rinv = __frcp_rn(1.0f + drho);
 #pragma unroll
     for (int a = 0; a < L::D; a++) {
         float s = 0.0f;
 #pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const int c = comp<L>(i, a);
-            if (c > 0) s += h[i];
-            if (c < 0) s -= h[i];
-        }
+        for (int i = 0; i < Q; i++)
+            if (comp<L>(i, a) > 0) s += h[i] - h[L::opp(i)];
         s = pc.csf * s * rinv;
         if (pc.force_vel && fluidlike) s += pc.hdtaf[a];
         u[a] = s;
@@ -326,24 +346,82 @@ __device__ __forceinline__ void MomentsShifted(const float* h,
 // parts even and odd in c_i saves arithmetic but rounds the even part, which
 // carries the mass, against the odd part; on a forced channel that was 15x
 // less accurate, so the direct form is used.)
+//
+// The collision relaxes the non-equilibrium part m_i = h_i - heq_i, after
+// projecting out of it the mass and momentum that rounding put there:
+// m_i -= w_i (M0 + 3 c_i . M), with M0 = sum m_i and M = sum c_i m_i minus
+// its exact value (-rho dt a / (2 CS) where the equilibrium velocity carries
+// the half-step force shift, else 0).  In FP32 the equilibrium's moments
+// miss the computed (rho, u) by ~1e-8 relative (the weights and CS are not
+// representable), always with the same sign while u changes slowly; a
+// forced flow accumulates that as a spurious force (1e-3 relative velocity
+// error after 5e4 steps of a channel spinning up); with the projection BGK
+// conserves mass and momentum to the final rounding.  m_i is small, so the
+// sums over opposite pairs are accurate to its own ulp.
 template <typename L>
 __device__ __forceinline__ void CollideShifted(float* h, const PhysConst& pc,
                                                bool fluidlike, float drho,
                                                const float u[3], float omc) {
     constexpr int Q = L::Q;
     const float rho = 1.0f + drho;
+    const float hr = 0.5f * rho;   // rest population: w (drho - rho u^2 / 2)
     const float cu0 = pc.csf * u[0], cu1 = pc.csf * u[1], cu2 = pc.csf * u[2];
     const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    // m_i = h_i - heq_i.  heq is evaluated whole for each direction (the
+    // pair i, opp(i) shares cu^2 - u^2 only): splitting it into an even and
+    // an odd part rounded separately biases the stress it carries, which a
+    // channel spinning up shows as a 10x larger velocity error.
+    float m[Q];
+    m[0] = fmaf(-pc.wf[0], fmaf(-hr, u2, drho), h[0]);
+    float m0 = m[0], mv0 = 0.0f, mv1 = 0.0f, mv2 = 0.0f;
+#pragma unroll
+    for (int i = 1; i < Q; i++) {
+        if (i > L::opp(i)) continue;
+        const int j = L::opp(i);
+        float cu = 0.0f;
+        if (L::cx(i) > 0) cu += cu0;
+        if (L::cx(i) < 0) cu -= cu0;
+        if (L::cy(i) > 0) cu += cu1;
+        if (L::cy(i) < 0) cu -= cu1;
+        if (L::cz(i) > 0) cu += cu2;
+        if (L::cz(i) < 0) cu -= cu2;
+        const float y = fmaf(cu, cu, -u2);
+        m[i] = fmaf(-pc.wf[i], fmaf(rho, fmaf(0.5f, y, cu), drho), h[i]);
+        m[j] = fmaf(-pc.wf[j], fmaf(rho, fmaf(0.5f, y, -cu), drho), h[j]);
+        m0 += m[i] + m[j];
+        const float d = m[i] - m[j];
+        if (L::cx(i) > 0) mv0 += d;
+        if (L::cx(i) < 0) mv0 -= d;
+        if (L::cy(i) > 0) mv1 += d;
+        if (L::cy(i) < 0) mv1 -= d;
+        if (L::cz(i) > 0) mv2 += d;
+        if (L::cz(i) < 0) mv2 -= d;
+    }
+    if (pc.force_vel && fluidlike) {
+        mv0 += rho * pc.hdta_csf[0];
+        mv1 += rho * pc.hdta_csf[1];
+        mv2 += rho * pc.hdta_csf[2];
+    }
+    mv0 *= 3.0f;
+    mv1 *= 3.0f;
+    mv2 *= 3.0f;
+    // g_i = h_i + omega (w_i (M0 + 3 c_i . M) - m_i + F_i / omega), with
+    // F_i = w_i CS c_i.a tau omega rho: one rounding at the size of h_i.
+    const float om = 1.0f - omc;
     const bool force = pc.force && fluidlike;
+    const float fr = pc.tw_omf * rho;
 #pragma unroll
     for (int i = 0; i < Q; i++) {
-        const float cu = (float)L::cx(i) * cu0 + (float)L::cy(i) * cu1 +
-                         (float)L::cz(i) * cu2;
-        const float heq =
-            pc.wf[i] * (drho + rho * (cu + 0.5f * (cu * cu - u2)));
-        float g = heq + omc * (h[i] - heq);
-        if (force) g += pc.twf * (pc.wf[i] * rho * pc.cff[i]);
-        h[i] = g;
+        float cm = m0;
+        if (L::cx(i) > 0) cm += mv0;
+        if (L::cx(i) < 0) cm -= mv0;
+        if (L::cy(i) > 0) cm += mv1;
+        if (L::cy(i) < 0) cm -= mv1;
+        if (L::cz(i) > 0) cm += mv2;
+        if (L::cz(i) < 0) cm -= mv2;
+        float t = fmaf(pc.wf[i], cm, -m[i]);
+        if (force) t = fmaf(fr, pc.wcff[i], t);
+        h[i] = fmaf(om, t, h[i]);
     }
 }
 
@@ -461,32 +539,32 @@ __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
 // Fused step over one block.  kModeStep writes g^{n+1}; kModeMacro and
 // kModeF recompute the current f = post-boundary populations from the
 // previous g and write moments or f (FP64, dense) instead.
-// The shifted forms are instruction-issue bound: holding them to 64
-// registers (8 CTAs of 128 threads per SM) keeps enough warps to issue from.
+// The shifted forms hold two interior nodes per thread (PureNodePair):
+// 6 CTAs of 128 threads per SM (<= 85 registers) keeps both nodes in
+// registers; 8 CTAs (64 registers) spilled and measured no faster.
 #ifndef MPLB_LP_MIN_BLOCKS
-#define MPLB_LP_MIN_BLOCKS 8
+#define MPLB_LP_MIN_BLOCKS 6
 #endif
 // The FP64 form holds 19 doubles per node; 5 CTAs per SM (<= 102 registers)
 // keeps it spill-free with 20 warps of loads in flight.
 #ifndef MPLB_F64_MIN_BLOCKS
 #define MPLB_F64_MIN_BLOCKS 5
 #endif
-template <int D, typename T, int MODE>
-__global__ void __launch_bounds__(128, std::is_same<T, double>::value
-                                           ? MPLB_F64_MIN_BLOCKS
-                                           : MPLB_LP_MIN_BLOCKS)
-    StepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
-               T* __restrict__ dst, double* __restrict__ out0,
-               double* __restrict__ out1, double* __restrict__ out2,
-               double* __restrict__ out3) {
+// One node of the step, any region class.
+template <int D, typename T, int MODE, bool O32>
+__device__ __forceinline__ void StepNode(const BlockDev& b,
+                                         const PhysConst& pc,
+                                         const T* __restrict__ src,
+                                         T* __restrict__ dst,
+                                         double* __restrict__ out0,
+                                         double* __restrict__ out1,
+                                         double* __restrict__ out2,
+                                         double* __restrict__ out3, int x,
+                                         int y, int z) {
     using L = Lattice<D>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = D == 3 ? (int)blockIdx.z : 0;
-    if (x >= b.n[0]) return;
     const int r = RegionOf(x, y, z, b.n, D);
     const int rf = b.rflags[r];
     const int cls = rf & 3;
@@ -494,9 +572,16 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     const long long node = NodeIndex<D>(b, x, y, z);
     C f[Q];
     if (cls == kPure) {
+        if constexpr (O32) {
+            const T* ps = src + node;
 #pragma unroll
-        for (int i = 0; i < Q; i++)
-            f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
+            for (int i = 0; i < Q; i++)
+                f[i] = P::Load(ps, b.pull_off32[i], i, pc);
+        } else {
+#pragma unroll
+            for (int i = 0; i < Q; i++)
+                f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
+        }
     } else {
         const RegionInfo& R = b.regions[r];
         const uint32_t pull = R.pull;
@@ -541,9 +626,167 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     }
     MomentsCollideT<L, T>(f, pc, fl);
     Rng rng = SeedRng(pc.seed, node);
+    if constexpr (O32) {
+        T* pd = dst + node;
 #pragma unroll
-    for (int i = 0; i < Q; i++)
-        P::Store(dst, OwnIndex(b, node, i), i, f[i], pc, rng);
+        for (int i = 0; i < Q; i++)
+            P::Store(pd, b.pop_off32[i], i, f[i], pc, rng);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            P::Store(dst, OwnIndex(b, node, i), i, f[i], pc, rng);
+    }
+}
+
+template <int D, typename T, int MODE, bool O32 = false>
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value
+                                           ? MPLB_F64_MIN_BLOCKS
+                                           : MPLB_LP_MIN_BLOCKS)
+    StepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
+               T* __restrict__ dst, double* __restrict__ out0,
+               double* __restrict__ out1, double* __restrict__ out2,
+               double* __restrict__ out3) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = D == 3 ? (int)blockIdx.z : 0;
+    if (x >= b.n[0]) return;
+    StepNode<D, T, MODE, O32>(b, pc, src, dst, out0, out1, out2, out3, x, y,
+                              z);
+}
+
+// Two interior nodes of the same x in consecutive interior rows: both
+// nodes' loads are issued before either is computed, so a warp keeps 38
+// loads in flight instead of 19 (the FP32 and FP16 forms move too few bytes
+// per load to cover HBM latency with one node per thread).
+template <int D, typename T, bool O32>
+__device__ __forceinline__ void PureNodePair(const BlockDev& b,
+                                             const PhysConst& pc,
+                                             const T* __restrict__ src,
+                                             T* __restrict__ dst, int x,
+                                             int ya, int za, int yb, int zb,
+                                             bool second) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int Q = L::Q;
+    const long long na = NodeIndex<D>(b, x, ya, za);
+    const long long nb = second ? NodeIndex<D>(b, x, yb, zb) : na;
+    C fa[Q], fb[Q];
+    if constexpr (O32) {
+        const T* pa = src + na;
+        const T* pb = src + nb;
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            fa[i] = P::Load(pa, b.pull_off32[i], i, pc);
+            fb[i] = P::Load(pb, b.pull_off32[i], i, pc);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            fa[i] = P::Load(src, PullIndex<L>(b, na, i), i, pc);
+            fb[i] = P::Load(src, PullIndex<L>(b, nb, i), i, pc);
+        }
+    }
+    const bool fl = b.center_fluid != 0;
+    MomentsCollideT<L, T>(fa, pc, fl);
+    Rng ra = SeedRng(pc.seed, na);
+    if constexpr (O32) {
+        T* pd = dst + na;
+#pragma unroll
+        for (int i = 0; i < Q; i++) P::Store(pd, b.pop_off32[i], i, fa[i], pc, ra);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            P::Store(dst, OwnIndex(b, na, i), i, fa[i], pc, ra);
+    }
+    if (!second) return;
+    MomentsCollideT<L, T>(fb, pc, fl);
+    Rng rb = SeedRng(pc.seed, nb);
+    if constexpr (O32) {
+        T* pd = dst + nb;
+#pragma unroll
+        for (int i = 0; i < Q; i++) P::Store(pd, b.pop_off32[i], i, fb[i], pc, rb);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            P::Store(dst, OwnIndex(b, nb, i), i, fb[i], pc, rb);
+    }
+}
+
+// Rows of interior nodes handled per x-face block of SplitStepKernel, and
+// interior rows per thread (two for the low-precision forms; the FP64 form
+// moves enough bytes per load and has no registers for a second node).
+constexpr int kSplitRows = 64;
+template <typename T>
+__host__ __device__ constexpr int SplitPair() { return sizeof(T) < 8 ? 2 : 1; }
+
+// The step with no warp mixing interior and boundary nodes (a warp holding
+// one boundary node runs that node's boundary programme with the other 31
+// lanes idle: at 128^3 a third of the issue slots had no work).  One launch,
+// three kinds of CTA by blockIdx.x:
+//   1. shell rows: every row with y or z on the block boundary (coalesced);
+//   2. per chunk of 64 interior rows, one CTA for their x = 0 and x = n0 - 1
+//      nodes, followed by
+//   3. the CTAs of those rows' interior nodes, two rows per CTA (each
+//      thread one node of each; PureNodePair).  A row's CTAs start on the
+//      row's first node so every store begins on the row's 32-byte boundary
+//      (the two x-face lanes idle); the x-face CTA runs next to them, so the
+//      sectors they share meet in L2 instead of costing a read-modify-write
+//      in HBM.
+template <int D, typename T, bool O32>
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value
+                                           ? MPLB_F64_MIN_BLOCKS
+                                           : MPLB_LP_MIN_BLOCKS)
+    SplitStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
+                    T* __restrict__ dst) {
+    const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int ny = b.n[1] - 2;
+    const int nz = D == 3 ? b.n[2] : 1;
+    const long long nsr = (long long)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
+    long long blk = blockIdx.x;
+    if (blk < nsr) {
+        const int row = (int)(blk / nbx);
+        const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
+        if (x >= b.n[0]) return;
+        int y, z;
+        if (row < 2 * nz) {
+            y = (row & 1) ? b.n[1] - 1 : 0;
+            z = row >> 1;
+        } else {
+            const int r2 = row - 2 * nz;
+            z = (r2 & 1) ? b.n[2] - 1 : 0;
+            y = 1 + (r2 >> 1);
+        }
+        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
+                                       nullptr, nullptr, x, y, z);
+        return;
+    }
+    blk -= nsr;
+    const long long rows = (long long)ny * (D == 3 ? b.n[2] - 2 : 1);
+    constexpr int pair = SplitPair<T>();
+    const long long per_chunk = 1 + (long long)(kSplitRows / pair) * nbx;
+    const long long chunk = blk / per_chunk;
+    const int w = (int)(blk % per_chunk);
+    if (w == 0) {
+        const long long r = chunk * kSplitRows + (threadIdx.x >> 1);
+        if (threadIdx.x >= 2 * kSplitRows || r >= rows) return;
+        const int x = (threadIdx.x & 1) ? b.n[0] - 1 : 0;
+        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
+                                       nullptr, nullptr, x,
+                                       1 + (int)(r % ny),
+                                       D == 3 ? 1 + (int)(r / ny) : 0);
+        return;
+    }
+    // interior CTAs: rows r (and r + 1 when paired)
+    const long long r = chunk * kSplitRows + pair * ((w - 1) / nbx);
+    const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
+    if (r >= rows || x < 1 || x > b.n[0] - 2) return;
+    const long long r1 = r + 1;
+    PureNodePair<D, T, O32>(b, pc, src, dst, x, 1 + (int)(r % ny),
+                            D == 3 ? 1 + (int)(r / ny) : 0,
+                            1 + (int)(r1 % ny),
+                            D == 3 ? 1 + (int)(r1 / ny) : 0,
+                            pair == 2 && r1 < rows);
 }
 
 // Deferred nodes: thread t -> (region, node).

@@ -11,7 +11,26 @@ cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const BlockDev& b, const PhysConst& pc,
                                const T* src, T* dst, double* o0, double* o1,
                                double* o2, double* o3) {
-    if (mode == kModeStep)
+    if (mode == kModeStep && b.split) {
+        const long long nbx = (b.n[0] + kStepThreads - 1) / kStepThreads;
+        const long long ny = b.n[1] - 2;
+        const long long nz = D == 3 ? b.n[2] : 1;
+        const long long rows = ny * (D == 3 ? b.n[2] - 2 : 1);
+        const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
+        const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
+        const long long blocks =
+            nsr + chunks * (1 + (kSplitRows / SplitPair<T>()) * nbx);
+        if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        if (b.off32)
+            SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(
+                b, pc, src, dst);
+        else
+            SplitStepKernel<D, T, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(
+                b, pc, src, dst);
+    } else if (mode == kModeStep && b.off32)
+        StepKernel<D, T, kModeStep, true><<<grid, kStepThreads, 0, s>>>(
+            b, pc, src, dst, o0, o1, o2, o3);
+    else if (mode == kModeStep)
         StepKernel<D, T, kModeStep><<<grid, kStepThreads, 0, s>>>(
             b, pc, src, dst, o0, o1, o2, o3);
     else if (mode == kModeMacro)

@@ -314,6 +314,9 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     pc.omcf = (float)P.omc;
     pc.twf = (float)P.tw;
     for (int a = 0; a < 3; a++) pc.hdtaf[a] = (float)P.hdta[a];
+    for (int a = 0; a < 3; a++) pc.hdta_csf[a] = (float)(P.hdta[a] / P.cs);
+    for (int i = 0; i < kMaxQ; i++) pc.wcff[i] = (float)(P.w[i] * P.cf[i]);
+    pc.tw_omf = (float)(P.tw / (1.0 - P.omc));
     auto fail_cuda = [&](cudaError_t e, const char* what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         FreeAll(c.get());
@@ -432,11 +435,25 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             d.pull_off[i] = (long long)i * B.popstride -
                             (cx + cy * B.pitch + cz * B.plane);
         }
+        // 32-bit offsets from the node's own address: every access stays
+        // within one population array of Q * popstride elements
+        const long long span = (long long)Q * B.popstride;
+        d.off32 = span < 0x7fffffffLL ? 1 : 0;
+        for (int i = 0; i < kMaxQ; i++) {
+            d.pull_off32[i] = d.off32 ? (int)d.pull_off[i] : 0;
+            d.pop_off32[i] = d.off32 ? (int)d.pop_off[i] : 0;
+        }
         for (int r = 0; r < kNumRegions; r++) {
             const RegionInfo& R = B.region[r];
             d.rflags[r] = (uint8_t)((R.cls < 0 ? kPure : R.cls) |
                                     (R.fluidlike ? 4 : 0));
         }
+        const int center = 13;   // interior on every axis (RegionOf)
+        d.split = (B.n[0] >= 3 && B.n[1] >= 3 && (P.dim == 2 || B.n[2] >= 3) &&
+                   (d.rflags[center] & 3) == kPure)
+                      ? 1
+                      : 0;
+        d.center_fluid = B.region[center].fluidlike ? 1 : 0;
     }
     for (const HaloCopy& h : P.halos) {
         DevHalo dh;

@@ -14,14 +14,6 @@ __device__ __forceinline__ uint8_t* Align1024(uint8_t* p) {
     return p + ((1024u - (s & 1023u)) & 1023u);
 }
 
-// Bounded wait that ignores the CTA's error word: used where the wait must
-// end before resources are released (in-flight copies, in-flight MMAs).
-__device__ __forceinline__ bool BarWaitDrain(uint64_t* bar, uint32_t parity) {
-    for (long long i = 0; i < kWaitLimit; i++)
-        if (BarTryWait(bar, parity)) return true;
-    return false;
-}
-
 __device__ __forceinline__ void Flag(volatile int* cta_err, int* err) {
     *cta_err = 1;
     atomicExch(err, 1);

@@ -78,6 +78,14 @@ __device__ __forceinline__ bool BarWait(uint64_t* bar, uint32_t parity,
     return false;
 }
 
+// Bounded wait that ignores any error word (used to drain copies still in
+// flight before a CTA exits after an error).
+__device__ __forceinline__ bool BarWaitDrain(uint64_t* bar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; i++)
+        if (BarTryWait(bar, parity)) return true;
+    return false;
+}
+
 __device__ __forceinline__ void PrefetchTmap(const CUtensorMap* m) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(m))
                  : "memory");
