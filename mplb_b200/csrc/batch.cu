@@ -139,6 +139,8 @@ int UploadActive(mplbgpu_batch* b) {
                             b->stream));
         pos += b->ntile[c];
     }
+    // one-step graphs are captured with one CTA per active tile
+    if (pos != b->ntiles_active && !b->tune.persistent) DropGraphs(b);
     b->ntiles_active = pos;
     BCK(cudaMemcpyAsync(b->ntiles_dev, &b->ntiles_active, sizeof(int),
                         cudaMemcpyHostToDevice, b->stream));
@@ -149,7 +151,12 @@ int UploadActive(mplbgpu_batch* b) {
     return MPLBGPU_OK;
 }
 
+// One-step launches: one CTA per active tile (the hardware keeps the SMs
+// full and a finished CTA's slot goes to the next tile; a grid-stride loop
+// over tiles serialised each CTA's dependent tile -> cavity -> population
+// loads).  Persistent launches: the co-resident CTA count.
 int Grid(mplbgpu_batch* b, bool persistent) {
+    if (!persistent) return std::max(1, b->ntiles_active);
     int dev = 0, sms = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -210,8 +217,9 @@ int Chunk(mplbgpu_batch* b, int nsteps, bool macro_last) {
 }
 
 // A chunk of `tune.chunk` steps replayed from a CUDA graph (captured on
-// first use; the active tile list lives in device memory, so the graph stays
-// valid when cavities converge).
+// first use; the active tile list lives in device memory, so a persistent
+// graph stays valid when cavities converge; one-step graphs are captured
+// again when the active tile count, their grid, changes).
 int GraphChunk(mplbgpu_batch* b, bool macro_last) {
     const int n = b->tune.chunk;
     cudaGraphExec_t& g = b->graph[macro_last ? 1 : 0];
@@ -351,6 +359,7 @@ mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
         const double omega = dt / (cv.tau_ref + 0.5 * dt);
         h.omc = 1 - omega;
         h.omcf = (float)h.omc;
+        h.ninv = 1.0f / (float)cv.n;
         h.dt = dt;
         for (int i = 0; i < 9; i++) {
             // 2 w_i (c_i . u_lid) in the halfway bounce-back's operation order

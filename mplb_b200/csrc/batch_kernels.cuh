@@ -25,7 +25,7 @@ struct BatchCav {
     double omc;        // 1 - omega of this cavity
     double dt;         // MPLB time step (residual normalisation)
     float omcf;
-    float pad2;
+    float ninv;        // 1 / n (row of node k: (k + 1/2) / n rounded down)
     double lidb[9];    // 2 w_i (c_i . u_lid) for populations bounced at the lid
     float lidbf[9];
 };
@@ -59,7 +59,11 @@ __device__ __forceinline__ void BatchNode(const BatchDev& bd,
     constexpr int Q = 9;
     const int n = cv.n;
     const long long nn = (long long)n * n;
-    const int x = k % n, y = k / n;
+    // k / n without an integer division: (k + 1/2) / n is at least 1/(2n)
+    // from an integer and the float product is off by less than
+    // (k + 1/2) / n * 2^-22, so truncating it is exact while n <= 1024
+    const int y = n <= 1024 ? (int)(((float)k + 0.5f) * cv.ninv) : k / n;
+    const int x = k - y * n;
     const T* s = src + cv.base;
     T* d = dst + cv.base;
     C f[Q];
