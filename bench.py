@@ -7,6 +7,7 @@ over the whole 256^3 block.  Each population array is 2.7 GB, far larger
 than the 126 MB L2, so consecutive timed steps cannot hit in L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --workload cavities-warmstart
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own cavity (no
 data-path exchange; weak scaling) and the value is the total node updates
@@ -38,6 +39,13 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
                   ("fp32", 2): 72, ("fp16", 3): 76, ("fp16", 2): 36}
+# DRAM bytes per node update of the step kernel measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of SplitStepKernel<3,double>
+# on the 128^3 cavity, 2 launches: 615 MB / 2,097,152 nodes; FP32: 311 MB;
+# traffic grows with the node count, so a 256^3 launch moves this x
+# 16,777,216 bytes); profiles/splitstepkernel_cavity3d_d3q19_fp64.md and
+# _fp32.md have the commands.
+TRAFFIC_PER_NODE = {("fp64", 3): 293.0, ("fp32", 3): 148.0}
 METRIC = "MLUPS (D3Q19 3D lid-driven cavity 256^3)"
 DTYPES = {"fp64": "f64", "fp32": "f32 (shifted f - w)",
           "fp16": "f16 storage of (f - w)/w, f32 arithmetic"}
@@ -53,6 +61,11 @@ def parse():
     p.add_argument("--precision", default="fp64",
                    choices=["fp64", "fp32", "fp16"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="cavity3d",
+                   choices=["cavity3d", "cavities-warmstart"],
+                   help="cavities-warmstart: the batched-cavity learned warm "
+                        "start experiment (minutes; 1 GPU)")
+    p.add_argument("--epochs", type=int, default=60)
     return p.parse_args()
 
 
@@ -205,11 +218,56 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def run_warmstart(args, rank, local):
+    """The second half of the metric: wall time to residual 1e-8 of the
+    1,024 held-out cavities of the 4,096-cavity batched workload, warm-
+    started from the trained network (inference, resampling and the solve
+    inside the timed region) against cold-started (the same batch object,
+    same tuning).  One GPU; the other ranks of a multi-rank launch idle."""
+    import torch
+    from mplb_b200 import warmstart as ws
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    res, _ = ws.pipeline(epochs=args.epochs, log=lambda m: None)
+    clk = clocks.stop()
+    line = {
+        "metric": "wall-time to residual 1e-8, 1,024 held-out D2Q9 "
+                  "cavities, learned warm start",
+        "value": res["warm_wall_s"], "unit": "s", "n_gpus": 1,
+        "steps": None, "warmup": None, "higher_is_better": False,
+        "scaling": "none", "vs_baseline": None,
+        "dtype": "f32 (shifted f - w) LBM; bf16 network", "data": "synthetic",
+        "config": {"workload": "4,096 D2Q9 lid-driven cavities (N in "
+                               "{64..256}, Re 100-3200, U 0.02-0.08, seed "
+                               "20261203); first 3,072 train, last 1,024 "
+                               "held out",
+                   "parallelism": "single GPU"},
+        "cold_wall_s": res["cold_wall_s"],
+        "speedup_vs_cold": res["speedup_wall"],
+        "warm_start": res,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args)
+    if args.impl == "reference" and args.workload == "cavities-warmstart":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no batched or learned "
+                              "solver; its CPU cavity solver is timed on "
+                              "the default workload"}))
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.workload == "cavities-warmstart":
+        run_warmstart(args, rank, local)
         return
     import numpy as np
     import torch
@@ -302,7 +360,10 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
-                     "bytes_per_node": bpn, "traffic": None},
+                     "bytes_per_node": bpn,
+                     "traffic": (TRAFFIC_PER_NODE[(case.precision, 3)] * nodes
+                                 if (case.precision, 3) in TRAFFIC_PER_NODE
+                                 else None)},
         "e2e": {"value": e2e, "unit": "MLUPS",
                 "h2d_bytes_per_step": 4 * 8 * nodes / args.steps,
                 "d2h_bytes_per_step": 4 * 8 * nodes / args.steps},
