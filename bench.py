@@ -7,6 +7,7 @@ over the whole 256^3 block.  Each population array is 2.7 GB, far larger
 than the 126 MB L2, so consecutive timed steps cannot hit in L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --workload cavities [--gpus N]
     python bench.py --workload cavities-warmstart
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own cavity (no
@@ -62,9 +63,10 @@ def parse():
                    choices=["fp64", "fp32", "fp16"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="cavity3d",
-                   choices=["cavity3d", "cavities-warmstart"],
-                   help="cavities-warmstart: the batched-cavity learned warm "
-                        "start experiment (minutes; 1 GPU)")
+                   choices=["cavity3d", "cavities", "cavities-warmstart"],
+                   help="cavities: throughput of the 4,096 batched D2Q9 "
+                        "cavities split over the ranks; cavities-warmstart: "
+                        "the learned warm start experiment (minutes; 1 GPU)")
     p.add_argument("--epochs", type=int, default=60)
     return p.parse_args()
 
@@ -218,6 +220,58 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def run_cavities(args, rank, world, local):
+    """Throughput of the batched workload: the 4,096 D2Q9 FP32 cavities
+    (seed 20261203) split over the ranks by LPT on the node count, no
+    exchange between ranks (strong scaling: the set is fixed).  K steps of
+    every cavity after W warm-up steps, CUDA events on each batch's stream,
+    max over ranks."""
+    import torch
+    from mplb_b200.batch import Batch, cavity_set, shard
+    torch.cuda.set_device(local)
+    specs = cavity_set()
+    mine = [specs[i] for i in shard(specs, rank, world)]
+    b = Batch(mine, "fp32")
+    b.set_tuning(tile_nodes=128, persistent=0, chunk=50, ctas_per_sm=8)
+    b.init()
+    b.step(max(args.warmup, 50))
+    s0 = b.stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    b.step(args.steps)
+    barrier(world)
+    clk = clocks.stop()
+    s1 = b.stats()
+    ms = max_over_ranks(s1["device_ms"] - s0["device_ms"], world)
+    total_nodes = sum(s.n * s.n for s in specs)
+    value = total_nodes * args.steps / (ms * 1e-3) / 1e6
+    peak, peak_kind = measured_peaks()
+    launches = s1["launches"] - s0["launches"]
+    b.close()
+    if rank != 0:
+        return
+    per_gpu_ms = ms / args.steps
+    achieved = 72.0 * total_nodes / world / (per_gpu_ms * 1e-3) / 1e9
+    print(json.dumps({
+        "metric": "MLUPS (4,096 batched D2Q9 lid-driven cavities, FP32)",
+        "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 50),
+        "ms_per_step": per_gpu_ms, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 (shifted f - w)", "data": "synthetic",
+        "config": {"workload": "4,096 D2Q9 cavities, N in {64..256}, Re "
+                               "100-3200, U 0.02-0.08, seed 20261203",
+                   "nodes": total_nodes,
+                   "parallelism": f"cavities split over {world} GPU(s) "
+                                  "(LPT on nodes)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_node": 72,
+                     "traffic": None},
+        "clocks": clk, "gpu_launches": launches}))
+
+
 def run_warmstart(args, rank, local):
     """The second half of the metric: wall time to residual 1e-8 of the
     1,024 held-out cavities of the 4,096-cavity batched workload, warm-
@@ -256,7 +310,7 @@ def run_warmstart(args, rank, local):
 def main():
     args = parse()
     rank, world, local = dist_setup(args)
-    if args.impl == "reference" and args.workload == "cavities-warmstart":
+    if args.impl == "reference" and args.workload != "cavity3d":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable":
                               "the reference has no batched or learned "
@@ -268,6 +322,9 @@ def main():
         return
     if args.workload == "cavities-warmstart":
         run_warmstart(args, rank, local)
+        return
+    if args.workload == "cavities":
+        run_cavities(args, rank, world, local)
         return
     import numpy as np
     import torch

@@ -8,6 +8,9 @@ cavity by cavity in the order N, Re, U from a 64-bit Mersenne twister
 its raw 64-bit outputs r:  N = sizes[r mod 5],  Re = exp(ln 100 +
 (r / 2^64) ln 32),  U = 0.02 + 0.06 r / 2^64.
 
+``lpt_shards`` / ``shard`` partition the cavities over ranks (one GPU each;
+the cavities are independent, so there is no data-path exchange).
+
 ``Batch`` wraps one batch on the GPU; ``autotune`` times tile size, launch
 style (CUDA-graph chunks of one-step launches or a persistent multi-step
 launch), CTAs per SM and chunk length on the batch itself and caches the
@@ -96,6 +99,32 @@ def cavity_set(count: int = 4096, seed: int = 20261203,
         lid = lid_range[0] + (lid_range[1] - lid_range[0]) * g.next() / 2.0 ** 64
         out.append(CavitySpec(n, re, lid))
     return out
+
+
+def lpt_shards(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Longest-processing-time partition of items over `world` ranks: items
+    in decreasing cost (ties by index) each go to the least-loaded rank (ties
+    to the lowest rank).  Deterministic, so every rank computes the same
+    partition without communicating.  Returns each rank's item indices in
+    increasing order."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += costs[i]
+        out[r].append(i)
+    return [sorted(o) for o in out]
+
+
+def shard(specs: Sequence[CavitySpec], rank: int, world: int,
+          cost=lambda s: float(s.n * s.n)) -> List[int]:
+    """Indices of the cavities rank `rank` of `world` runs (LPT on `cost`,
+    by default the node count, i.e. the work of one step; weight by the
+    expected steps to convergence to balance a solve to the criterion)."""
+    if world <= 1:
+        return list(range(len(specs)))
+    return lpt_shards([cost(s) for s in specs], world)[rank]
 
 
 class BatchError(RuntimeError):
