@@ -43,9 +43,11 @@ BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
 # DRAM bytes per node update of the step kernel measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of SplitStepKernel<3,double>
 # on the 128^3 cavity, 2 launches: 615 MB / 2,097,152 nodes; FP32: 311 MB;
-# traffic grows with the node count, so a 256^3 launch moves this x
-# 16,777,216 bytes); profiles/splitstepkernel_cavity3d_d3q19_fp64.md and
-# _fp32.md have the commands.
+# captured with `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+# --clock-control none -k regex:SplitStepKernel -s 5 -c 2 python bench.py
+# --size 128 --steps 10 --warmup 3 --no-cpu-baseline --precision fp64`).
+# Traffic grows with the node count, so a 256^3 launch moves this x
+# 16,777,216 bytes.
 TRAFFIC_PER_NODE = {("fp64", 3): 293.0, ("fp32", 3): 148.0}
 METRIC = "MLUPS (D3Q19 3D lid-driven cavity 256^3)"
 DTYPES = {"fp64": "f64", "fp32": "f32 (shifted f - w)",

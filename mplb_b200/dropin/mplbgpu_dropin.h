@@ -1,7 +1,10 @@
 // Drop-in glue: MPLB's StreamCollision / UpdateMacroVars(3D) /
 // CalcResidualError on the B200 path.  Compiled into the reference's own
-// build (with its headers and OPS); see INTEGRATION.md for the three early
-// returns that route the reference's functions here.
+// build (with its headers and OPS) with -DMPLB_B200, together with three
+// early returns in the reference that route its functions here:
+// StreamCollision (Src/evolution.cpp) calls mplbgpu_dropin::StreamCollision,
+// and UpdateMacroVars(3D) (Src/model_wrapper.cpp) and CalcResidualError
+// (Src/flowfield_wrapper.cpp) call the glue's versions when Active().
 //
 // On the first StreamCollision the glue reads what the setup API holds
 // (g_Block() and each Block::Neighbors(), BlockBoundaries(), g_Components(),
