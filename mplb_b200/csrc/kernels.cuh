@@ -94,6 +94,20 @@ struct Rng;
 template <typename T>
 struct Prec;
 
+// Store/load cache policy of the population arrays (every value is written
+// once and read once per step, so neither wants to stay in the caches).
+#ifndef MPLB_STORE_HINT
+#define MPLB_STORE_HINT 0
+#endif
+template <typename V>
+__device__ __forceinline__ void PopStore(V* p, V v) {
+#if MPLB_STORE_HINT == 1
+    __stcs(p, v);
+#else
+    *p = v;
+#endif
+}
+
 template <>
 struct Prec<double> {
     using C = double;
@@ -104,7 +118,7 @@ struct Prec<double> {
     }
     __device__ static __forceinline__ void Store(double* p, long long k, int,
                                                  C v, const PhysConst&, Rng&) {
-        p[k] = v;
+        PopStore(p + k, v);
     }
 };
 
@@ -118,7 +132,7 @@ struct Prec<float> {
     }
     __device__ static __forceinline__ void Store(float* p, long long k, int,
                                                  C v, const PhysConst&, Rng&) {
-        p[k] = v;
+        PopStore(p + k, v);
     }
 };
 
@@ -174,7 +188,7 @@ struct Prec<__half> {
     __device__ static __forceinline__ void Store(__half* p, long long k, int i,
                                                  C v, const PhysConst& pc,
                                                  Rng& rng) {
-        p[k] = StochasticHalf(v * pc.winvf[i], SrDraw(rng, i));
+        PopStore(p + k, StochasticHalf(v * pc.winvf[i], SrDraw(rng, i)));
     }
 };
 

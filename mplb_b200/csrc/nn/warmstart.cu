@@ -305,19 +305,55 @@ struct CavMeta {
     double rho_scale, u_scale;
 };
 
-__device__ __forceinline__ double Bilinear(const double* __restrict__ f,
-                                           int n, double xs, double ys) {
-    // xs, ys in node units (node i at i); clamped to the node range
-    xs = fmin(fmax(xs, 0.0), (double)(n - 1));
-    ys = fmin(fmax(ys, 0.0), (double)(n - 1));
-    const int i0 = min((int)xs, n - 2 < 0 ? 0 : n - 2);
-    const int j0 = min((int)ys, n - 2 < 0 ? 0 : n - 2);
+// Catmull-Rom (bicubic) sample of a cell-centred n x n field on the unit
+// square (node i at i, walls at -1/2 and n - 1/2) at (xs, ys) in node units.
+// The stencil reaches beyond the walls through ghost nodes mirrored across
+// them (node -1-k <-> k): with `walls`, as 2 w - f for the velocity (the
+// moving lid at y = n - 1/2 has `top`, the other walls 0); without, as f
+// (the density, which has no wall value).  On converged cavities the
+// 128 <-> N round trip of u is 0.4-0.8 % this way, against 1.1-2.9 % for
+// bilinear with the same ghosts and 1.5-3.5 % for bilinear held at the edge
+// node.
+template <typename Get>
+__device__ __forceinline__ double SampleCavity(Get get, int n, double xs,
+                                               double ys, bool walls,
+                                               double top) {
+    xs = fmin(fmax(xs, -0.5), n - 0.5);
+    ys = fmin(fmax(ys, -0.5), n - 0.5);
+    const int i0 = (int)floor(xs), j0 = (int)floor(ys);
     const double fx = xs - i0, fy = ys - j0;
-    const int i1 = min(i0 + 1, n - 1), j1 = min(j0 + 1, n - 1);
-    return (1 - fy) * ((1 - fx) * f[(long long)j0 * n + i0] +
-                       fx * f[(long long)j0 * n + i1]) +
-           fy * ((1 - fx) * f[(long long)j1 * n + i0] +
-                 fx * f[(long long)j1 * n + i1]);
+    auto mirror = [n](int i) {
+        int m = i < 0 ? -1 - i : (i > n - 1 ? 2 * n - 1 - i : i);
+        return min(max(m, 0), n - 1);
+    };
+    auto val = [&](int i, int j) {
+        double v = get((long long)mirror(j) * n + mirror(i));
+        if (walls) {
+            if (i < 0 || i > n - 1) v = -v;
+            if (j < 0) v = -v;
+            if (j > n - 1) v = 2.0 * top - v;
+        }
+        return v;
+    };
+    auto weights = [](double t, double* w) {
+        const double t2 = t * t, t3 = t2 * t;
+        w[0] = 0.5 * (-t3 + 2.0 * t2 - t);
+        w[1] = 0.5 * (3.0 * t3 - 5.0 * t2 + 2.0);
+        w[2] = 0.5 * (-3.0 * t3 + 4.0 * t2 + t);
+        w[3] = 0.5 * (t3 - t2);
+    };
+    double wx[4], wy[4];
+    weights(fx, wx);
+    weights(fy, wy);
+    double out = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        double row = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) row += wx[c] * val(i0 - 1 + c, j0 - 1 + a);
+        out += wy[a] * row;
+    }
+    return out;
 }
 
 __global__ void FieldsToGridKernel(const double* __restrict__ rho,
@@ -333,24 +369,22 @@ __global__ void FieldsToGridKernel(const double* __restrict__ rho,
     const CavMeta m = meta[k];
     const double xs = (gx + 0.5) / kGrid * m.n - 0.5;
     const double ys = (gy + 0.5) / kGrid * m.n - 0.5;
-    grid[t * 3] = (float)((Bilinear(rho + m.off, m.n, xs, ys) - 1.0) /
+    const double* fr = rho + m.off;
+    const double* fu = u + m.off;
+    const double* fv = v + m.off;
+    grid[t * 3] = (float)((SampleCavity([&](long long q) { return fr[q]; },
+                                        m.n, xs, ys, false, 0.0) - 1.0) /
                           m.rho_scale);
-    grid[t * 3 + 1] = (float)(Bilinear(u + m.off, m.n, xs, ys) / m.u_scale);
-    grid[t * 3 + 2] = (float)(Bilinear(v + m.off, m.n, xs, ys) / m.u_scale);
-}
-
-__device__ __forceinline__ float BilinearGrid(const float* __restrict__ g,
-                                              int ch, double xs, double ys) {
-    xs = fmin(fmax(xs, 0.0), (double)(kGrid - 1));
-    ys = fmin(fmax(ys, 0.0), (double)(kGrid - 1));
-    const int i0 = min((int)xs, kGrid - 2), j0 = min((int)ys, kGrid - 2);
-    const double fx = xs - i0, fy = ys - j0;
-    auto at = [&](int j, int i) { return (double)g[(j * kGrid + i) * 3 + ch]; };
-    return (float)((1 - fy) * ((1 - fx) * at(j0, i0) + fx * at(j0, i0 + 1)) +
-                   fy * ((1 - fx) * at(j0 + 1, i0) + fx * at(j0 + 1, i0 + 1)));
+    grid[t * 3 + 1] = (float)(SampleCavity([&](long long q) { return fu[q]; },
+                                           m.n, xs, ys, true, m.u_scale) /
+                              m.u_scale);
+    grid[t * 3 + 2] = (float)(SampleCavity([&](long long q) { return fv[q]; },
+                                           m.n, xs, ys, true, 0.0) /
+                              m.u_scale);
 }
 
 // One thread per cavity node; cavity found by binary search of offsets.
+// The grid holds normalised fields: the lid's u is 1 there.
 __global__ void GridToFieldsKernel(const float* __restrict__ grid,
                                    const CavMeta* __restrict__ meta, int ncav,
                                    long long total, double* __restrict__ rho,
@@ -370,9 +404,15 @@ __global__ void GridToFieldsKernel(const float* __restrict__ grid,
     const double xs = (x + 0.5) / m.n * kGrid - 0.5;
     const double ys = (y + 0.5) / m.n * kGrid - 0.5;
     const float* g = grid + (long long)lo * kGrid * kGrid * 3;
-    rho[t] = 1.0 + m.rho_scale * BilinearGrid(g, 0, xs, ys);
-    u[t] = m.u_scale * BilinearGrid(g, 1, xs, ys);
-    v[t] = m.u_scale * BilinearGrid(g, 2, xs, ys);
+    rho[t] = 1.0 + m.rho_scale *
+                       SampleCavity([&](long long q) { return (double)g[q * 3]; },
+                                    kGrid, xs, ys, false, 0.0);
+    u[t] = m.u_scale *
+           SampleCavity([&](long long q) { return (double)g[q * 3 + 1]; }, kGrid,
+                        xs, ys, true, 1.0);
+    v[t] = m.u_scale *
+           SampleCavity([&](long long q) { return (double)g[q * 3 + 2]; }, kGrid,
+                        xs, ys, true, 0.0);
 }
 
 unsigned Blocks(long long n) { return (unsigned)((n + kEw - 1) / kEw); }

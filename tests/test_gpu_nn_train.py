@@ -87,12 +87,14 @@ def test_resampling_round_trip(gpu_lib, torch_mod):
              bmod.CavitySpec(256, 1000.0, 0.08)]
     rs, us = ws.scales(specs)
     fields = [[], [], []]
+    # cavity-like fields: u = lid speed at the top wall and 0 on the others
+    # (except at the top corners), v = 0 on every wall, rho free
     for s, r_, u_ in zip(specs, rs, us):
         c = (np.arange(s.n) + 0.5) / s.n
         X, Y = np.meshgrid(c, c)
         fields[0].append(1.0 + r_ * np.cos(np.pi * X) * np.cos(np.pi * Y))
-        fields[1].append(u_ * np.sin(np.pi * X) * Y * Y)
-        fields[2].append(-u_ * np.sin(np.pi * Y) * X)
+        fields[1].append(u_ * Y * Y * (1.0 - (2.0 * X - 1.0) ** 8))
+        fields[2].append(-u_ * np.sin(np.pi * Y) * np.sin(np.pi * X) * X)
     dev = [torch.from_numpy(np.concatenate([f.reshape(-1) for f in fl])).cuda()
            for fl in fields]
     net = ws.Network(1)
@@ -105,11 +107,14 @@ def test_resampling_round_trip(gpu_lib, torch_mod):
         b = dev[k][:n0].cpu().numpy()
         scale = rs[0] if k == 0 else us[0]
         assert np.abs(a - b).max() <= 1e-6 * scale
-    # other sides: bilinear there and back, smooth fields
-    for k in range(3):
+    # other sides: bicubic there and back.  rho and v are smooth and meet
+    # their wall conditions; this u reaches 0 at the top corners where the
+    # resampling assumes the lid speed along the whole top wall (a real
+    # cavity's discontinuity), hence its looser bound.
+    for k, tol in ((0, 1e-4), (1, 2e-2), (2, 1e-4)):
         err = ws.rel_l2_per_cavity(specs, back[k] - (1.0 if k == 0 else 0.0),
                                    dev[k] - (1.0 if k == 0 else 0.0))
-        assert err.max() < 2e-3, (k, err)
+        assert err.max() < tol, (k, err)
 
 
 def test_warm_start_beats_cold_start(gpu_lib, torch_mod):
