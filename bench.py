@@ -69,7 +69,7 @@ def parse():
                    help="cavities: throughput of the 4,096 batched D2Q9 "
                         "cavities split over the ranks; cavities-warmstart: "
                         "the learned warm start experiment (minutes; 1 GPU)")
-    p.add_argument("--epochs", type=int, default=60)
+    p.add_argument("--epochs", type=int, default=200)
     return p.parse_args()
 
 

@@ -668,23 +668,27 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                               z);
 }
 
-// Two interior nodes of the same x in consecutive interior rows: both
-// nodes' loads are issued before either is computed, so a warp keeps 38
-// loads in flight instead of 19 (the FP32 and FP16 forms move too few bytes
-// per load to cover HBM latency with one node per thread).
+// Two interior nodes per thread, 32 apart along x: both nodes' loads are
+// issued before either is computed, so a warp keeps 38 loads in flight
+// instead of 19, and each population access of the warp covers 256
+// contiguous bytes as in the FP64 form (the FP32 and FP16 forms otherwise
+// move 128 or 64 bytes per access).
 template <int D, typename T, bool O32>
 __device__ __forceinline__ void PureNodePair(const BlockDev& b,
                                              const PhysConst& pc,
                                              const T* __restrict__ src,
-                                             T* __restrict__ dst, int x,
-                                             int ya, int za, int yb, int zb,
-                                             bool second) {
+                                             T* __restrict__ dst, int xa,
+                                             int ya, int za, int xb, int yb,
+                                             int zb, bool first, bool second) {
     using L = Lattice<D>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const long long na = NodeIndex<D>(b, x, ya, za);
-    const long long nb = second ? NodeIndex<D>(b, x, yb, zb) : na;
+    const long long na0 = NodeIndex<D>(b, xa, ya, za);
+    const long long nb0 = NodeIndex<D>(b, xb, yb, zb);
+    // an invalid node loads from (and is not stored to) the valid one
+    const long long na = first ? na0 : nb0;
+    const long long nb = second ? nb0 : na0;
     C fa[Q], fb[Q];
     if constexpr (O32) {
         const T* pa = src + na;
@@ -702,6 +706,7 @@ __device__ __forceinline__ void PureNodePair(const BlockDev& b,
         }
     }
     const bool fl = b.center_fluid != 0;
+    if (first) {
     MomentsCollideT<L, T>(fa, pc, fl);
     Rng ra = SeedRng(pc.seed, na);
     if constexpr (O32) {
@@ -712,6 +717,7 @@ __device__ __forceinline__ void PureNodePair(const BlockDev& b,
 #pragma unroll
         for (int i = 0; i < Q; i++)
             P::Store(dst, OwnIndex(b, na, i), i, fa[i], pc, ra);
+    }
     }
     if (!second) return;
     MomentsCollideT<L, T>(fb, pc, fl);
@@ -728,9 +734,10 @@ __device__ __forceinline__ void PureNodePair(const BlockDev& b,
 }
 
 // Rows of interior nodes handled per x-face block of SplitStepKernel, and
-// interior rows per thread (two for the low-precision forms; the FP64 form
+// interior nodes per thread (two for the low-precision forms; the FP64 form
 // moves enough bytes per load and has no registers for a second node).
 constexpr int kSplitRows = 64;
+constexpr int kSplitCta = 128;   // threads per CTA of SplitStepKernel
 template <typename T>
 __host__ __device__ constexpr int SplitPair() { return sizeof(T) < 8 ? 2 : 1; }
 
@@ -741,8 +748,9 @@ __host__ __device__ constexpr int SplitPair() { return sizeof(T) < 8 ? 2 : 1; }
 //   1. shell rows: every row with y or z on the block boundary (coalesced);
 //   2. per chunk of 64 interior rows, one CTA for their x = 0 and x = n0 - 1
 //      nodes, followed by
-//   3. the CTAs of those rows' interior nodes, two rows per CTA (each
-//      thread one node of each; PureNodePair).  A row's CTAs start on the
+//   3. the CTAs of those rows' interior nodes: 256 nodes of a row per CTA
+//      for FP32 / FP16 (two per thread, 32 apart; PureNodePair), 128 for
+//      FP64 (one per thread).  A row's CTAs start on the
 //      row's first node so every store begins on the row's 32-byte boundary
 //      (the two x-face lanes idle); the x-face CTA runs next to them, so the
 //      sectors they share meet in L2 instead of costing a read-modify-write
@@ -778,7 +786,9 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     blk -= nsr;
     const long long rows = (long long)ny * (D == 3 ? b.n[2] - 2 : 1);
     constexpr int pair = SplitPair<T>();
-    const long long per_chunk = 1 + (long long)(kSplitRows / pair) * nbx;
+    const int nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
+    const long long per_chunk =
+        1 + (long long)kSplitRows * (pair == 2 ? nbx2 : nbx);
     const long long chunk = blk / per_chunk;
     const int w = (int)(blk % per_chunk);
     if (w == 0) {
@@ -791,16 +801,30 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                        D == 3 ? 1 + (int)(r / ny) : 0);
         return;
     }
-    // interior CTAs: rows r (and r + 1 when paired)
-    const long long r = chunk * kSplitRows + pair * ((w - 1) / nbx);
-    const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
-    if (r >= rows || x < 1 || x > b.n[0] - 2) return;
-    const long long r1 = r + 1;
-    PureNodePair<D, T, O32>(b, pc, src, dst, x, 1 + (int)(r % ny),
-                            D == 3 ? 1 + (int)(r / ny) : 0,
-                            1 + (int)(r1 % ny),
-                            D == 3 ? 1 + (int)(r1 / ny) : 0,
-                            pair == 2 && r1 < rows);
+    if constexpr (pair == 2) {
+        // interior CTAs: 256 nodes of one row; warp w has [64 w, 64 w + 64),
+        // lane l the nodes 64 w + l and 64 w + 32 + l, so each of the
+        // warp's population accesses covers 256 contiguous bytes
+        const long long r = chunk * kSplitRows + (w - 1) / nbx2;
+        const int xa = ((w - 1) % nbx2) * 2 * kSplitCta +
+                       (threadIdx.x >> 5) * 64 + (threadIdx.x & 31);
+        const int xb = xa + 32;
+        const bool va = xa >= 1 && xa <= b.n[0] - 2;
+        const bool vb = xb >= 1 && xb <= b.n[0] - 2;
+        if (r >= rows || (!va && !vb)) return;
+        const int y = 1 + (int)(r % ny);
+        const int z = D == 3 ? 1 + (int)(r / ny) : 0;
+        PureNodePair<D, T, O32>(b, pc, src, dst, xa, y, z, xb, y, z, va, vb);
+    } else {
+        // interior CTAs: 128 nodes of one row
+        const long long r = chunk * kSplitRows + (w - 1) / nbx;
+        const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
+        if (r >= rows || x < 1 || x > b.n[0] - 2) return;
+        const int y = 1 + (int)(r % ny);
+        const int z = D == 3 ? 1 + (int)(r / ny) : 0;
+        PureNodePair<D, T, O32>(b, pc, src, dst, x, y, z, x, y, z, true,
+                                false);
+    }
 }
 
 // Deferred nodes: thread t -> (region, node).

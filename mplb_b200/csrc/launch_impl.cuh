@@ -6,6 +6,8 @@
 
 namespace mplb {
 
+static_assert(kSplitCta == kStepThreads, "SplitStepKernel CTA size");
+
 template <int D, typename T>
 cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const BlockDev& b, const PhysConst& pc,
@@ -18,8 +20,9 @@ cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
         const long long rows = ny * (D == 3 ? b.n[2] - 2 : 1);
         const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
         const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
+        const long long nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
         const long long blocks =
-            nsr + chunks * (1 + (kSplitRows / SplitPair<T>()) * nbx);
+            nsr + chunks * (1 + kSplitRows * (SplitPair<T>() == 2 ? nbx2 : nbx));
         if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
         if (b.off32)
             SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(

@@ -302,7 +302,7 @@ def rel_l2_per_cavity(specs, a, b):
 
 
 def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
-             check_period=1000, criterion=1e-8, epochs=60, batch=32,
+             check_period=1000, criterion=1e-8, epochs=200, batch=32,
              log=print, tuning=None, lr_max=2e-3, details=None, **cavity_kw):
     """The warm-start experiment; cavity_kw goes to cavity_set (sizes,
     re_range, lid_range).  Returns (summary dict, trained network); per-
@@ -414,7 +414,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--quick", action="store_true",
                     help="256 cavities of side 64/96, 20 epochs")
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--max-steps", type=int, default=2_000_000)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=None)
