@@ -82,8 +82,11 @@ struct BlockDev {
     // region PURE); center_fluid: the interior is fluid-like
     int split;
     int center_fluid;
-    // per region: class (bits 0-1) and fluid-like flag (bit 2)
+    // per region: class (bits 0-1) and fluid-like flag (bit 2); the pulled
+    // and the stale populations (copies of RegionInfo::pull / ::stale)
     uint8_t rflags[kNumRegions];
+    uint32_t rpull[kNumRegions];
+    uint32_t rstale[kNumRegions];
 };
 
 enum StepMode : int { kModeStep = 0, kModeMacro = 1, kModeF = 2 };
@@ -597,21 +600,29 @@ __device__ __forceinline__ void StepNode(const BlockDev& b,
                 f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
         }
     } else {
-        const RegionInfo& R = b.regions[r];
-        const uint32_t pull = R.pull;
-        const uint32_t stale = R.stale;
-        const double* st =
-            b.stale + (R.side_base >= 0
-                           ? (R.side_base + LocalIndex(R, x, y, z)) * Q
-                           : 0);
+        // pull and stale masks from the kernel parameters, so the population
+        // loads do not wait for the region record
+        const uint32_t pull = b.rpull[r];
+        const uint32_t stale = b.rstale[r];
+        const T* ps = src + node;
 #pragma unroll
         for (int i = 0; i < Q; i++) {
-            if (pull >> i & 1u)
-                f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
-            else if (stale >> i & 1u)
-                f[i] = (C)st[i];
-            else
+            if (pull >> i & 1u) {
+                if constexpr (O32) f[i] = P::Load(ps, b.pull_off32[i], i, pc);
+                else f[i] = P::Load(src, PullIndex<L>(b, node, i), i, pc);
+            } else {
                 f[i] = (C)0;
+            }
+        }
+        const RegionInfo& R = b.regions[r];
+        if (stale) {
+            const double* st =
+                b.stale + (R.side_base >= 0
+                               ? (R.side_base + LocalIndex(R, x, y, z)) * Q
+                               : 0);
+#pragma unroll
+            for (int i = 0; i < Q; i++)
+                if (stale >> i & 1u) f[i] = (C)st[i];
         }
         for (int k = 0; k < R.nops; k++) {
             const RegionOp& op = b.ops[R.op[k]];

@@ -447,6 +447,8 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             const RegionInfo& R = B.region[r];
             d.rflags[r] = (uint8_t)((R.cls < 0 ? kPure : R.cls) |
                                     (R.fluidlike ? 4 : 0));
+            d.rpull[r] = R.pull;
+            d.rstale[r] = R.stale;
         }
         const int center = 13;   // interior on every axis (RegionOf)
         d.split = (B.n[0] >= 3 && B.n[1] >= 3 && (P.dim == 2 || B.n[2] >= 3) &&
