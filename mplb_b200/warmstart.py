@@ -303,10 +303,14 @@ def rel_l2_per_cavity(specs, a, b):
 
 def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
              check_period=1000, criterion=1e-8, epochs=200, batch=32,
-             log=print, tuning=None, lr_max=2e-3, details=None, **cavity_kw):
+             log=print, tuning=None, lr_max=2e-3, details=None,
+             reference_check=True, **cavity_kw):
     """The warm-start experiment; cavity_kw goes to cavity_set (sizes,
     re_range, lid_range).  Returns (summary dict, trained network); per-
-    cavity arrays of the held-out set are added to `details` if given."""
+    cavity arrays of the held-out set are added to `details` if given.
+    With reference_check the held-out set is also run to a 1000x tighter
+    residual, and the cold- and warm-converged fields are compared with that
+    reference (the same steady-state error on both sides)."""
     torch = _torch()
     specs = cavity_set(count, seed, **cavity_kw)
     train_specs, held = specs[:n_train], specs[n_train:]
@@ -347,6 +351,29 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
     init_err = rel_l2_per_cavity(held, fields[1], cold[1])
     final_diff = rel_l2_per_cavity(held, warm[1], cold[1])
     both = cconv & wconv
+    ref_err = {}
+    if reference_check:
+        # the steady state to a 1000x tighter residual, restarted from the
+        # warm-converged fields: the error of each converged field against it
+        rsteps, rres, rconv, rwall = solve(hb, max_steps, check_period,
+                                           criterion * 1e-3, warm)
+        ref = device_macro(hb)
+        err_cold = rel_l2_per_cavity(held, cold[1], ref[1])
+        err_warm = rel_l2_per_cavity(held, warm[1], ref[1])
+        sel = both & rconv
+        ref_err = {
+            "reference_criterion": criterion * 1e-3,
+            "reference_converged": int(rconv.sum()),
+            "cold_u_error_vs_reference_median": float(np.median(err_cold[sel])),
+            "warm_u_error_vs_reference_median": float(np.median(err_warm[sel])),
+            "cold_u_error_vs_reference_p90": float(np.quantile(err_cold[sel], 0.9)),
+            "warm_u_error_vs_reference_p90": float(np.quantile(err_warm[sel], 0.9)),
+            "warm_error_le_cold_fraction": float(np.mean(err_warm[sel] <= err_cold[sel])),
+        }
+        if details is not None:
+            details.update({"cold_u_error_vs_reference": err_cold.tolist(),
+                            "warm_u_error_vs_reference": err_warm.tolist(),
+                            "reference_conv": rconv.tolist()})
     res.update({
         "cold_wall_s": cwall, "warm_wall_s": wwall + infer_s,
         "warm_infer_s": infer_s, "speedup_wall": cwall / (wwall + infer_s),
@@ -367,6 +394,7 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
         if both.any() else None,
         "total_s": time.perf_counter() - t0,
     })
+    res.update(ref_err)
     if details is not None:
         details.update({
             "n": [s.n for s in held], "re": [s.re for s in held],

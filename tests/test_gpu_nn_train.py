@@ -124,8 +124,13 @@ def test_warm_start_beats_cold_start(gpu_lib, torch_mod):
     and converge to the same field."""
     res, _ = ws.pipeline(count=112, seed=77, n_train=96, sizes=(64,),
                          re_range=(100.0, 400.0), max_steps=400_000,
-                         epochs=150, batch=16, log=lambda m: None)
+                         epochs=150, batch=16, log=lambda m: None,
+                         reference_check=True)
     assert res["train_converged"] == 96
     assert res["cold_converged"] == res["warm_converged"] == 16
     assert res["warm_node_steps"] < 0.8 * res["cold_node_steps"], res
     assert res["final_u_difference_median"] < 5e-3, res
+    # both converged fields are as close to the tightly converged steady
+    # state as each other
+    assert res["warm_u_error_vs_reference_median"] <= \
+        2.0 * res["cold_u_error_vs_reference_median"] + 1e-6, res
