@@ -308,9 +308,9 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
     """The warm-start experiment; cavity_kw goes to cavity_set (sizes,
     re_range, lid_range).  Returns (summary dict, trained network); per-
     cavity arrays of the held-out set are added to `details` if given.
-    With reference_check the held-out set is also run to a 1000x tighter
-    residual, and the cold- and warm-converged fields are compared with that
-    reference (the same steady-state error on both sides)."""
+    With reference_check the held-out set is also run in FP64 to a 1000x
+    tighter residual, and the cold- and warm-converged fields are compared
+    with that reference (the same steady-state error on both sides)."""
     torch = _torch()
     specs = cavity_set(count, seed, **cavity_kw)
     train_specs, held = specs[:n_train], specs[n_train:]
@@ -353,17 +353,21 @@ def pipeline(count=4096, seed=20261203, n_train=3072, max_steps=2_000_000,
     both = cconv & wconv
     ref_err = {}
     if reference_check:
-        # the steady state to a 1000x tighter residual, restarted from the
+        # the steady state to a 1000x tighter residual in FP64 (an FP32 run
+        # may stall on its rounding noise above that), restarted from the
         # warm-converged fields: the error of each converged field against it
-        rsteps, rres, rconv, rwall = solve(hb, max_steps, check_period,
+        rb = Batch(held, "fp64")
+        rsteps, rres, rconv, rwall = solve(rb, max_steps, check_period,
                                            criterion * 1e-3, warm)
-        ref = device_macro(hb)
+        ref = device_macro(rb)
+        rb.close()
         err_cold = rel_l2_per_cavity(held, cold[1], ref[1])
         err_warm = rel_l2_per_cavity(held, warm[1], ref[1])
         sel = both & rconv
         ref_err = {
             "reference_criterion": criterion * 1e-3,
             "reference_converged": int(rconv.sum()),
+            "reference_wall_s": rwall,
             "cold_u_error_vs_reference_median": float(np.median(err_cold[sel])),
             "warm_u_error_vs_reference_median": float(np.median(err_warm[sel])),
             "cold_u_error_vs_reference_p90": float(np.quantile(err_cold[sel], 0.9)),
