@@ -70,12 +70,20 @@ def parse():
                         "cavities split over the ranks; cavities-warmstart: "
                         "the learned warm start experiment (minutes; 1 GPU)")
     p.add_argument("--epochs", type=int, default=200)
+    p.add_argument("--scheme", default="stream", choices=["stream", "swap"],
+                   help="swap: the reference's one-array swap step "
+                        "(Scheme_StreamCollision_Swap), half the memory")
     return p.parse_args()
 
 
-def workload(n, precision="fp64"):
+SCHEMES = {"stream": "Scheme_StreamCollision",
+           "swap": "Scheme_StreamCollision_Swap"}
+
+
+def workload(n, precision="fp64", scheme="stream"):
     from mplb_b200 import config
-    case = config.cavity(3, n, 0.05, re=400, precision=precision)
+    case = config.cavity(3, n, 0.05, re=400, precision=precision,
+                         scheme=SCHEMES[scheme])
     return case
 
 
@@ -191,7 +199,9 @@ def max_over_ranks(v, world):
 
 
 def run_reference_arm(args, rank, world):
-    case = workload(args.size)
+    case = workload(args.size, "fp64", args.scheme)
+    swap = args.scheme == "swap"
+    step_name = "SwapStreamCollision" if swap else "StreamCollision"
     if rank != 0:
         return
     res = cpu_reference(case, max(1, min(args.warmup, 1)), args.steps,
@@ -202,17 +212,20 @@ def run_reference_arm(args, rank, world):
         return
     mlups, n, threads, secs = res
     line = {
-        "impl": "reference", "metric": METRIC, "value": mlups,
+        "impl": "reference",
+        "metric": METRIC if not swap else METRIC[:-1] +
+        ", one-array swap scheme)", "value": mlups,
         "unit": "MLUPS", "n_gpus": args.gpus, "steps": n,
         "warmup": 1, "ms_per_step": secs / n * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
-                               "FP64, lid 0.05, Re 400",
+                               "FP64, lid 0.05, Re 400" +
+                               (", swap scheme (one array)" if swap else ""),
                    "nodes": case.nodes()},
         "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads,
                          "kind": "reference",
-                         "sample": f"{n} StreamCollision steps of the "
+                         "sample": f"{n} {step_name} steps of the "
                                    f"{args.size}^3 cavity after 1 warm-up "
                                    "step (reference sources + sequential "
                                    "OPS stand-in, OpenMP)"},
@@ -332,10 +345,11 @@ def main():
     import torch
     from mplb_b200 import Solver, abi
     torch.cuda.set_device(local)
-    case = workload(args.size, args.precision)
+    case = workload(args.size, args.precision, args.scheme)
     nodes = case.nodes()
     nx, ny, nz = case.size3(0)
     lib = abi.load_library()
+    swap = args.scheme == "swap"
 
     # --- device-resident timing ------------------------------------------
     s = Solver(case, lib)
@@ -400,19 +414,25 @@ def main():
             mlups, n, threads, secs = res
             cpu = {"value": mlups, "unit": "MLUPS", "cores": threads,
                    "kind": "reference",
-                   "sample": f"{n} StreamCollision steps of the same "
+                   "sample": f"{n} {'SwapStreamCollision' if swap else 'StreamCollision'} "
+                             f"steps of the same "
                              f"{args.size}^3 cavity after 1 warm-up step "
                              "(reference sources + sequential OPS stand-in, "
                              "OpenMP)"}
+    metric = METRIC if not swap else METRIC[:-1] + ", one-array swap scheme)"
+    traffic = (TRAFFIC_PER_NODE[(case.precision, 3)] * nodes
+               if (case.precision, 3) in TRAFFIC_PER_NODE and not swap
+               else None)
     line = {
-        "metric": METRIC, "value": value, "unit": "MLUPS",
+        "metric": metric, "value": value, "unit": "MLUPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": DTYPES[args.precision], "data": "synthetic",
         "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
                                f"{args.precision.upper()}, lid 0.05 "
-                               "(lattice), Re 400",
+                               "(lattice), Re 400" +
+                               (", swap scheme (one array)" if swap else ""),
                    "nodes_per_gpu": nodes, "parallelism": f"replicas{world}",
                    "l2": "population arrays of 0.7-2.7 GB each, larger "
                          "than L2"},
@@ -420,9 +440,7 @@ def main():
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
                      "bytes_per_node": bpn,
-                     "traffic": (TRAFFIC_PER_NODE[(case.precision, 3)] * nodes
-                                 if (case.precision, 3) in TRAFFIC_PER_NODE
-                                 else None)},
+                     "traffic": traffic},
         "e2e": {"value": e2e, "unit": "MLUPS",
                 "h2d_bytes_per_step": 4 * 8 * nodes / args.steps,
                 "d2h_bytes_per_step": 4 * 8 * nodes / args.steps},

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MPLBGPU_ABI_VERSION 1
+#define MPLBGPU_ABI_VERSION 2
 
 typedef int mplbgpu_status;
 enum {
@@ -99,6 +99,16 @@ enum {
 /* BodyForceType, Src/model.h:101-106 */
 enum { MPLBGPU_FORCE_NONE = 0, MPLBGPU_FORCE_1ST = 1 };
 
+/* SchemeType, Src/scheme.h:67-72.  The swap scheme stands for the
+ * reference's one-array trio Scheme_StreamCollision_Swap +
+ * Collision_BGKIsothermal2nd_Swap + BodyForce_{None,1st}_Swap
+ * (SwapStreamCollision, Src/evolution.cpp:195-252): D3Q19, one block
+ * without connections, every block-boundary node under EQMDiffuseRefl. */
+enum {
+    MPLBGPU_SCHEME_STREAM_COLLISION = 10,      /* 0 means the same */
+    MPLBGPU_SCHEME_STREAM_COLLISION_SWAP = 11
+};
+
 typedef struct {
     int id;       /* block id as given to DefineBlocks */
     int size[3];  /* nodes per axis; size[2] = 1 for 2D */
@@ -139,6 +149,7 @@ typedef struct {
     double accel[3];  /* uniform body acceleration (MPLB units) */
     int force_velocity; /* 1 when the velocity moments are Variable_U_Force
                            etc.: u += dt*a/2 at Fluid/MDPeriodic nodes */
+    int scheme;       /* SchemeType (DefineScheme, Src/scheme.cpp:92-110) */
 } mplbgpu_desc;
 
 typedef struct mplbgpu_ctx mplbgpu_ctx;

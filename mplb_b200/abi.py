@@ -7,7 +7,7 @@ missing or unloadable library raises ``NativeLibraryError``.
 import ctypes
 import os
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERR_INVALID = 1
@@ -54,6 +54,11 @@ FP16_SHIFTED = 2
 PRECISIONS = {"fp64": FP64, "fp32": FP32_SHIFTED, "fp16": FP16_SHIFTED}
 FORCE_NONE = 0
 FORCE_1ST = 1
+# SchemeType (Src/scheme.h:67-72)
+SCHEME_STREAM_COLLISION = 10
+SCHEME_STREAM_COLLISION_SWAP = 11
+SCHEMES = {"Scheme_StreamCollision": SCHEME_STREAM_COLLISION,
+           "Scheme_StreamCollision_Swap": SCHEME_STREAM_COLLISION_SWAP}
 
 
 class Block(ctypes.Structure):
@@ -84,6 +89,7 @@ class Desc(ctypes.Structure):
         ("tau_ref", ctypes.c_double), ("dt", ctypes.c_double),
         ("cs", ctypes.c_double), ("body_force", ctypes.c_int),
         ("accel", ctypes.c_double * 3), ("force_velocity", ctypes.c_int),
+        ("scheme", ctypes.c_int),
     ]
 
 

@@ -24,7 +24,7 @@ UNITS = [("mplbgpu.cu", ["-fmad=false"]), ("kernels_f64.cu", ["-fmad=false"]),
 SOURCES = [os.path.join(CSRC, u) for u, _ in UNITS]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "lattice.h",
                                             "plan.h", "launch.h",
-                                            "launch_impl.cuh",
+                                            "launch_impl.cuh", "swap.cuh",
                                             "batch_kernels.cuh",
                                             "nn/umma.cuh", "nn/conv.cuh",
                                             "nn/conv_host.h")] + [

@@ -70,6 +70,11 @@ class CaseConfig:
     convergence: float = 1e-8
     steps: int = 0
     precision: str = "fp64"
+    scheme: str = "Scheme_StreamCollision"
+
+    @property
+    def swap(self) -> bool:
+        return self.scheme == "Scheme_StreamCollision_Swap"
 
     @property
     def lattice(self) -> int:
@@ -101,6 +106,9 @@ class CaseConfig:
         if self.force_velocity:
             mv = [mv[0]] + [m + "_Force" for m in mv[1:]]
         names = ["rho", "u", "v", "w"][:d + 1]
+        # the swap scheme runs with the _Swap collision and body-force types
+        # (Apps/3DCavity-Swap/lbm3d_cavity_swap.cpp:72-106)
+        sfx = "_Swap" if self.swap else ""
         out = {
             "CaseName": self.case_name,
             "SpaceDim": d,
@@ -118,13 +126,13 @@ class CaseConfig:
             "MacroVarIds": list(range(d + 1)),
             "MacroCompoIds": [0] * (d + 1),
             "MacroVarTypes": mv,
-            "CollisionType": ["Collision_BGKIsothermal2nd"],
+            "CollisionType": ["Collision_BGKIsothermal2nd" + sfx],
             "CollisionCompoIds": [0],
             "InitialType": ["Initial_BGKFeq2nd"],
             "InitialCompoIds": [0],
-            "BodyForceType": [self.body_force],
+            "BodyForceType": [self.body_force + sfx],
             "BodyForceCompoId": [0],
-            "SchemeType": "Scheme_StreamCollision",
+            "SchemeType": self.scheme,
             "CurrentTimeStep": 0,
             "CheckPeriod": self.check_period,
             "ConvergenceCriteria": self.convergence,
@@ -173,9 +181,19 @@ class CaseConfig:
         latt = js["LatticeName"][0]
         if (d, latt) not in ((2, "d2q9"), (3, "d3q19")):
             raise ValueError(f"lattice {latt} in {d}D is not supported")
+        scheme = js.get("SchemeType", "Scheme_StreamCollision")
+        if scheme not in abi.SCHEMES:
+            raise ValueError(f"scheme {scheme} is not supported")
+        sfx = "_Swap" if scheme == "Scheme_StreamCollision_Swap" else ""
         coll = js.get("CollisionType", ["Collision_BGKIsothermal2nd"])[0]
-        if coll != "Collision_BGKIsothermal2nd":
-            raise ValueError(f"collision {coll} is not supported")
+        if coll != "Collision_BGKIsothermal2nd" + sfx:
+            raise ValueError(f"collision {coll} is not supported with "
+                             f"{scheme}")
+        force = js.get("BodyForceType", ["BodyForce_None" + sfx])[0]
+        if force not in ("BodyForce_None" + sfx, "BodyForce_1st" + sfx):
+            raise ValueError(f"body force {force} is not supported with "
+                             f"{scheme}")
+        force = force[:len(force) - len(sfx)]
         mv = js.get("MacroVarTypes", [])
         bounds = []
         i = 0
@@ -205,7 +223,7 @@ class CaseConfig:
             connections=conns,
             start_pos={int(k): v for k, v in sp.items()} if sp else None,
             force_velocity=any(m.endswith("_Force") for m in mv),
-            body_force=js.get("BodyForceType", ["BodyForce_None"])[0],
+            body_force=force, scheme=scheme,
             accel=tuple(acc[:3]),
             initial=(float(im.get("rho", 1.0)), float(im.get("u", 0.0)),
                      float(im.get("v", 0.0)), float(im.get("w", 0.0))),
@@ -270,6 +288,7 @@ class CaseConfig:
         for k in range(3):
             d.accel[k] = self.accel[k]
         d.force_velocity = 1 if self.force_velocity else 0
+        d.scheme = abi.SCHEMES[self.scheme]
         return d, (blocks, conns, bcs)
 
 
@@ -286,7 +305,8 @@ def lattice_tau_to_tauref(tau_l: float, dt: float) -> float:
 def cavity(dim: int, n: int, lid_u_lattice: float, re: float = None,
            tau_lattice: float = None, wall: str = "EQMDiffuseRefl",
            order=None, precision: str = "fp64",
-           check_period: int = 1000) -> CaseConfig:
+           check_period: int = 1000,
+           scheme: str = "Scheme_StreamCollision") -> CaseConfig:
     """Lid-driven cavity with n nodes per side.  The lid is Top in 2D and
     Front (z-max) in 3D and moves along +x.  tau_L comes from Re
     (nu = U N / Re, tau = 3 nu + 1/2) unless given."""
@@ -308,7 +328,7 @@ def cavity(dim: int, n: int, lid_u_lattice: float, re: float = None,
         case_name=f"cavity{dim}d", space_dim=dim, block_ids=[0],
         block_names=["Cavity"], block_sizes=[(n,) * dim], mesh_size=mesh,
         tau_ref=lattice_tau_to_tauref(tau_lattice, dt), boundaries=bounds,
-        precision=precision, check_period=check_period)
+        precision=precision, check_period=check_period, scheme=scheme)
 
 
 def _bc(block, surface, scheme, vtype, given=(), dim=3):

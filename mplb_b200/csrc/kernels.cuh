@@ -87,6 +87,14 @@ struct BlockDev {
     uint8_t rflags[kNumRegions];
     uint32_t rpull[kNumRegions];
     uint32_t rstale[kNumRegions];
+    // swap scheme (swap.cuh): per region the slots that live at slot opp(k)
+    // of the upstream node and the local-swap map; per population the
+    // element offset of that upstream slot (opp(k) * popstride - c_k .
+    // strides), 64- and 32-bit
+    uint32_t swap_exch[kNumRegions];
+    uint8_t swap_sigma[kNumRegions][kMaxQ];
+    long long swap_off[kMaxQ];
+    int swap_off32[kMaxQ];
 };
 
 enum StepMode : int { kModeStep = 0, kModeMacro = 1, kModeF = 2 };
@@ -1085,6 +1093,7 @@ __global__ void __launch_bounds__(128)
             for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = (double)f[i];
         }
     }
+    if (g == nullptr) return;   // one-array scheme: f^0 only
     MomentsCollideT<L, T>(f, pc, R.fluidlike != 0);
 #pragma unroll
     for (int i = 0; i < Q; i++)

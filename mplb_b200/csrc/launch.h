@@ -38,6 +38,13 @@ struct Launch {
     static cudaError_t Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
                             const BlockDev& fb, const BlockDev& tb,
                             const T* cur_from, const T* prev_from, T* cur_to);
+    // swap scheme (3D only): one step (kModeStep) or an observation of the
+    // current f, from the array in place; gather: slots at their streamed
+    // places; bc: boundary programme pending
+    static cudaError_t Swap(int mode, bool gather, bool bc, dim3 grid,
+                            cudaStream_t s, const BlockDev& b,
+                            const PhysConst& pc, T* f, double* o0, double* o1,
+                            double* o2, double* o3);
 };
 
 constexpr int kStepThreads = 128;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "launch.h"
+#include "swap.cuh"
 
 namespace mplb {
 
@@ -115,6 +116,45 @@ cudaError_t Launch<D, T>::Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
     HaloKernel<D, T><<<grid, 256, 0, s>>>(h, fb, tb, cur_from, prev_from,
                                           cur_to);
     return cudaGetLastError();
+}
+
+template <typename T, int MODE, bool O32>
+cudaError_t LaunchSwap(bool gather, bool bc, dim3 grid, cudaStream_t s,
+                       const BlockDev& b, const PhysConst& pc, T* f,
+                       double* o0, double* o1, double* o2, double* o3) {
+    if (gather && bc)
+        SwapKernel<T, MODE, true, true, O32><<<grid, kStepThreads, 0, s>>>(
+            b, pc, f, o0, o1, o2, o3);
+    else if (gather)
+        return cudaErrorInvalidValue;   // a gathered state always has one
+    else if (bc)
+        SwapKernel<T, MODE, false, true, O32><<<grid, kStepThreads, 0, s>>>(
+            b, pc, f, o0, o1, o2, o3);
+    else
+        SwapKernel<T, MODE, false, false, O32><<<grid, kStepThreads, 0, s>>>(
+            b, pc, f, o0, o1, o2, o3);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::Swap(int mode, bool gather, bool bc, dim3 grid,
+                               cudaStream_t s, const BlockDev& b,
+                               const PhysConst& pc, T* f, double* o0,
+                               double* o1, double* o2, double* o3) {
+    if constexpr (D != 3) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (mode == kModeStep)
+            return b.off32 ? LaunchSwap<T, kModeStep, true>(
+                                 gather, bc, grid, s, b, pc, f, o0, o1, o2, o3)
+                           : LaunchSwap<T, kModeStep, false>(
+                                 gather, bc, grid, s, b, pc, f, o0, o1, o2, o3);
+        if (mode == kModeMacro)
+            return LaunchSwap<T, kModeMacro, false>(gather, bc, grid, s, b, pc,
+                                                    f, o0, o1, o2, o3);
+        return LaunchSwap<T, kModeF, false>(gather, bc, grid, s, b, pc, f, o0,
+                                            o1, o2, o3);
+    }
 }
 
 }  // namespace mplb

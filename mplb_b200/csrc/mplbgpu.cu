@@ -1,7 +1,8 @@
 // C ABI of the B200 stream-collision path (include/mplbgpu.h).
 //
 // A context owns one CUDA stream and, per block, two population arrays in
-// the halo layout of kernels.cuh (ping-pong between steps), the boundary
+// the halo layout of kernels.cuh (ping-pong between steps; one array updated
+// in place under the swap scheme, swap.cuh), the boundary
 // tables produced by plan.cpp, the stale/deferred stores and the dense
 // macroscopic fields used by the residual.  Every entry point validates its
 // arguments and returns a status; CUDA errors are reported with the failing
@@ -58,6 +59,10 @@ struct mplbgpu_ctx {
     std::vector<DevHalo> halos;
     int cur = 0;            // pop[cur] holds the latest g
     bool initial = true;    // pop[1 - cur] holds f^0 itself
+    // swap scheme, contents of pop[0]: 0 f itself (initial or uploaded),
+    // 1 the locally swapped collided state, 2 the streamed state whose
+    // boundary programme is still to be applied
+    int swap_state = 0;
     bool halos_pending = true;
     std::vector<bool> initialised;
     cudaStream_t stream = nullptr;
@@ -187,8 +192,27 @@ int RunHalosT(mplbgpu_ctx* ctx) {
 
 int RunHalos(mplbgpu_ctx* ctx) { return MPLB_DISPATCH(ctx, RunHalosT, ctx); }
 
+// One step of the swap scheme (single block, no halos): from f itself or
+// the streamed state the node reads its own slots, from the locally swapped
+// state it gathers the streamed slots.
+template <int D, typename T>
+int SwapStepOnce(mplbgpu_ctx* ctx) {
+    ctx->pc.seed = (uint32_t)(++ctx->step_count);
+    DevBlock& b = ctx->blocks[0];
+    const BlockPlan& B = ctx->plan.blocks[0];
+    const int st = ctx->swap_state;
+    CK_LAUNCH_E(Launch<D, T>::Swap(kModeStep, st == 1, st != 0,
+                                   NodeGrid(B, D), ctx->stream, b.dev, ctx->pc,
+                                   static_cast<T*>(b.pop[0]), nullptr, nullptr,
+                                   nullptr, nullptr));
+    ctx->swap_state = st == 1 ? 2 : 1;
+    ctx->initial = false;
+    return MPLBGPU_OK;
+}
+
 template <int D, typename T>
 int StepOnce(mplbgpu_ctx* ctx) {
+    if (ctx->plan.swap) return SwapStepOnce<D, T>(ctx);
     const int src = ctx->cur, dst = 1 - ctx->cur;
     ctx->pc.seed = (uint32_t)(++ctx->step_count);
     for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
@@ -226,6 +250,14 @@ int Observe(mplbgpu_ctx* ctx, int mode, size_t bi, double* o0, double* o1,
             double* o2, double* o3) {
     DevBlock& b = ctx->blocks[bi];
     const BlockPlan& B = ctx->plan.blocks[bi];
+    if (ctx->plan.swap) {
+        const int st = ctx->swap_state;
+        CK_LAUNCH_E(Launch<D, T>::Swap(mode, st == 1, st != 0, NodeGrid(B, D),
+                                       ctx->stream, b.dev, ctx->pc,
+                                       static_cast<T*>(b.pop[0]), o0, o1, o2,
+                                       o3));
+        return MPLBGPU_OK;
+    }
     const int prev = 1 - ctx->cur;
     const T* pv = static_cast<const T*>(b.pop[prev]);
     if (ctx->initial) {
@@ -272,6 +304,13 @@ int InitBlock(mplbgpu_ctx* ctx, size_t bi, const double* d_rho,
               const double* d_f) {
     DevBlock& b = ctx->blocks[bi];
     const BlockPlan& B = ctx->plan.blocks[bi];
+    if (ctx->plan.swap) {
+        CK_LAUNCH_E(Launch<D, T>::Init(NodeGrid(B, D), ctx->stream, b.dev,
+                                       ctx->pc, d_rho, d_u, d_v, d_w, d_f,
+                                       static_cast<T*>(b.pop[0]), nullptr));
+        ctx->swap_state = 0;
+        return MPLBGPU_OK;
+    }
     CK_LAUNCH_E(Launch<D, T>::Init(NodeGrid(B, D), ctx->stream, b.dev,
                                    ctx->pc, d_rho, d_u, d_v, d_w, d_f,
                                    static_cast<T*>(b.pop[1 - ctx->cur]),
@@ -317,6 +356,13 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     for (int a = 0; a < 3; a++) pc.hdta_csf[a] = (float)(P.hdta[a] / P.cs);
     for (int i = 0; i < kMaxQ; i++) pc.wcff[i] = (float)(P.w[i] * P.cf[i]);
     pc.tw_omf = (float)(P.tw / (1.0 - P.omc));
+    if (P.swap) {
+        // KerSwapCalcBodyForce1ST3D adds the first-order force term itself
+        // after the collision, not tau * omega times it
+        pc.tw = 1.0;
+        pc.twf = 1.0f;
+        pc.tw_omf = (float)(1.0 / (1.0 - P.omc));
+    }
     auto fail_cuda = [&](cudaError_t e, const char* what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         FreeAll(c.get());
@@ -338,7 +384,7 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
         const BlockPlan& B = P.blocks[bi];
         DevBlock& b = c->blocks[bi];
         const size_t popbytes = (size_t)Q * B.popstride * P.elem_bytes;
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < (P.swap ? 1 : 2); k++) {
             if ((e = cudaMalloc(&b.pop[k], popbytes)) != cudaSuccess)
                 return fail_cuda(e, "cudaMalloc(populations)");
             if ((e = cudaMemsetAsync(b.pop[k], 0, popbytes, c->stream)) !=
@@ -449,6 +495,18 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
                                     (R.fluidlike ? 4 : 0));
             d.rpull[r] = R.pull;
             d.rstale[r] = R.stale;
+        }
+        for (int r = 0; r < kNumRegions; r++) {
+            d.swap_exch[r] = P.swap ? B.swap_exch[r] : 0u;
+            for (int k = 0; k < kMaxQ; k++)
+                d.swap_sigma[r][k] = P.swap ? B.swap_sigma[r][k] : (uint8_t)k;
+        }
+        for (int i = 0; i < kMaxQ; i++) {
+            const int o = i < Q ? (P.dim == 3 ? Lattice<3>::opp(i)
+                                              : Lattice<2>::opp(i))
+                                : i;
+            d.swap_off[i] = d.pull_off[i] + (long long)(o - i) * B.popstride;
+            d.swap_off32[i] = d.off32 ? (int)d.swap_off[i] : 0;
         }
         const int center = 13;   // interior on every axis (RegionOf)
         d.split = (B.n[0] >= 3 && B.n[1] >= 3 && (P.dim == 2 || B.n[2] >= 3) &&

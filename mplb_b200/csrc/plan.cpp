@@ -321,6 +321,133 @@ RegionOp MakeHbb(const Lat& L, double CS, const int n[3], const int p[3],
     return op;
 }
 
+// Swap scheme of the reference (KerLocalSwap3D / KerSwapStream3D,
+// Src/scheme_kernel.inc:959-1398).  A node exchanges its population l + Q/2
+// with population l of x + c_l (l = 1..Q/2) when it is fluid-like
+// (Fluid, MDPeriodic, VirtualBoundary) or, for a boundary-typed node, when
+// c_l has no component pointing out of any of its faces.
+bool SwapExchanges(const Lat& L, int vt, int nf, const int axis[3],
+                   const int sign[3], int l) {
+    if (vt == kVtSolid) return false;
+    if (PullsAll(vt)) return true;
+    if (nf == 0) return false;
+    for (int q = 0; q < nf; q++)
+        if (sign[q] * L.c[l][axis[q]] < 0) return false;
+    return true;
+}
+
+// The node's local swap as a map from slots to the collided populations.
+// Fluid-like nodes swap each population with its opposite; a boundary-typed
+// node walks l = 1..Q-1 in order over the directions with no inward
+// component (pointing out of or along its faces): a direction lying in all
+// of its faces is exchanged with its opposite (the walk meets both members
+// of the pair, so the pair ends where it began), any other direction takes
+// a copy of its opposite slot.
+void SwapLocal(const Lat& L, int vt, int nf, const int axis[3],
+               const int sign[3], uint8_t* sigma) {
+    const int half = (L.Q - 1) / 2;
+    for (int k = 0; k < kMaxQ; k++) sigma[k] = (uint8_t)(k < L.Q ? k : 0);
+    if (vt == kVtSolid) return;
+    if (PullsAll(vt)) {
+        for (int l = 1; l <= half; l++) std::swap(sigma[l], sigma[l + half]);
+        return;
+    }
+    for (int l = 1; l < L.Q && nf > 0; l++) {
+        bool out = true, along = true;
+        for (int q = 0; q < nf; q++) {
+            const int c = sign[q] * L.c[l][axis[q]];
+            if (c > 0) out = false;
+            if (c != 0) along = false;
+        }
+        if (!out) continue;
+        if (along) std::swap(sigma[l], sigma[L.opp[l]]);
+        else sigma[l] = sigma[L.opp[l]];
+    }
+}
+
+// Exchange masks and local-swap maps of every region.  In pull form slot k
+// (k <= Q/2) of x comes from the upstream node x - c_k when that node
+// exchanges direction k, slot k > Q/2 when x itself exchanges direction
+// k - Q/2 (it then lives at slot k - Q/2 = opp(k) of x + c_(k - Q/2) =
+// x - c_k).  Within a region the upstream node may sit in different
+// regions; the plan is accepted only where they all agree.
+int PlanSwap(const Lat& L, BlockPlan& B, std::string* err) {
+    const int half = (L.Q - 1) / 2;
+    for (int r = 0; r < kNumRegions; r++) {
+        const RegionInfo& R = B.region[r];
+        B.swap_exch[r] = 0;
+        for (int k = 0; k < kMaxQ; k++) B.swap_sigma[r][k] = (uint8_t)k;
+        if (R.cls < 0) continue;
+        int axis[3], sign[3];
+        const int nf = NodeFaces(3, B.n, R.org, axis, sign);
+        SwapLocal(L, R.vt, nf, axis, sign, B.swap_sigma[r]);
+        for (int k = 0; k < L.Q; k++) {
+            const int sg = B.swap_sigma[r][k];
+            if (sg != k && sg != L.opp[k]) {
+                *err = "local swap moves a population across directions";
+                return MPLBGPU_ERR_UNSUPPORTED;
+            }
+        }
+        const int rc[3] = {r % 3, (r / 3) % 3, r / 9};
+        for (int k = 1; k < L.Q; k++) {
+            if (k > half) {
+                const int l = k - half;
+                if (!SwapExchanges(L, R.vt, nf, axis, sign, l)) continue;
+                for (int a = 0; a < 3; a++) {
+                    const int c = L.c[l][a];
+                    if ((rc[a] == 0 && c < 0) || (rc[a] == 2 && c > 0)) {
+                        *err = "the swap scheme would exchange with a halo "
+                               "node (a fluid-like node on the block "
+                               "boundary)";
+                        return MPLBGPU_ERR_UNSUPPORTED;
+                    }
+                }
+                B.swap_exch[r] |= 1u << k;
+                continue;
+            }
+            // upstream node z = x - c_k: its possible regions per axis
+            int opts[3][2], nopt[3];
+            bool outside = false;
+            for (int a = 0; a < 3; a++) {
+                const int c = L.c[k][a];
+                nopt[a] = 0;
+                if (rc[a] == 0) {
+                    if (c > 0) outside = true;
+                    else opts[a][nopt[a]++] = c < 0 ? 1 : 0;
+                } else if (rc[a] == 2) {
+                    if (c < 0) outside = true;
+                    else opts[a][nopt[a]++] = c > 0 ? 1 : 2;
+                } else {
+                    opts[a][nopt[a]++] = 1;
+                    if (c > 0) opts[a][nopt[a]++] = 0;
+                    if (c < 0) opts[a][nopt[a]++] = 2;
+                }
+            }
+            if (outside) continue;
+            int verdict = -1;
+            for (int i0 = 0; i0 < nopt[0]; i0++)
+                for (int i1 = 0; i1 < nopt[1]; i1++)
+                    for (int i2 = 0; i2 < nopt[2]; i2++) {
+                        const int zr = opts[0][i0] + 3 * opts[1][i1] +
+                                       9 * opts[2][i2];
+                        const RegionInfo& Z = B.region[zr];
+                        if (Z.cls < 0) continue;
+                        int za[3], zs[3];
+                        const int zf = NodeFaces(3, B.n, Z.org, za, zs);
+                        const int e = SwapExchanges(L, Z.vt, zf, za, zs, k);
+                        if (verdict >= 0 && verdict != e) {
+                            *err = "swap exchange pattern differs within a "
+                                   "region";
+                            return MPLBGPU_ERR_UNSUPPORTED;
+                        }
+                        verdict = e;
+                    }
+            if (verdict == 1) B.swap_exch[r] |= 1u << k;
+        }
+    }
+    return MPLBGPU_OK;
+}
+
 bool Dispatched(int scheme) {
     return scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL ||
            scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST ||
@@ -348,6 +475,14 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
         return fail(MPLBGPU_ERR_INVALID, "dt, cs and tau must be positive");
     if (d.body_force != MPLBGPU_FORCE_NONE && d.body_force != MPLBGPU_FORCE_1ST)
         return fail(MPLBGPU_ERR_UNSUPPORTED, "unknown body force type");
+    if (d.scheme != 0 && d.scheme != MPLBGPU_SCHEME_STREAM_COLLISION &&
+        d.scheme != MPLBGPU_SCHEME_STREAM_COLLISION_SWAP)
+        return fail(MPLBGPU_ERR_UNSUPPORTED, "unknown scheme");
+    const bool swap = d.scheme == MPLBGPU_SCHEME_STREAM_COLLISION_SWAP;
+    if (swap && (d.space_dim != 3 || d.nblocks != 1 || d.nconnections != 0))
+        return fail(MPLBGPU_ERR_UNSUPPORTED,
+                    "the swap scheme runs on one 3D block without "
+                    "connections (the reference's swap kernels are 3D)");
 
     Plan& P = *plan;
     P.dim = d.space_dim;
@@ -365,6 +500,7 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
     P.tw = tau * P.omega;
     P.body_force = d.body_force;
     P.force_velocity = d.force_velocity ? 1 : 0;
+    P.swap = swap ? 1 : 0;
     Lat L{};
     if (P.dim == 2) FillLat<2>(&L); else FillLat<3>(&L);
     for (int a = 0; a < 3; a++) {
@@ -622,6 +758,32 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                 if (!dop.segments.empty()) B.dops.push_back(dop);
             }
         }
+    }
+
+    // swap scheme: node-local boundary programmes (EQMDiffuseRefl or no
+    // kernel), at least three nodes per axis
+    if (P.swap) {
+        BlockPlan& B = P.blocks[0];
+        for (int a = 0; a < 3; a++)
+            if (B.n[a] < 3)
+                return fail(MPLBGPU_ERR_UNSUPPORTED,
+                            "the swap scheme needs at least 3 nodes per axis");
+        for (int r = 0; r < kNumRegions; r++) {
+            if ((int)B.allops[r].size() > kMaxOps)
+                return fail(MPLBGPU_ERR_UNSUPPORTED,
+                            "too many boundary conditions on one node");
+            for (int oi : B.allops[r])
+                if (B.ops[oi].kind != kOpEqm)
+                    return fail(MPLBGPU_ERR_UNSUPPORTED,
+                                "the swap scheme takes node-local boundary "
+                                "conditions only (EQMDiffuseRefl)");
+        }
+        const RegionInfo& C = B.region[13];
+        if (!C.fluidlike || !B.allops[13].empty())
+            return fail(MPLBGPU_ERR_UNSUPPORTED,
+                        "the swap scheme needs a fluid interior");
+        int rc = PlanSwap(L, B, err);
+        if (rc != MPLBGPU_OK) return rc;
     }
 
     // halo transfers: Field::CreateHalos order, Src/field.h:215-395

@@ -93,6 +93,12 @@ struct BlockPlan {
     long long ndeferred;
     std::vector<DeferredOp> dops;
     std::vector<int> allops[kNumRegions];  // every op of a region (host)
+    // swap scheme: per region, slot k of a node holds population
+    // swap_sigma[r][k] of the collided node after its local swap, and
+    // swap_exch[r] bit k says that slot k lives at slot opp(k) of the
+    // upstream node x - c_k instead of the node's own slot k
+    uint8_t swap_sigma[kNumRegions][kMaxQ];
+    uint32_t swap_exch[kNumRegions];
     bool any_deferred() const { return ndeferred > 0; }
     long long nodes() const { return (long long)n[0] * n[1] * n[2]; }
 };
@@ -124,6 +130,7 @@ struct Plan {
     double hdta[3] = {0, 0, 0};  // dt * a / 2
     double cf[kMaxQ] = {};       // CS c_i . a  (CalcBodyForce sum)
     double w[kMaxQ] = {};
+    int swap = 0;       // Scheme_StreamCollision_Swap: one population array
     std::vector<BlockPlan> blocks;  // sorted by id
     std::vector<HaloCopy> halos;
 };

@@ -12,6 +12,7 @@
 #include "flowfield.h"
 #include "model.h"
 #include "mplbgpu.h"
+#include "scheme.h"
 
 namespace mplbgpu_dropin {
 namespace {
@@ -97,7 +98,13 @@ void Create() {
     d.tau_ref = compo.tauRef;
     d.dt = TimeStep();
     d.cs = SoundSpeed();
-    d.body_force = (int)compo.bodyForceType;
+    // the _Swap force types add the same first-order term after the
+    // collision instead of inside it; the scheme tells the two apart
+    d.body_force = (compo.bodyForceType == BodyForce_1st ||
+                    compo.bodyForceType == BodyForce_1st_Swap)
+                       ? MPLBGPU_FORCE_1ST
+                       : MPLBGPU_FORCE_NONE;
+    d.scheme = (int)Scheme();
     d.force_velocity =
         compo.macroVars.count(Variable_U_Force) ? 1 : 0;
     // uniform body acceleration: the force field's first node
@@ -126,6 +133,8 @@ void StreamCollision(const Real /*time*/) {
     if (g_ctx == nullptr) Create();
     Check(mplbgpu_step(g_ctx, 1), "mplbgpu_step");
 }
+
+void SwapStreamCollision(const Real time) { StreamCollision(time); }
 
 void UpdateMacroVars() {
     Check(mplbgpu_update_macro(g_ctx), "mplbgpu_update_macro");

@@ -27,6 +27,10 @@ bool Active();
 // Replaces the body of StreamCollision(time) (Src/evolution.cpp:137-193).
 void StreamCollision(const Real time);
 
+// Replaces the body of SwapStreamCollision(time) (Src/evolution.cpp:
+// 195-252); the context was created with the swap scheme (Scheme()).
+void SwapStreamCollision(const Real time);
+
 // Replaces UpdateMacroVars3D / UpdateMacroVars when Active().
 void UpdateMacroVars();
 

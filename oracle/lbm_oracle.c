@@ -41,6 +41,7 @@ struct lbm_oracle {
     int dim, Q, nmac;
     double cs, tau, dt;
     int body_force, force_vel;
+    int swap;     /* Scheme_StreamCollision_Swap */
     double accel[3];
     double xi[19 * 3];
     double w[19];
@@ -325,6 +326,8 @@ static int bdy_dv_type(const lbm_oracle* o, int vg, int l) {
 /* Stream selection of KerStream / KerStream3D for boundary-typed nodes,
  * Src/scheme_kernel.inc:53-221, 1400-2051: pull direction l when every
  * inward component of c_l is <= 0 (faces: one, edges: both, corners: all). */
+static int is_fluidlike(int vt);
+
 static int stream_pulls(const lbm_oracle* o, int vg, int l) {
     int axis[3], sign[3];
     const int n = decode_vg(vg, axis, sign);
@@ -351,6 +354,18 @@ int lbmo_create(const mplbgpu_desc* d, lbm_oracle** out) {
     o->dt = d->dt;
     o->body_force = d->body_force;
     o->force_vel = d->force_velocity;
+    o->swap = d->scheme == MPLBGPU_SCHEME_STREAM_COLLISION_SWAP;
+    if (d->scheme != 0 && d->scheme != MPLBGPU_SCHEME_STREAM_COLLISION &&
+        !o->swap) {
+        free(o);
+        return fail("unknown scheme");
+    }
+    if (o->swap && (d->space_dim != 3 || d->nblocks != 1 ||
+                    d->nconnections != 0)) {
+        free(o);
+        return fail("the swap scheme runs on one 3D block without "
+                    "connections");
+    }
     for (int a = 0; a < 3; a++) o->accel[a] = d->accel[a];
     setup_lattice(o);
     /* blocks sorted by id: the reference keeps them in a std::map */
@@ -404,6 +419,12 @@ int lbmo_create(const mplbgpu_desc* d, lbm_oracle** out) {
             lbmo_destroy(o);
             return fail("FDPeriodic reads a halo of f that is never "
                         "transferred");
+        }
+        if (o->swap && (o->bc[i].scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST ||
+                        o->bc[i].scheme == MPLBGPU_BC_HALFWAY_BOUNCE_BACK)) {
+            lbmo_destroy(o);
+            return fail("the swap scheme takes node-local boundary "
+                        "conditions only");
         }
         int found = 0;
         for (int j = 0; j < o->nb; j++) found |= o->b[j].id == o->bc[i].block;
@@ -509,6 +530,23 @@ int lbmo_create(const mplbgpu_desc* d, lbm_oracle** out) {
             }
         }
         fill_int(b, b->vt, r, bc->vertex_type);
+    }
+    if (o->swap) {
+        /* a fluid-like node on the block boundary would swap with its halo */
+        const oblock* b = &o->b[0];
+        for (int k = 0; k < b->n[2]; k++)
+            for (int j = 0; j < b->n[1]; j++)
+                for (int i = 0; i < b->n[0]; i++) {
+                    if (i > 0 && i < b->n[0] - 1 && j > 0 &&
+                        j < b->n[1] - 1 && k > 0 && k < b->n[2] - 1)
+                        continue;
+                    const int vt = b->vt[pidx(b, i, j, k)];
+                    if (is_fluidlike(vt) || vt == VT_VIRTUAL_BOUNDARY) {
+                        lbmo_destroy(o);
+                        return fail("the swap scheme needs a boundary "
+                                    "condition on every block face");
+                    }
+                }
     }
     *out = o;
     return 0;
@@ -943,8 +981,124 @@ static void one_step(lbm_oracle* o) {
     }
 }
 
+/* KerLocalSwap3D, Src/scheme_kernel.inc:959-1194, on one node.  Fluid-like
+ * nodes exchange each population with its opposite (l <-> l + half).  A
+ * boundary-typed node walks l = 1..Q-1 in order over the directions that
+ * point outward or along its faces (every inward component <= 0): a
+ * direction lying in all of its faces is exchanged with its opposite (the
+ * walk meets both members of such a pair, so the pair ends where it began),
+ * any other takes a copy of its opposite.  Geometry codes without faces
+ * leave the node alone. */
+static void swap_local(const lbm_oracle* o, int vt, int vg, double* f) {
+    const int Q = o->Q, half = (Q - 1) / 2;
+    if (vt == VT_IMMERSED_SOLID) return;
+    if (is_fluidlike(vt) || vt == VT_VIRTUAL_BOUNDARY) {
+        for (int l = 1; l <= half; l++) {
+            const double t = f[l];
+            f[l] = f[l + half];
+            f[l + half] = t;
+        }
+        return;
+    }
+    int axis[3], sign[3];
+    const int n = decode_vg(vg, axis, sign);
+    for (int l = 1; l < Q && n > 0; l++) {
+        int outward = 1, along = 1;
+        for (int p = 0; p < n; p++) {
+            const int c = sign[p] * C(o, l, axis[p]);
+            if (c > 0) outward = 0;
+            if (c != 0) along = 0;
+        }
+        if (!outward) continue;
+        if (along) {
+            const double t = f[l];
+            f[l] = f[o->opp[l]];
+            f[o->opp[l]] = t;
+        } else {
+            f[l] = f[o->opp[l]];
+        }
+    }
+}
+
+/* KerSwapStream3D, Src/scheme_kernel.inc:1196-1398: node x exchanges its
+ * population l + half with population l of x + c_l, for l = 1..half; a
+ * boundary-typed node only for directions with every inward component >= 0
+ * (those whose opposite does not point into the node from outside). */
+static int swap_streams(const lbm_oracle* o, int vt, int vg, int l) {
+    if (vt == VT_IMMERSED_SOLID) return 0;
+    if (is_fluidlike(vt) || vt == VT_VIRTUAL_BOUNDARY) return 1;
+    int axis[3], sign[3];
+    const int n = decode_vg(vg, axis, sign);
+    if (n == 0) return 0;
+    for (int p = 0; p < n; p++)
+        if (sign[p] * C(o, l, axis[p]) < 0) return 0;
+    return 1;
+}
+
+/* SwapStreamCollision, Src/evolution.cpp:195-252: moments, in-place
+ * collision (KerSwapCollideBGKIsothermal3D, Src/model_kernel.inc:385-408),
+ * body force added after it (KerSwapCalcBodyForce1ST3D, :543-568), local
+ * swap, swap streaming, boundary conditions on f. */
+static void swap_step(lbm_oracle* o) {
+    const int Q = o->Q, D = o->dim, half = (Q - 1) / 2;
+    const double CS = o->cs;
+    update_macro(o);
+    oblock* b = &o->b[0];
+    const double tau = o->tau;
+    const double dtOvertauPlusdt = o->dt / (tau + 0.5 * o->dt);
+    for (int k = 0; k < b->n[2]; k++)
+        for (int j = 0; j < b->n[1]; j++)
+            for (int i = 0; i < b->n[0]; i++) {
+                const size_t p = pidx(b, i, j, k);
+                double* f = &b->f[p * Q];
+                const double rho = b->mac[0][p], u = b->mac[1][p],
+                             v = b->mac[2][p], w = b->mac[3][p];
+                for (int l = 0; l < Q; l++) {
+                    const double fe = feq(o, l, rho, u, v, w);
+                    f[l] = fe + (1 - dtOvertauPlusdt) * (f[l] - fe);
+                }
+                if (o->body_force == MPLBGPU_FORCE_1ST &&
+                    is_fluidlike(b->vt[p])) {
+                    for (int l = 0; l < Q; l++) {
+                        double cf = 0;
+                        for (int a = 0; a < D; a++)
+                            cf += CS * o->xi[l * D + a] * o->accel[a];
+                        f[l] += o->w[l] * b->mac[0][p] * cf;
+                    }
+                }
+            }
+    for (int k = 0; k < b->n[2]; k++)
+        for (int j = 0; j < b->n[1]; j++)
+            for (int i = 0; i < b->n[0]; i++) {
+                const size_t p = pidx(b, i, j, k);
+                swap_local(o, b->vt[p], b->vg[p], &b->f[p * Q]);
+            }
+    for (int k = 0; k < b->n[2]; k++)
+        for (int j = 0; j < b->n[1]; j++)
+            for (int i = 0; i < b->n[0]; i++) {
+                const size_t p = pidx(b, i, j, k);
+                for (int l = 1; l <= half; l++) {
+                    if (!swap_streams(o, b->vt[p], b->vg[p], l)) continue;
+                    const size_t q = pidx(b, i + C(o, l, 0), j + C(o, l, 1),
+                                          k + C(o, l, 2));
+                    const double t = b->f[p * Q + l + half];
+                    b->f[p * Q + l + half] = b->f[q * Q + l];
+                    b->f[q * Q + l] = t;
+                }
+            }
+    for (int i = 0; i < o->nbc; i++) {
+        const mplbgpu_boundary* bc = &o->bc[i];
+        int r[6];
+        surface_range(o, b, bc->surface, r);
+        if (bc->scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL) bc_eqm(o, b, r, bc->given);
+    }
+}
+
 int lbmo_step(lbm_oracle* o, int nsteps) {
-    for (int s = 0; s < nsteps; s++) one_step(o);
+    for (int s = 0; s < nsteps; s++) {
+        if (o->swap) swap_step(o);
+        else one_step(o);
+    }
     return 0;
 }
 

@@ -127,10 +127,18 @@ static void UpdateMacro() {
 #endif
 }
 
+// The case's "SchemeType": Scheme_StreamCollision_Swap selects the
+// reference's one-array swap step (Src/evolution.cpp:195-252).
+bool g_swapScheme{false};
+
 static void Step(Real time) {
 #ifdef MPLB_DROPIN
     mplbgpu_dropin::StreamCollision(time);
 #else
+    if (g_swapScheme) {
+        SwapStreamCollision(time);
+        return;
+    }
     StreamCollision(time);
 #endif
 }
@@ -175,6 +183,7 @@ int main(int argc, const char** argv) {
     ReadConfiguration(configFile);
     const Configuration& config{Config()};
     const nlohmann::json& js{JsonConfig()};
+    g_swapScheme = config.schemeType == Scheme_StreamCollision_Swap;
     if (js.contains("InitialMacroVars")) {
         const auto& im = js["InitialMacroVars"];
         if (im.contains("rho")) g_rho0 = im["rho"].get<Real>();

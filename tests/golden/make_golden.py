@@ -6,8 +6,12 @@ the reference's JSON format; the final moments, distributions and residual
 history are saved as .npz.  Run in a checkout that has the reference
 sources available:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [name ...]
+
+(all cases, or only the named ones).  The *_swap cases run the reference's
+one-array swap step (SchemeType Scheme_StreamCollision_Swap).
 """
+import dataclasses
 import json
 import os
 import sys
@@ -33,11 +37,32 @@ CASES = {
                      300, 100),
     "poiseuille3d": (lambda: config.poiseuille(3, 6, 8, 5, g_lattice=1e-4),
                      80, 40),
+    "cavity3d_10_swap": (lambda: config.cavity(
+        3, 10, 0.05, re=400, scheme="Scheme_StreamCollision_Swap"), 60, 20),
+    # non-cubic box, first-order body force with the force-shifted velocity
+    "box3d_force_swap": (lambda: dataclasses.replace(
+        config.cavity(3, 10, 0.05, re=400,
+                      scheme="Scheme_StreamCollision_Swap"),
+        block_sizes=[(12, 9, 7)], body_force="BodyForce_1st",
+        accel=(3e-3, -2e-3, 1e-3), force_velocity=True), 41, 10),
+    # another definition order and a face whose scheme dispatches no kernel
+    "box3d_order_swap": (lambda: _order_swap(), 25, 5),
 }
 
 
-def main():
+def _order_swap():
+    c = config.cavity(3, 8, 0.05, re=100, scheme="Scheme_StreamCollision_Swap",
+                      order=("Front", "Back", "Top", "Bottom", "Left",
+                             "Right"))
+    b = list(c.boundaries)
+    b[3] = dataclasses.replace(b[3], scheme="BounceBack")
+    return dataclasses.replace(c, block_sizes=[(8, 11, 6)], boundaries=b)
+
+
+def main(names=None):
     for name, (build, steps, cp) in CASES.items():
+        if names and name not in names:
+            continue
         case = build()
         case.check_period = cp
         ref = pyoracle.run_reference(case, steps)
@@ -56,4 +81,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -2,6 +2,8 @@
 bitwise against the golden fixtures made by the reference itself, and -
 where the reference build is present - against the reference on more
 cases."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -34,8 +36,19 @@ def test_oracle_matches_reference_golden(oracle_mod, name):
     assert np.array_equal(np.array([h[0] for h in hist]), g["residual_max"])
 
 
+def _swap_box():
+    c = config.cavity(3, 13, 0.05, re=200,
+                      scheme="Scheme_StreamCollision_Swap")
+    return dataclasses.replace(c, block_sizes=[(13, 10, 9)],
+                               body_force="BodyForce_1st",
+                               accel=(-2e-3, 1e-3, 4e-3))
+
+
 REF_CASES = {
     "cavity3d_13": (lambda: config.cavity(3, 13, 0.05, re=400), 40, 20),
+    # the reference's one-array swap step, force without the shifted
+    # velocity
+    "swap_box_force": (_swap_box, 33, 11),
     "cavity2d_lid_first": (lambda: config.cavity(
         2, 15, 0.1, re=30, order=("Top", "Left", "Right", "Bottom")), 120, 40),
     "lchannel_app_9": (lambda: config.lchannel_app(9), 50, 25),
@@ -107,3 +120,17 @@ def test_json_round_trip():
     case = config.lchannel(leg=12, side=8, depth=6)
     back = config.CaseConfig.from_json(case.to_json())
     assert back.to_json() == case.to_json()
+
+
+def test_oracle_rejects_swap_outside_its_scope(oracle_mod):
+    """The swap scheme of this path: one 3D block, no connections,
+    node-local boundary conditions on every face."""
+    swap = "Scheme_StreamCollision_Swap"
+    bad = [config.cavity(2, 9, 0.05, re=100, scheme=swap),
+           config.cavity(3, 9, 0.05, re=100, scheme=swap,
+                         wall="HalfwayBounceBack"),
+           dataclasses.replace(config.lchannel(leg=9, side=6, depth=4),
+                               scheme=swap)]
+    for case in bad:
+        with pytest.raises(ValueError):
+            oracle_mod.Oracle(case)
