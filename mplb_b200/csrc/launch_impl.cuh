@@ -9,22 +9,30 @@ namespace mplb {
 
 static_assert(kSplitCta == kStepThreads, "SplitStepKernel CTA size");
 
+// CTAs of SplitStepKernel / SplitSwapKernel for block b (0: too many).
+template <int D, typename T>
+long long SplitBlocks(const BlockDev& b) {
+    const long long nbx = (b.n[0] + kStepThreads - 1) / kStepThreads;
+    const long long ny = b.n[1] - 2;
+    const long long nz = D == 3 ? b.n[2] : 1;
+    const long long rows = ny * (D == 3 ? b.n[2] - 2 : 1);
+    const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
+    const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
+    const long long nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
+    const long long blocks =
+        nsr + chunks * (1 + kSplitRows * (SplitPair<T>() == 2 ? nbx2 : nbx));
+    return blocks > 0x7fffffffLL ? 0 : blocks;
+}
+
+
 template <int D, typename T>
 cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const BlockDev& b, const PhysConst& pc,
                                const T* src, T* dst, double* o0, double* o1,
                                double* o2, double* o3) {
     if (mode == kModeStep && b.split) {
-        const long long nbx = (b.n[0] + kStepThreads - 1) / kStepThreads;
-        const long long ny = b.n[1] - 2;
-        const long long nz = D == 3 ? b.n[2] : 1;
-        const long long rows = ny * (D == 3 ? b.n[2] - 2 : 1);
-        const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
-        const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
-        const long long nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
-        const long long blocks =
-            nsr + chunks * (1 + kSplitRows * (SplitPair<T>() == 2 ? nbx2 : nbx));
-        if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        const long long blocks = SplitBlocks<D, T>(b);
+        if (blocks == 0) return cudaErrorInvalidConfiguration;
         if (b.off32)
             SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(
                 b, pc, src, dst);
@@ -118,10 +126,26 @@ cudaError_t Launch<D, T>::Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
     return cudaGetLastError();
 }
 
+template <typename T, bool GATHER, bool BC, bool O32>
+cudaError_t LaunchSplitSwap(cudaStream_t s, const BlockDev& b,
+                            const PhysConst& pc, T* f) {
+    const long long blocks = SplitBlocks<3, T>(b);
+    if (blocks == 0) return cudaErrorInvalidConfiguration;
+    SplitSwapKernel<T, GATHER, BC, O32><<<(unsigned)blocks, kStepThreads, 0,
+                                          s>>>(b, pc, f);
+    return cudaGetLastError();
+}
+
 template <typename T, int MODE, bool O32>
 cudaError_t LaunchSwap(bool gather, bool bc, dim3 grid, cudaStream_t s,
                        const BlockDev& b, const PhysConst& pc, T* f,
                        double* o0, double* o1, double* o2, double* o3) {
+    if (MODE == kModeStep && b.split) {
+        if (gather && !bc) return cudaErrorInvalidValue;
+        if (gather) return LaunchSplitSwap<T, true, true, O32>(s, b, pc, f);
+        if (bc) return LaunchSplitSwap<T, false, true, O32>(s, b, pc, f);
+        return LaunchSplitSwap<T, false, false, O32>(s, b, pc, f);
+    }
     if (gather && bc)
         SwapKernel<T, MODE, true, true, O32><<<grid, kStepThreads, 0, s>>>(
             b, pc, f, o0, o1, o2, o3);

@@ -42,21 +42,19 @@ __device__ __forceinline__ long long SwapSlot(const BlockDev& b,
         return node + (exch ? b.swap_off[k] : b.pop_off[k]);
 }
 
+// One node, any region.
 template <typename T, int MODE, bool GATHER, bool BC, bool O32>
-__global__ void __launch_bounds__(128, std::is_same<T, double>::value
-                                           ? MPLB_F64_MIN_BLOCKS
-                                           : MPLB_LP_MIN_BLOCKS)
-    SwapKernel(BlockDev b, PhysConst pc, T* f, double* __restrict__ out0,
-               double* __restrict__ out1, double* __restrict__ out2,
-               double* __restrict__ out3) {
+__device__ __forceinline__ void SwapNode(const BlockDev& b,
+                                         const PhysConst& pc, T* f,
+                                         double* __restrict__ out0,
+                                         double* __restrict__ out1,
+                                         double* __restrict__ out2,
+                                         double* __restrict__ out3, int x,
+                                         int y, int z) {
     using L = Lattice<3>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    const int z = blockIdx.z;
-    if (x >= b.n[0]) return;
     const int r = RegionOf(x, y, z, b.n, 3);
     const bool interior = r == 13;
     const long long node = NodeIndex<3>(b, x, y, z);
@@ -109,6 +107,144 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
             P::Store(f, SwapSlot<O32>(b, node, k, exch >> k & 1u), k, w, pc,
                      rng);
         }
+    }
+}
+
+// One node per thread over the whole block (observations, and steps of
+// blocks too thin for SplitSwapKernel).
+template <typename T, int MODE, bool GATHER, bool BC, bool O32>
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value
+                                           ? MPLB_F64_MIN_BLOCKS
+                                           : MPLB_LP_MIN_BLOCKS)
+    SwapKernel(BlockDev b, PhysConst pc, T* f, double* __restrict__ out0,
+               double* __restrict__ out1, double* __restrict__ out2,
+               double* __restrict__ out3) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= b.n[0]) return;
+    SwapNode<T, MODE, GATHER, BC, O32>(b, pc, f, out0, out1, out2, out3, x,
+                                       blockIdx.y, blockIdx.z);
+}
+
+// Interior nodes of one row: the pair (xa, xb) for the low-precision forms
+// (32 apart, so each warp access covers 256 contiguous bytes), xa alone for
+// FP64.  No boundary programme, opposite local swap, every moving slot
+// exchanged when gathering.
+template <typename T, bool GATHER, bool O32>
+__device__ __forceinline__ void SwapInteriorPair(const BlockDev& b,
+                                                 const PhysConst& pc, T* f,
+                                                 int xa, int xb, int y, int z,
+                                                 bool first, bool second) {
+    using L = Lattice<3>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int Q = L::Q;
+    const long long na0 = NodeIndex<3>(b, xa, y, z);
+    const long long nb0 = NodeIndex<3>(b, xb, y, z);
+    // an invalid node loads from (and is not stored to) the valid one
+    const long long na = first ? na0 : nb0;
+    const long long nb = second ? nb0 : na0;
+    constexpr bool two = sizeof(T) < 8;
+    C fa[Q], fb[two ? Q : 1];
+#pragma unroll
+    for (int k = 0; k < Q; k++) {
+        const bool e = GATHER && k != 0;
+        fa[k] = P::Load(f, SwapSlot<O32>(b, na, k, e), k, pc);
+        if constexpr (two) fb[k] = P::Load(f, SwapSlot<O32>(b, nb, k, e), k, pc);
+    }
+    const bool fl = b.center_fluid != 0;
+    if (first) {
+        MomentsCollideT<L, T>(fa, pc, fl);
+        Rng ra = SeedRng(pc.seed, na);
+#pragma unroll
+        for (int k = 0; k < Q; k++)
+            P::Store(f, SwapSlot<O32>(b, na, k, GATHER && k != 0), k,
+                     fa[L::opp(k)], pc, ra);
+    }
+    if constexpr (two) {
+        if (!second) return;
+        MomentsCollideT<L, T>(fb, pc, fl);
+        Rng rb = SeedRng(pc.seed, nb);
+#pragma unroll
+        for (int k = 0; k < Q; k++)
+            P::Store(f, SwapSlot<O32>(b, nb, k, GATHER && k != 0), k,
+                     fb[L::opp(k)], pc, rb);
+    }
+}
+
+// CTAs per SM of the FP64 swap step: 4 (128 registers); at 5 the in-place
+// step spills.
+#ifndef MPLB_SWAP_F64_MIN_BLOCKS
+#define MPLB_SWAP_F64_MIN_BLOCKS 4
+#endif
+
+// A step with no warp mixing interior and boundary nodes, in the CTA layout
+// of SplitStepKernel: shell rows (y or z on the block boundary), then per
+// chunk of kSplitRows interior rows one CTA for their x faces followed by
+// the CTAs of the rows' interior nodes (the x-face CTA runs next to its
+// rows, so the sectors they share meet in L2; as separate launches FP32 lost
+// 11 %).
+template <typename T, bool GATHER, bool BC, bool O32>
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value
+                                           ? MPLB_SWAP_F64_MIN_BLOCKS
+                                           : MPLB_LP_MIN_BLOCKS)
+    SplitSwapKernel(BlockDev b, PhysConst pc, T* f) {
+    const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int ny = b.n[1] - 2;
+    const int nz = b.n[2];
+    const long long nsr = (long long)nbx * (2 * nz + 2 * ny);
+    long long blk = blockIdx.x;
+    if (blk < nsr) {
+        const int row = (int)(blk / nbx);
+        const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
+        if (x >= b.n[0]) return;
+        int y, z;
+        if (row < 2 * nz) {
+            y = (row & 1) ? b.n[1] - 1 : 0;
+            z = row >> 1;
+        } else {
+            const int r2 = row - 2 * nz;
+            z = (r2 & 1) ? b.n[2] - 1 : 0;
+            y = 1 + (r2 >> 1);
+        }
+        SwapNode<T, kModeStep, GATHER, BC, O32>(b, pc, f, nullptr, nullptr,
+                                                nullptr, nullptr, x, y, z);
+        return;
+    }
+    blk -= nsr;
+    const long long rows = (long long)ny * (b.n[2] - 2);
+    constexpr int pair = SplitPair<T>();
+    const int nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
+    const long long per_chunk =
+        1 + (long long)kSplitRows * (pair == 2 ? nbx2 : nbx);
+    const long long chunk = blk / per_chunk;
+    const int w = (int)(blk % per_chunk);
+    if (w == 0) {
+        const long long r = chunk * kSplitRows + (threadIdx.x >> 1);
+        if (threadIdx.x >= 2 * kSplitRows || r >= rows) return;
+        const int x = (threadIdx.x & 1) ? b.n[0] - 1 : 0;
+        SwapNode<T, kModeStep, GATHER, BC, O32>(
+            b, pc, f, nullptr, nullptr, nullptr, nullptr, x,
+            1 + (int)(r % ny), 1 + (int)(r / ny));
+        return;
+    }
+    if constexpr (pair == 2) {
+        // warp v of the CTA has [64 v, 64 v + 64) of the row's 256 nodes,
+        // lane l the nodes 64 v + l and 64 v + 32 + l
+        const long long r = chunk * kSplitRows + (w - 1) / nbx2;
+        const int xa = ((w - 1) % nbx2) * 2 * kSplitCta +
+                       (threadIdx.x >> 5) * 64 + (threadIdx.x & 31);
+        const int xb = xa + 32;
+        const bool va = xa >= 1 && xa <= b.n[0] - 2;
+        const bool vb = xb >= 1 && xb <= b.n[0] - 2;
+        if (r >= rows || (!va && !vb)) return;
+        SwapInteriorPair<T, GATHER, O32>(b, pc, f, xa, xb, 1 + (int)(r % ny),
+                                         1 + (int)(r / ny), va, vb);
+    } else {
+        const long long r = chunk * kSplitRows + (w - 1) / nbx;
+        const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
+        if (r >= rows || x < 1 || x > b.n[0] - 2) return;
+        SwapInteriorPair<T, GATHER, O32>(b, pc, f, x, x, 1 + (int)(r % ny),
+                                         1 + (int)(r / ny), true, false);
     }
 }
 

@@ -52,7 +52,18 @@ long long Nodes(const Block& block) {
     return n;
 }
 
-void Create() {
+// Index (0 rho, 1 u, 2 v, 3 w) of a macroscopic variable type, or -1.
+int MacroSlot(int type) {
+    switch (type) {
+        case Variable_Rho: return 0;
+        case Variable_U: case Variable_U_Force: return 1;
+        case Variable_V: case Variable_V_Force: return 2;
+        case Variable_W: case Variable_W_Force: return 3;
+        default: return -1;
+    }
+}
+
+void Create(Real time) {
     const Component& compo = TheComponent();
     std::vector<mplbgpu_block> blocks;
     std::vector<mplbgpu_connection> conns;
@@ -118,6 +129,25 @@ void Create() {
     Check(mplbgpu_create(&d, &g_ctx), "mplbgpu_create");
     for (const auto& idBlock : g_Block()) {
         const Block& block = idBlock.second;
+        if (time == 0) {
+            // fresh start: f is feq of the initial macroscopic fields
+            // (PreDefinedInitialCondition3D), which are also the residual's
+            // previous values; rebuilding f from them keeps both
+            std::vector<Real> q[4];
+            const double* p[4] = {nullptr, nullptr, nullptr, nullptr};
+            for (const auto& tv : compo.macroVars) {
+                const int m = MacroSlot(tv.first);
+                if (m < 0 || m > SpaceDim()) continue;
+                q[m].resize((size_t)Nodes(block));
+                ops_dat_fetch_data(g_MacroVars().at(tv.second.id).at(block.ID()),
+                                   0, reinterpret_cast<char*>(q[m].data()));
+                p[m] = q[m].data();
+            }
+            Check(mplbgpu_init_macro(g_ctx, block.ID(), p[0], p[1], p[2], p[3]),
+                  "mplbgpu_init_macro");
+            continue;
+        }
+        // restart: the distributions as read back by the reference
         std::vector<Real> f((size_t)Nodes(block) * NUMXI);
         ops_dat_fetch_data(g_f().at(block.ID()), 0,
                            reinterpret_cast<char*>(f.data()));
@@ -129,8 +159,8 @@ void Create() {
 
 bool Active() { return g_ctx != nullptr; }
 
-void StreamCollision(const Real /*time*/) {
-    if (g_ctx == nullptr) Create();
+void StreamCollision(const Real time) {
+    if (g_ctx == nullptr) Create(time);
     Check(mplbgpu_step(g_ctx, 1), "mplbgpu_step");
 }
 
@@ -150,14 +180,7 @@ void UpdateMacroVars() {
                                      q[1].data(), q[2].data(), q[3].data()),
               "mplbgpu_download_macro");
         for (const auto& tv : compo.macroVars) {
-            int m = -1;
-            switch (tv.first) {
-                case Variable_Rho: m = 0; break;
-                case Variable_U: case Variable_U_Force: m = 1; break;
-                case Variable_V: case Variable_V_Force: m = 2; break;
-                case Variable_W: case Variable_W_Force: m = 3; break;
-                default: break;
-            }
+            const int m = MacroSlot(tv.first);
             if (m < 0 || m > SpaceDim()) continue;
             ops_dat_set_data(g_MacroVars().at(tv.second.id).at(block.ID()), 0,
                              reinterpret_cast<char*>(q[m].data()));
@@ -178,14 +201,7 @@ void CalcResidualError() {
     Check(mplbgpu_residual(g_ctx, 1, per, &mx), "mplbgpu_residual");
     const Component& compo = TheComponent();
     for (const auto& tv : compo.macroVars) {
-        int m = -1;
-        switch (tv.first) {
-            case Variable_Rho: m = 0; break;
-            case Variable_U: case Variable_U_Force: m = 1; break;
-            case Variable_V: case Variable_V_Force: m = 2; break;
-            case Variable_W: case Variable_W_Force: m = 3; break;
-            default: break;
-        }
+        const int m = MacroSlot(tv.first);
         if (m >= 0 && m <= SpaceDim()) g_ResidualError().at(tv.second.id) = per[m];
     }
 }

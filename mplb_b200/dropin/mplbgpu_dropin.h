@@ -8,9 +8,11 @@
 //
 // On the first StreamCollision the glue reads what the setup API holds
 // (g_Block() and each Block::Neighbors(), BlockBoundaries(), g_Components(),
-// TimeStep(), SoundSpeed(), g_MacroBodyforce(), g_f()), creates an
-// mplbgpu context and uploads f; from then on the distributions stay on the
-// GPU.  UpdateMacroVars copies the moments (and, unless MPLB_B200_SYNC_F=0,
+// TimeStep(), SoundSpeed(), g_MacroBodyforce(), g_MacroVars(), g_f()),
+// creates an mplbgpu context and sets its state - from the initial
+// macroscopic fields when the first step is at time 0 (f = feq of them, and
+// they are the residual's previous values as in the reference), else by
+// uploading f (restart); from then on the distributions stay on the GPU.  UpdateMacroVars copies the moments (and, unless MPLB_B200_SYNC_F=0,
 // the distributions) back into the reference's dats so that Iterate's HDF5
 // writers see current data.  MPLB_B200_PRECISION=fp32|fp16 selects a
 // shifted storage form (default fp64, bit-identical to the reference).
