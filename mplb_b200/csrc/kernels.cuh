@@ -78,6 +78,7 @@ struct BlockDev {
     int pull_off32[kMaxQ];
     int pop_off32[kMaxQ];
     int off32;
+    int plane32, pitch32;   // strides in 32 bits (valid when off32)
     // the step runs as SplitStepKernel (every extent >= 3 and the interior
     // region PURE); center_fluid: the interior is fluid-like
     int split;
@@ -232,6 +233,17 @@ __device__ __forceinline__ long long NodeIndex(const BlockDev& b, int x, int y,
                                                int z) {
     return (long long)(D == 3 ? z + 1 : 0) * b.plane +
            (long long)(y + 1) * b.pitch + (long long)(x + b.xoff);
+}
+
+// The same in 32-bit arithmetic when the population array fits (off32).
+template <int D, bool O32>
+__device__ __forceinline__ long long NodeIndexT(const BlockDev& b, int x, int y,
+                                                int z) {
+    if constexpr (O32)
+        return (D == 3 ? z + 1 : 0) * b.plane32 + (y + 1) * b.pitch32 +
+               (x + b.xoff);
+    else
+        return NodeIndex<D>(b, x, y, z);
 }
 
 template <typename L>
@@ -594,7 +606,7 @@ __device__ __forceinline__ void StepNode(const BlockDev& b,
     const int rf = b.rflags[r];
     const int cls = rf & 3;
     if (cls == kDeferred) return;
-    const long long node = NodeIndex<D>(b, x, y, z);
+    const long long node = NodeIndexT<D, O32>(b, x, y, z);
     C f[Q];
     if (cls == kPure) {
         if constexpr (O32) {
@@ -703,8 +715,8 @@ __device__ __forceinline__ void PureNodePair(const BlockDev& b,
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const long long na0 = NodeIndex<D>(b, xa, ya, za);
-    const long long nb0 = NodeIndex<D>(b, xb, yb, zb);
+    const long long na0 = NodeIndexT<D, O32>(b, xa, ya, za);
+    const long long nb0 = NodeIndexT<D, O32>(b, xb, yb, zb);
     // an invalid node loads from (and is not stored to) the valid one
     const long long na = first ? na0 : nb0;
     const long long nb = second ? nb0 : na0;
@@ -780,11 +792,13 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                            : MPLB_LP_MIN_BLOCKS)
     SplitStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
                     T* __restrict__ dst) {
+    // block and row counts fit in 32 bits (the launcher checks the grid),
+    // so the index arithmetic stays 32-bit
     const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
     const int ny = b.n[1] - 2;
     const int nz = D == 3 ? b.n[2] : 1;
-    const long long nsr = (long long)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
-    long long blk = blockIdx.x;
+    const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
+    unsigned blk = blockIdx.x;
     if (blk < nsr) {
         const int row = (int)(blk / nbx);
         const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
@@ -803,44 +817,42 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
         return;
     }
     blk -= nsr;
-    const long long rows = (long long)ny * (D == 3 ? b.n[2] - 2 : 1);
+    const int rows = ny * (D == 3 ? b.n[2] - 2 : 1);
     constexpr int pair = SplitPair<T>();
     const int nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
-    const long long per_chunk =
-        1 + (long long)kSplitRows * (pair == 2 ? nbx2 : nbx);
-    const long long chunk = blk / per_chunk;
+    const unsigned per_chunk = 1 + kSplitRows * (pair == 2 ? nbx2 : nbx);
+    const int chunk = (int)(blk / per_chunk);
     const int w = (int)(blk % per_chunk);
     if (w == 0) {
-        const long long r = chunk * kSplitRows + (threadIdx.x >> 1);
+        const int r = chunk * kSplitRows + (int)(threadIdx.x >> 1);
         if (threadIdx.x >= 2 * kSplitRows || r >= rows) return;
         const int x = (threadIdx.x & 1) ? b.n[0] - 1 : 0;
         StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
-                                       nullptr, nullptr, x,
-                                       1 + (int)(r % ny),
-                                       D == 3 ? 1 + (int)(r / ny) : 0);
+                                       nullptr, nullptr, x, 1 + r % ny,
+                                       D == 3 ? 1 + r / ny : 0);
         return;
     }
     if constexpr (pair == 2) {
         // interior CTAs: 256 nodes of one row; warp w has [64 w, 64 w + 64),
         // lane l the nodes 64 w + l and 64 w + 32 + l, so each of the
         // warp's population accesses covers 256 contiguous bytes
-        const long long r = chunk * kSplitRows + (w - 1) / nbx2;
+        const int r = chunk * kSplitRows + (w - 1) / nbx2;
         const int xa = ((w - 1) % nbx2) * 2 * kSplitCta +
                        (threadIdx.x >> 5) * 64 + (threadIdx.x & 31);
         const int xb = xa + 32;
         const bool va = xa >= 1 && xa <= b.n[0] - 2;
         const bool vb = xb >= 1 && xb <= b.n[0] - 2;
         if (r >= rows || (!va && !vb)) return;
-        const int y = 1 + (int)(r % ny);
-        const int z = D == 3 ? 1 + (int)(r / ny) : 0;
+        const int y = 1 + r % ny;
+        const int z = D == 3 ? 1 + r / ny : 0;
         PureNodePair<D, T, O32>(b, pc, src, dst, xa, y, z, xb, y, z, va, vb);
     } else {
         // interior CTAs: 128 nodes of one row
-        const long long r = chunk * kSplitRows + (w - 1) / nbx;
+        const int r = chunk * kSplitRows + (w - 1) / nbx;
         const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
         if (r >= rows || x < 1 || x > b.n[0] - 2) return;
-        const int y = 1 + (int)(r % ny);
-        const int z = D == 3 ? 1 + (int)(r / ny) : 0;
+        const int y = 1 + r % ny;
+        const int z = D == 3 ? 1 + r / ny : 0;
         PureNodePair<D, T, O32>(b, pc, src, dst, x, y, z, x, y, z, true,
                                 false);
     }

@@ -489,6 +489,8 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             d.pull_off32[i] = d.off32 ? (int)d.pull_off[i] : 0;
             d.pop_off32[i] = d.off32 ? (int)d.pop_off[i] : 0;
         }
+        d.plane32 = d.off32 ? (int)B.plane : 0;
+        d.pitch32 = d.off32 ? (int)B.pitch : 0;
         for (int r = 0; r < kNumRegions; r++) {
             const RegionInfo& R = B.region[r];
             d.rflags[r] = (uint8_t)((R.cls < 0 ? kPure : R.cls) |

@@ -57,7 +57,7 @@ __device__ __forceinline__ void SwapNode(const BlockDev& b,
     constexpr int Q = L::Q;
     const int r = RegionOf(x, y, z, b.n, 3);
     const bool interior = r == 13;
-    const long long node = NodeIndex<3>(b, x, y, z);
+    const long long node = NodeIndexT<3, O32>(b, x, y, z);
     // the interior exchanges every moving population, its local swap is the
     // opposite map, and it has no boundary programme
     const uint32_t exch = GATHER ? (interior ? ~1u : b.swap_exch[r]) : 0u;
@@ -138,8 +138,8 @@ __device__ __forceinline__ void SwapInteriorPair(const BlockDev& b,
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const long long na0 = NodeIndex<3>(b, xa, y, z);
-    const long long nb0 = NodeIndex<3>(b, xb, y, z);
+    const long long na0 = NodeIndexT<3, O32>(b, xa, y, z);
+    const long long nb0 = NodeIndexT<3, O32>(b, xb, y, z);
     // an invalid node loads from (and is not stored to) the valid one
     const long long na = first ? na0 : nb0;
     const long long nb = second ? nb0 : na0;
@@ -191,8 +191,8 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
     const int ny = b.n[1] - 2;
     const int nz = b.n[2];
-    const long long nsr = (long long)nbx * (2 * nz + 2 * ny);
-    long long blk = blockIdx.x;
+    const unsigned nsr = (unsigned)nbx * (2 * nz + 2 * ny);
+    unsigned blk = blockIdx.x;
     if (blk < nsr) {
         const int row = (int)(blk / nbx);
         const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
@@ -211,40 +211,39 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
         return;
     }
     blk -= nsr;
-    const long long rows = (long long)ny * (b.n[2] - 2);
+    const int rows = ny * (b.n[2] - 2);
     constexpr int pair = SplitPair<T>();
     const int nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
-    const long long per_chunk =
-        1 + (long long)kSplitRows * (pair == 2 ? nbx2 : nbx);
-    const long long chunk = blk / per_chunk;
+    const unsigned per_chunk = 1 + kSplitRows * (pair == 2 ? nbx2 : nbx);
+    const int chunk = (int)(blk / per_chunk);
     const int w = (int)(blk % per_chunk);
     if (w == 0) {
-        const long long r = chunk * kSplitRows + (threadIdx.x >> 1);
+        const int r = chunk * kSplitRows + (int)(threadIdx.x >> 1);
         if (threadIdx.x >= 2 * kSplitRows || r >= rows) return;
         const int x = (threadIdx.x & 1) ? b.n[0] - 1 : 0;
-        SwapNode<T, kModeStep, GATHER, BC, O32>(
-            b, pc, f, nullptr, nullptr, nullptr, nullptr, x,
-            1 + (int)(r % ny), 1 + (int)(r / ny));
+        SwapNode<T, kModeStep, GATHER, BC, O32>(b, pc, f, nullptr, nullptr,
+                                                nullptr, nullptr, x,
+                                                1 + r % ny, 1 + r / ny);
         return;
     }
     if constexpr (pair == 2) {
         // warp v of the CTA has [64 v, 64 v + 64) of the row's 256 nodes,
         // lane l the nodes 64 v + l and 64 v + 32 + l
-        const long long r = chunk * kSplitRows + (w - 1) / nbx2;
+        const int r = chunk * kSplitRows + (w - 1) / nbx2;
         const int xa = ((w - 1) % nbx2) * 2 * kSplitCta +
                        (threadIdx.x >> 5) * 64 + (threadIdx.x & 31);
         const int xb = xa + 32;
         const bool va = xa >= 1 && xa <= b.n[0] - 2;
         const bool vb = xb >= 1 && xb <= b.n[0] - 2;
         if (r >= rows || (!va && !vb)) return;
-        SwapInteriorPair<T, GATHER, O32>(b, pc, f, xa, xb, 1 + (int)(r % ny),
-                                         1 + (int)(r / ny), va, vb);
+        SwapInteriorPair<T, GATHER, O32>(b, pc, f, xa, xb, 1 + r % ny,
+                                         1 + r / ny, va, vb);
     } else {
-        const long long r = chunk * kSplitRows + (w - 1) / nbx;
+        const int r = chunk * kSplitRows + (w - 1) / nbx;
         const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
         if (r >= rows || x < 1 || x > b.n[0] - 2) return;
-        SwapInteriorPair<T, GATHER, O32>(b, pc, f, x, x, 1 + (int)(r % ny),
-                                         1 + (int)(r / ny), true, false);
+        SwapInteriorPair<T, GATHER, O32>(b, pc, f, x, x, 1 + r % ny,
+                                         1 + r / ny, true, false);
     }
 }
 
