@@ -576,7 +576,7 @@ __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
 // Fused step over one block.  kModeStep writes g^{n+1}; kModeMacro and
 // kModeF recompute the current f = post-boundary populations from the
 // previous g and write moments or f (FP64, dense) instead.
-// The shifted forms hold two interior nodes per thread (PureNodePair):
+// The shifted forms hold two interior nodes per thread (PureNodeGroup):
 // 6 CTAs of 128 threads per SM (<= 85 registers) keeps both nodes in
 // registers; 8 CTAs (64 registers) spilled and measured no faster.
 #ifndef MPLB_LP_MIN_BLOCKS
@@ -699,78 +699,105 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                               z);
 }
 
-// Two interior nodes per thread, 32 apart along x: both nodes' loads are
-// issued before either is computed, so a warp keeps 38 loads in flight
-// instead of 19, and each population access of the warp covers 256
-// contiguous bytes as in the FP64 form (the FP32 and FP16 forms otherwise
-// move 128 or 64 bytes per access).
-template <int D, typename T, bool O32>
-__device__ __forceinline__ void PureNodePair(const BlockDev& b,
-                                             const PhysConst& pc,
-                                             const T* __restrict__ src,
-                                             T* __restrict__ dst, int xa,
-                                             int ya, int za, int xb, int yb,
-                                             int zb, bool first, bool second) {
+// Interior nodes per thread (G, 32 apart along x): all G nodes' loads are
+// issued before any is computed, so a warp keeps 19 G loads in flight, and
+// for G >= 2 each population access of the warp covers 32 G contiguous
+// values (the FP32 and FP16 forms otherwise move 128 or 64 bytes per
+// access).  The FP64 form moves enough bytes per load and has no registers
+// for a second node.
+#ifndef MPLB_LP_GROUP
+#define MPLB_LP_GROUP 2
+#endif
+template <typename T>
+__host__ __device__ constexpr int SplitGroup() {
+    return sizeof(T) < 8 ? MPLB_LP_GROUP : 1;
+}
+
+// The G nodes x0 + 32 j (j < G) of one interior row; nodes outside
+// [1, n0 - 2] load from the first valid one and are not stored.
+template <int D, typename T, bool O32, int G>
+__device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
+                                              const PhysConst& pc,
+                                              const T* __restrict__ src,
+                                              T* __restrict__ dst, int x0,
+                                              int y, int z) {
     using L = Lattice<D>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const long long na0 = NodeIndexT<D, O32>(b, xa, ya, za);
-    const long long nb0 = NodeIndexT<D, O32>(b, xb, yb, zb);
-    // an invalid node loads from (and is not stored to) the valid one
-    const long long na = first ? na0 : nb0;
-    const long long nb = second ? nb0 : na0;
-    C fa[Q], fb[Q];
-    if constexpr (O32) {
-        const T* pa = src + na;
-        const T* pb = src + nb;
+    bool valid[G];
+    int first = -1;
 #pragma unroll
-        for (int i = 0; i < Q; i++) {
-            fa[i] = P::Load(pa, b.pull_off32[i], i, pc);
-            fb[i] = P::Load(pb, b.pull_off32[i], i, pc);
-        }
-    } else {
+    for (int j = 0; j < G; j++) {
+        const int x = x0 + 32 * j;
+        valid[j] = x >= 1 && x <= b.n[0] - 2;
+        if (valid[j] && first < 0) first = j;
+    }
+    if (first < 0) return;
+    long long node[G];
 #pragma unroll
-        for (int i = 0; i < Q; i++) {
-            fa[i] = P::Load(src, PullIndex<L>(b, na, i), i, pc);
-            fb[i] = P::Load(src, PullIndex<L>(b, nb, i), i, pc);
+    for (int j = 0; j < G; j++)
+        node[j] = NodeIndexT<D, O32>(b, x0 + 32 * (valid[j] ? j : first), y, z);
+    C f[G][Q];
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+#pragma unroll
+        for (int j = 0; j < G; j++) {
+            if constexpr (O32)
+                f[j][i] = P::Load(src + node[j], b.pull_off32[i], i, pc);
+            else
+                f[j][i] = P::Load(src, PullIndex<L>(b, node[j], i), i, pc);
         }
     }
     const bool fl = b.center_fluid != 0;
-    if (first) {
-    MomentsCollideT<L, T>(fa, pc, fl);
-    Rng ra = SeedRng(pc.seed, na);
-    if constexpr (O32) {
-        T* pd = dst + na;
 #pragma unroll
-        for (int i = 0; i < Q; i++) P::Store(pd, b.pop_off32[i], i, fa[i], pc, ra);
-    } else {
+    for (int j = 0; j < G; j++) {
+        if (!valid[j]) continue;
+        MomentsCollideT<L, T>(f[j], pc, fl);
+        Rng rg = SeedRng(pc.seed, node[j]);
+        if constexpr (O32) {
+            T* pd = dst + node[j];
 #pragma unroll
-        for (int i = 0; i < Q; i++)
-            P::Store(dst, OwnIndex(b, na, i), i, fa[i], pc, ra);
-    }
-    }
-    if (!second) return;
-    MomentsCollideT<L, T>(fb, pc, fl);
-    Rng rb = SeedRng(pc.seed, nb);
-    if constexpr (O32) {
-        T* pd = dst + nb;
+            for (int i = 0; i < Q; i++)
+                P::Store(pd, b.pop_off32[i], i, f[j][i], pc, rg);
+        } else {
 #pragma unroll
-        for (int i = 0; i < Q; i++) P::Store(pd, b.pop_off32[i], i, fb[i], pc, rb);
-    } else {
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            P::Store(dst, OwnIndex(b, nb, i), i, fb[i], pc, rb);
+            for (int i = 0; i < Q; i++)
+                P::Store(dst, OwnIndex(b, node[j], i), i, f[j][i], pc, rg);
+        }
     }
 }
 
-// Rows of interior nodes handled per x-face block of SplitStepKernel, and
-// interior nodes per thread (two for the low-precision forms; the FP64 form
-// moves enough bytes per load and has no registers for a second node).
+// Rows of interior nodes handled per x-face block of SplitStepKernel.
 constexpr int kSplitRows = 64;
 constexpr int kSplitCta = 128;   // threads per CTA of SplitStepKernel
-template <typename T>
-__host__ __device__ constexpr int SplitPair() { return sizeof(T) < 8 ? 2 : 1; }
+constexpr int kSplitWarps = kSplitCta / 32;
+
+// Interior "warp tasks": 32 G consecutive nodes of a row per warp; CTA c of
+// a chunk's interior takes tasks kSplitWarps c .. + kSplitWarps - 1.
+struct SplitTask {
+    int r;    // interior row (chunk-relative rows included), or -1
+    int x0;   // first node of the lane
+};
+template <int G>
+__device__ __forceinline__ SplitTask InteriorTask(const BlockDev& b,
+                                                  int chunk, int w) {
+    const int tpr = (b.n[0] + 32 * G - 1) / (32 * G);   // tasks per row
+    const int t = (w - 1) * kSplitWarps + (int)(threadIdx.x >> 5);
+    const int rl = t / tpr;
+    SplitTask k;
+    k.r = rl < kSplitRows ? chunk * kSplitRows + rl : -1;
+    k.x0 = (t - rl * tpr) * 32 * G + (int)(threadIdx.x & 31);
+    return k;
+}
+
+// CTAs of one chunk: the x-face CTA and the interior CTAs.
+template <int G>
+__host__ __device__ constexpr long long SplitChunkCtas(int n0) {
+    return 1 + ((long long)kSplitRows * ((n0 + 32 * G - 1) / (32 * G)) +
+                kSplitWarps - 1) /
+                   kSplitWarps;
+}
 
 // The step with no warp mixing interior and boundary nodes (a warp holding
 // one boundary node runs that node's boundary programme with the other 31
@@ -779,13 +806,12 @@ __host__ __device__ constexpr int SplitPair() { return sizeof(T) < 8 ? 2 : 1; }
 //   1. shell rows: every row with y or z on the block boundary (coalesced);
 //   2. per chunk of 64 interior rows, one CTA for their x = 0 and x = n0 - 1
 //      nodes, followed by
-//   3. the CTAs of those rows' interior nodes: 256 nodes of a row per CTA
-//      for FP32 / FP16 (two per thread, 32 apart; PureNodePair), 128 for
-//      FP64 (one per thread).  A row's CTAs start on the
-//      row's first node so every store begins on the row's 32-byte boundary
-//      (the two x-face lanes idle); the x-face CTA runs next to them, so the
-//      sectors they share meet in L2 instead of costing a read-modify-write
-//      in HBM.
+//   3. the CTAs of those rows' interior nodes, each warp taking 32 G
+//      consecutive nodes of a row (PureNodeGroup).  A row's tasks start on
+//      the row's first node so every store begins on the row's 32-byte
+//      boundary (the x-face lanes idle); the x-face CTA runs next to them,
+//      so the sectors they share meet in L2 instead of costing a
+//      read-modify-write in HBM.
 template <int D, typename T, bool O32>
 __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                            ? MPLB_F64_MIN_BLOCKS
@@ -818,9 +844,8 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     }
     blk -= nsr;
     const int rows = ny * (D == 3 ? b.n[2] - 2 : 1);
-    constexpr int pair = SplitPair<T>();
-    const int nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
-    const unsigned per_chunk = 1 + kSplitRows * (pair == 2 ? nbx2 : nbx);
+    constexpr int G = SplitGroup<T>();
+    const unsigned per_chunk = (unsigned)SplitChunkCtas<G>(b.n[0]);
     const int chunk = (int)(blk / per_chunk);
     const int w = (int)(blk % per_chunk);
     if (w == 0) {
@@ -832,30 +857,10 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                        D == 3 ? 1 + r / ny : 0);
         return;
     }
-    if constexpr (pair == 2) {
-        // interior CTAs: 256 nodes of one row; warp w has [64 w, 64 w + 64),
-        // lane l the nodes 64 w + l and 64 w + 32 + l, so each of the
-        // warp's population accesses covers 256 contiguous bytes
-        const int r = chunk * kSplitRows + (w - 1) / nbx2;
-        const int xa = ((w - 1) % nbx2) * 2 * kSplitCta +
-                       (threadIdx.x >> 5) * 64 + (threadIdx.x & 31);
-        const int xb = xa + 32;
-        const bool va = xa >= 1 && xa <= b.n[0] - 2;
-        const bool vb = xb >= 1 && xb <= b.n[0] - 2;
-        if (r >= rows || (!va && !vb)) return;
-        const int y = 1 + r % ny;
-        const int z = D == 3 ? 1 + r / ny : 0;
-        PureNodePair<D, T, O32>(b, pc, src, dst, xa, y, z, xb, y, z, va, vb);
-    } else {
-        // interior CTAs: 128 nodes of one row
-        const int r = chunk * kSplitRows + (w - 1) / nbx;
-        const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
-        if (r >= rows || x < 1 || x > b.n[0] - 2) return;
-        const int y = 1 + r % ny;
-        const int z = D == 3 ? 1 + r / ny : 0;
-        PureNodePair<D, T, O32>(b, pc, src, dst, x, y, z, x, y, z, true,
-                                false);
-    }
+    const SplitTask k = InteriorTask<G>(b, chunk, w);
+    if (k.r < 0 || k.r >= rows) return;
+    PureNodeGroup<D, T, O32, G>(b, pc, src, dst, k.x0, 1 + k.r % ny,
+                                D == 3 ? 1 + k.r / ny : 0);
 }
 
 // Deferred nodes: thread t -> (region, node).

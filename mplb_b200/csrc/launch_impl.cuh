@@ -18,12 +18,10 @@ long long SplitBlocks(const BlockDev& b) {
     const long long rows = ny * (D == 3 ? b.n[2] - 2 : 1);
     const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
     const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
-    const long long nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
     const long long blocks =
-        nsr + chunks * (1 + kSplitRows * (SplitPair<T>() == 2 ? nbx2 : nbx));
+        nsr + chunks * SplitChunkCtas<SplitGroup<T>()>(b.n[0]);
     return blocks > 0x7fffffffLL ? 0 : blocks;
 }
-
 
 template <int D, typename T>
 cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,

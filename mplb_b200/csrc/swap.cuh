@@ -125,49 +125,54 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                        blockIdx.y, blockIdx.z);
 }
 
-// Interior nodes of one row: the pair (xa, xb) for the low-precision forms
-// (32 apart, so each warp access covers 256 contiguous bytes), xa alone for
-// FP64.  No boundary programme, opposite local swap, every moving slot
-// exchanged when gathering.
-template <typename T, bool GATHER, bool O32>
-__device__ __forceinline__ void SwapInteriorPair(const BlockDev& b,
-                                                 const PhysConst& pc, T* f,
-                                                 int xa, int xb, int y, int z,
-                                                 bool first, bool second) {
+// The G interior nodes x0 + 32 j of one row (the layout of
+// PureNodeGroup): no boundary programme, opposite local swap, every moving
+// slot exchanged when gathering.
+template <typename T, bool GATHER, bool O32, int G>
+__device__ __forceinline__ void SwapInteriorGroup(const BlockDev& b,
+                                                  const PhysConst& pc, T* f,
+                                                  int x0, int y, int z) {
     using L = Lattice<3>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = L::Q;
-    const long long na0 = NodeIndexT<3, O32>(b, xa, y, z);
-    const long long nb0 = NodeIndexT<3, O32>(b, xb, y, z);
-    // an invalid node loads from (and is not stored to) the valid one
-    const long long na = first ? na0 : nb0;
-    const long long nb = second ? nb0 : na0;
-    constexpr bool two = sizeof(T) < 8;
-    C fa[Q], fb[two ? Q : 1];
+    bool valid[G];
+    int first = -1;
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+        const int x = x0 + 32 * j;
+        valid[j] = x >= 1 && x <= b.n[0] - 2;
+        if (valid[j] && first < 0) first = j;
+    }
+    if (first < 0) return;
+    T* p[G];
+    long long node[G];
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+        node[j] = NodeIndexT<3, O32>(b, x0 + 32 * (valid[j] ? j : first), y, z);
+        p[j] = f + node[j];
+    }
+    // element offset of slot k from the node (compile-time choice per k)
+    auto off = [&](int k) -> long long {
+        const bool e = GATHER && k != 0;
+        if constexpr (O32) return e ? b.swap_off32[k] : b.pop_off32[k];
+        else return e ? b.swap_off[k] : b.pop_off[k];
+    };
+    C v[G][Q];
 #pragma unroll
     for (int k = 0; k < Q; k++) {
-        const bool e = GATHER && k != 0;
-        fa[k] = P::Load(f, SwapSlot<O32>(b, na, k, e), k, pc);
-        if constexpr (two) fb[k] = P::Load(f, SwapSlot<O32>(b, nb, k, e), k, pc);
+#pragma unroll
+        for (int j = 0; j < G; j++) v[j][k] = P::Load(p[j], off(k), k, pc);
     }
     const bool fl = b.center_fluid != 0;
-    if (first) {
-        MomentsCollideT<L, T>(fa, pc, fl);
-        Rng ra = SeedRng(pc.seed, na);
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+        if (!valid[j]) continue;
+        MomentsCollideT<L, T>(v[j], pc, fl);
+        Rng rg = SeedRng(pc.seed, node[j]);
 #pragma unroll
         for (int k = 0; k < Q; k++)
-            P::Store(f, SwapSlot<O32>(b, na, k, GATHER && k != 0), k,
-                     fa[L::opp(k)], pc, ra);
-    }
-    if constexpr (two) {
-        if (!second) return;
-        MomentsCollideT<L, T>(fb, pc, fl);
-        Rng rb = SeedRng(pc.seed, nb);
-#pragma unroll
-        for (int k = 0; k < Q; k++)
-            P::Store(f, SwapSlot<O32>(b, nb, k, GATHER && k != 0), k,
-                     fb[L::opp(k)], pc, rb);
+            P::Store(p[j], off(k), k, v[j][L::opp(k)], pc, rg);
     }
 }
 
@@ -212,9 +217,8 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     }
     blk -= nsr;
     const int rows = ny * (b.n[2] - 2);
-    constexpr int pair = SplitPair<T>();
-    const int nbx2 = (b.n[0] + 2 * kSplitCta - 1) / (2 * kSplitCta);
-    const unsigned per_chunk = 1 + kSplitRows * (pair == 2 ? nbx2 : nbx);
+    constexpr int G = SplitGroup<T>();
+    const unsigned per_chunk = (unsigned)SplitChunkCtas<G>(b.n[0]);
     const int chunk = (int)(blk / per_chunk);
     const int w = (int)(blk % per_chunk);
     if (w == 0) {
@@ -226,25 +230,10 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                                 1 + r % ny, 1 + r / ny);
         return;
     }
-    if constexpr (pair == 2) {
-        // warp v of the CTA has [64 v, 64 v + 64) of the row's 256 nodes,
-        // lane l the nodes 64 v + l and 64 v + 32 + l
-        const int r = chunk * kSplitRows + (w - 1) / nbx2;
-        const int xa = ((w - 1) % nbx2) * 2 * kSplitCta +
-                       (threadIdx.x >> 5) * 64 + (threadIdx.x & 31);
-        const int xb = xa + 32;
-        const bool va = xa >= 1 && xa <= b.n[0] - 2;
-        const bool vb = xb >= 1 && xb <= b.n[0] - 2;
-        if (r >= rows || (!va && !vb)) return;
-        SwapInteriorPair<T, GATHER, O32>(b, pc, f, xa, xb, 1 + r % ny,
-                                         1 + r / ny, va, vb);
-    } else {
-        const int r = chunk * kSplitRows + (w - 1) / nbx;
-        const int x = ((w - 1) % nbx) * blockDim.x + threadIdx.x;
-        if (r >= rows || x < 1 || x > b.n[0] - 2) return;
-        SwapInteriorPair<T, GATHER, O32>(b, pc, f, x, x, 1 + r % ny,
-                                         1 + r / ny, true, false);
-    }
+    const SplitTask k = InteriorTask<G>(b, chunk, w);
+    if (k.r < 0 || k.r >= rows) return;
+    SwapInteriorGroup<T, GATHER, O32, G>(b, pc, f, k.x0, 1 + k.r % ny,
+                                         1 + k.r / ny);
 }
 
 }  // namespace mplb
