@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MPLBGPU_ABI_VERSION 2
+#define MPLBGPU_ABI_VERSION 3
 
 typedef int mplbgpu_status;
 enum {
@@ -112,6 +112,12 @@ enum {
 typedef struct {
     int id;       /* block id as given to DefineBlocks */
     int size[3];  /* nodes per axis; size[2] = 1 for 2D */
+    int cut;      /* bit s set: surface s (MPLBGPU_LEFT..MPLBGPU_BACK) is not
+                     a boundary but continues into a block held by another
+                     context (decomposition of one block over GPUs, the
+                     job OPS's MPI partition does for the reference); its
+                     halo layer is filled with mplbgpu_import_face.  0 for
+                     the reference's own blocks. */
 } mplbgpu_block;
 
 typedef struct {  /* one entry of DefineBlockConnection */
@@ -192,6 +198,34 @@ mplbgpu_status mplbgpu_download_macro(mplbgpu_ctx* ctx, int block,
                                       double* rho, double* u, double* v,
                                       double* w);
 mplbgpu_status mplbgpu_download_f(mplbgpu_ctx* ctx, int block, double* f);
+
+/* Decomposed blocks (cut faces).  Before each mplbgpu_step the caller moves,
+ * for every cut face, the populations leaving the neighbouring context's
+ * block through its opposite face into this block's halo layer:
+ *   mplbgpu_face_size   elements (and bytes per element, the storage form's)
+ *                       of one face buffer: the populations crossing the
+ *                       face, population-major, then the face's nodes with
+ *                       the lower in-plane axis fastest;
+ *   mplbgpu_export_face the populations leaving through `surface` from the
+ *                       block's layer next to it, into device buffer `buf`;
+ *   mplbgpu_import_face `buf` (the neighbour's export through the opposite
+ *                       face) into the halo layer beyond `surface`.
+ * Both run on the context's stream (mplbgpu_synchronize before handing the
+ * buffer to another stream).  A block split into slabs this way steps bit
+ * for bit as the whole block does. */
+mplbgpu_status mplbgpu_face_size(mplbgpu_ctx* ctx, int block, int surface,
+                                 long long* elems, int* elem_bytes);
+mplbgpu_status mplbgpu_export_face(mplbgpu_ctx* ctx, int block, int surface,
+                                   void* buf);
+mplbgpu_status mplbgpu_import_face(mplbgpu_ctx* ctx, int block, int surface,
+                                   const void* buf);
+
+/* The residual's sums over this context's nodes (CalcResidualError before
+ * the division, Src/flowfield_wrapper.cpp:31-89): per variable
+ * diff = sum((q - q_old)^2) and sum = sum(q^2) (space_dim + 1 entries
+ * each); q_old becomes q.  Decomposed runs add them over contexts. */
+mplbgpu_status mplbgpu_residual_sums(mplbgpu_ctx* ctx, double* diff,
+                                     double* sum);
 
 /* FP64 sum of rho over all nodes of all blocks, from the current f. */
 mplbgpu_status mplbgpu_mass(mplbgpu_ctx* ctx, double* mass);

@@ -7,7 +7,7 @@ missing or unloadable library raises ``NativeLibraryError``.
 import ctypes
 import os
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 ERR_INVALID = 1
@@ -62,7 +62,8 @@ SCHEMES = {"Scheme_StreamCollision": SCHEME_STREAM_COLLISION,
 
 
 class Block(ctypes.Structure):
-    _fields_ = [("id", ctypes.c_int), ("size", ctypes.c_int * 3)]
+    _fields_ = [("id", ctypes.c_int), ("size", ctypes.c_int * 3),
+                ("cut", ctypes.c_int)]
 
 
 class Connection(ctypes.Structure):
@@ -130,6 +131,15 @@ _SIGNATURES = {
     "mplbgpu_download_f": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_void_p]),
     "mplbgpu_mass": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mplbgpu_face_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    "mplbgpu_export_face": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_void_p]),
+    "mplbgpu_import_face": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_void_p]),
+    "mplbgpu_residual_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p]),
     "mplbgpu_check_health": (ctypes.c_int, [ctypes.c_void_p]),
     "mplbgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "mplbgpu_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),

@@ -71,6 +71,9 @@ class CaseConfig:
     steps: int = 0
     precision: str = "fp64"
     scheme: str = "Scheme_StreamCollision"
+    # decomposition (not part of the reference's JSON): per block id, bit s
+    # set when surface s is cut, i.e. continues in another context
+    cuts: Optional[Dict[int, int]] = None
 
     @property
     def swap(self) -> bool:
@@ -252,6 +255,7 @@ class CaseConfig:
             blocks[i].size[0] = s[0]
             blocks[i].size[1] = s[1]
             blocks[i].size[2] = s[2] if len(s) > 2 else 1
+            blocks[i].cut = (self.cuts or {}).get(bid, 0)
         nc = len(self.connections)
         conns = (abi.Connection * max(nc, 1))()
         for i, c in enumerate(self.connections):

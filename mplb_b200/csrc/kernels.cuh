@@ -1197,6 +1197,40 @@ __global__ void HaloKernel(HaloDev h, BlockDev fb, BlockDev tb,
 // Residual sums of one macroscopic variable over one block, per CTA:
 // sum (q - q_old)^2 and sum q^2 (KerCalcMacroVarSquareofDifference /
 // KerCalcMacroVarSquare, Src/flowfield_kernel.inc:131-153); q_old <- q.
+// Face exchange of a decomposed block (cut faces): element t of the face
+// buffer is population pop[t / (nu nv)] of the face node (u, v) =
+// (t % nu, (t / nu) % nv) on layer `layer` of the face's axis (the block's
+// own boundary layer for an export, the halo layer -1 or n for an import).
+struct FaceDev {
+    int axis, layer;
+    int ua, va;          // in-plane axes (va = -1 in 2D)
+    int nu, nv;
+    int npop;
+    int pop[kMaxQ];
+};
+
+template <int D, typename T, bool EXPORT>
+__global__ void __launch_bounds__(256)
+    FaceKernel(BlockDev b, FaceDev fd, T* __restrict__ f,
+               T* __restrict__ buf) {
+    const long long total = (long long)fd.npop * fd.nu * fd.nv;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+         t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int u = (int)(t % fd.nu);
+        const long long r = t / fd.nu;
+        const int v = (int)(r % fd.nv);
+        const int p = (int)(r / fd.nv);
+        int c[3] = {0, 0, 0};
+        c[fd.axis] = fd.layer;
+        c[fd.ua] = u;
+        if (fd.va >= 0) c[fd.va] = v;
+        const long long e = (long long)fd.pop[p] * b.popstride +
+                            NodeIndex<D>(b, c[0], c[1], c[2]);
+        if (EXPORT) buf[t] = f[e];
+        else f[e] = buf[t];
+    }
+}
+
 __global__ void ResidualPartialKernel(const double* __restrict__ q,
                                       double* __restrict__ qold, long long n,
                                       double* __restrict__ part);

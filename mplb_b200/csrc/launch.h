@@ -38,6 +38,10 @@ struct Launch {
     static cudaError_t Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
                             const BlockDev& fb, const BlockDev& tb,
                             const T* cur_from, const T* prev_from, T* cur_to);
+    // face exchange of a decomposed block: export (block -> buf) or import
+    static cudaError_t Face(bool exp, unsigned grid, cudaStream_t s,
+                            const BlockDev& b, const FaceDev& fd, T* f,
+                            T* buf);
     // swap scheme (3D only): one step (kModeStep) or an observation of the
     // current f, from the array in place; gather: slots at their streamed
     // places; bc: boundary programme pending

@@ -115,6 +115,17 @@ cudaError_t Launch<D, T>::DirectObserve(int mode, dim3 grid, cudaStream_t s,
 }
 
 template <int D, typename T>
+cudaError_t Launch<D, T>::Face(bool exp, unsigned grid, cudaStream_t s,
+                               const BlockDev& b, const FaceDev& fd, T* f,
+                               T* buf) {
+    if (exp)
+        FaceKernel<D, T, true><<<grid, 256, 0, s>>>(b, fd, f, buf);
+    else
+        FaceKernel<D, T, false><<<grid, 256, 0, s>>>(b, fd, f, buf);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
 cudaError_t Launch<D, T>::Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
                                const BlockDev& fb, const BlockDev& tb,
                                const T* cur_from, const T* prev_from,

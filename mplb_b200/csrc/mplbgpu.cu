@@ -318,6 +318,56 @@ int InitBlock(mplbgpu_ctx* ctx, size_t bi, const double* d_rho,
     return MPLBGPU_OK;
 }
 
+// Face of a decomposed block: the populations crossing it and the layer.
+int FaceSetup(mplbgpu_ctx* ctx, int block, int surface, bool exp,
+                     size_t* bi, FaceDev* fd) {
+    const BlockPlan* B = FindPlan(ctx, block);
+    if (!B) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    const int dim = ctx->plan.dim;
+    if (surface < 0 || surface >= 2 * dim || !(B->cut >> surface & 1))
+        return SetErr(ctx, MPLBGPU_ERR_INVALID,
+                      "surface is not a cut face of the block");
+    static const int axis_of[6] = {0, 0, 1, 1, 2, 2};
+    static const int side_of[6] = {0, 1, 1, 0, 1, 0};   // 1: max face
+    const int a = axis_of[surface], side = side_of[surface];
+    *bi = (size_t)B->index;
+    FaceDev& f = *fd;
+    f = FaceDev{};
+    f.axis = a;
+    f.layer = exp ? (side ? B->n[a] - 1 : 0) : (side ? B->n[a] : -1);
+    f.ua = f.va = -1;
+    for (int q = 0; q < dim; q++) {
+        if (q == a) continue;
+        if (f.ua < 0) f.ua = q;
+        else f.va = q;
+    }
+    f.nu = B->n[f.ua];
+    f.nv = f.va >= 0 ? B->n[f.va] : 1;
+    // leaving through the face (export) = entering the neighbour's halo
+    // through its opposite face (import): c_a = +1 across a max face
+    const int c_out = side ? 1 : -1;
+    const int want = exp ? c_out : -c_out;
+    f.npop = 0;
+    for (int i = 0; i < ctx->plan.Q; i++) {
+        const int c = dim == 3 ? comp<Lattice<3>>(i, a) : comp<Lattice<2>>(i, a);
+        if (c == want) f.pop[f.npop++] = i;
+    }
+    return MPLBGPU_OK;
+}
+
+template <int D, typename T>
+int FaceCopy(mplbgpu_ctx* ctx, size_t bi, const FaceDev& fd, bool exp,
+                    void* buf) {
+    DevBlock& b = ctx->blocks[bi];
+    const long long total = (long long)fd.npop * fd.nu * fd.nv;
+    const unsigned grid =
+        (unsigned)std::min<long long>((total + 255) / 256, 4096);
+    CK_LAUNCH_E(Launch<D, T>::Face(exp, grid, ctx->stream, b.dev, fd,
+                                   static_cast<T*>(b.pop[ctx->cur]),
+                                   static_cast<T*>(buf)));
+    return MPLBGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -663,13 +713,11 @@ mplbgpu_status mplbgpu_update_macro(mplbgpu_ctx* ctx) {
     return MPLBGPU_OK;
 }
 
-mplbgpu_status mplbgpu_residual(mplbgpu_ctx* ctx, int check_period,
-                                double* per_var, double* max_residual) {
-    if (!ctx) return MPLBGPU_ERR_INVALID;
-    if (check_period <= 0)
-        return SetErr(ctx, MPLBGPU_ERR_INVALID, "check_period must be > 0");
+mplbgpu_status mplbgpu_residual_sums(mplbgpu_ctx* ctx, double* diff,
+                                     double* sum) {
+    if (!ctx || !diff || !sum) return MPLBGPU_ERR_INVALID;
     const int nv = ctx->plan.dim + 1;
-    double diff[4] = {0, 0, 0, 0}, sum[4] = {0, 0, 0, 0};
+    for (int m = 0; m < nv; m++) diff[m] = sum[m] = 0.0;
     std::vector<double> part(2 * kRedBlocks);
     for (int m = 0; m < nv; m++) {
         for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
@@ -688,6 +736,18 @@ mplbgpu_status mplbgpu_residual(mplbgpu_ctx* ctx, int check_period,
             }
         }
     }
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_residual(mplbgpu_ctx* ctx, int check_period,
+                                double* per_var, double* max_residual) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    if (check_period <= 0)
+        return SetErr(ctx, MPLBGPU_ERR_INVALID, "check_period must be > 0");
+    const int nv = ctx->plan.dim + 1;
+    double diff[4] = {0, 0, 0, 0}, sum[4] = {0, 0, 0, 0};
+    int rc = mplbgpu_residual_sums(ctx, diff, sum);
+    if (rc != MPLBGPU_OK) return rc;
     // GetMaximumResidual, Src/flowfield.cpp:148-158
     double mx = 0;
     for (int m = 0; m < nv; m++) {
@@ -735,6 +795,45 @@ mplbgpu_status mplbgpu_download_f(mplbgpu_ctx* ctx, int block, double* f) {
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_face_size(mplbgpu_ctx* ctx, int block, int surface,
+                                 long long* elems, int* elem_bytes) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    size_t bi;
+    FaceDev fd;
+    int rc = FaceSetup(ctx, block, surface, true, &bi, &fd);
+    if (rc != MPLBGPU_OK) return rc;
+    if (elems) *elems = (long long)fd.npop * fd.nu * fd.nv;
+    if (elem_bytes) *elem_bytes = ctx->plan.elem_bytes;
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_export_face(mplbgpu_ctx* ctx, int block, int surface,
+                                   void* buf) {
+    if (!ctx || !buf) return ctx ? SetErr(ctx, MPLBGPU_ERR_INVALID, "null buffer")
+                                 : MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    size_t bi;
+    FaceDev fd;
+    rc = FaceSetup(ctx, block, surface, true, &bi, &fd);
+    if (rc != MPLBGPU_OK) return rc;
+    return MPLB_DISPATCH(ctx, FaceCopy, ctx, bi, fd, true, buf);
+}
+
+mplbgpu_status mplbgpu_import_face(mplbgpu_ctx* ctx, int block, int surface,
+                                   const void* buf) {
+    if (!ctx || !buf) return ctx ? SetErr(ctx, MPLBGPU_ERR_INVALID, "null buffer")
+                                 : MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    size_t bi;
+    FaceDev fd;
+    rc = FaceSetup(ctx, block, surface, false, &bi, &fd);
+    if (rc != MPLBGPU_OK) return rc;
+    return MPLB_DISPATCH(ctx, FaceCopy, ctx, bi, fd, false,
+                         const_cast<void*>(buf));
 }
 
 static int SumRho(mplbgpu_ctx* ctx, double* total, unsigned long long* nbad) {

@@ -156,16 +156,27 @@ bool InRange(const int p[3], const int r[6]) {
            p[2] >= r[4] && p[2] < r[5];
 }
 
+// Surface (BoundarySurface) of the min (side 0) or max (side 1) face of an
+// axis.
+int FaceSurface(int axis, int side) {
+    static const int tab[3][2] = {{MPLBGPU_LEFT, MPLBGPU_RIGHT},
+                                  {MPLBGPU_BOTTOM, MPLBGPU_TOP},
+                                  {MPLBGPU_BACK, MPLBGPU_FRONT}};
+    return tab[axis][side];
+}
+
 // Boundary faces of a node: axes on which it is the first/last node, with
-// the inward sign (+1 on the first node: the "P" codes).
+// the inward sign (+1 on the first node: the "P" codes).  Faces in `cut`
+// (bit s: surface s continues into a block of another context) are not
+// boundaries: the node is interior there.
 int NodeFaces(int dim, const int n[3], const int p[3], int axis[3],
-              int sign[3]) {
+              int sign[3], int cut = 0) {
     int k = 0;
     for (int a = 0; a < dim; a++) {
-        if (p[a] == 0) {
+        if (p[a] == 0 && !(cut >> FaceSurface(a, 0) & 1)) {
             axis[k] = a;
             sign[k++] = 1;
-        } else if (p[a] == n[a] - 1) {
+        } else if (p[a] == n[a] - 1 && !(cut >> FaceSurface(a, 1) & 1)) {
             axis[k] = a;
             sign[k++] = -1;
         }
@@ -175,9 +186,9 @@ int NodeFaces(int dim, const int n[3], const int p[3], int axis[3],
 
 // VertexGeometryType of a node from its position: the code written last by
 // SetBlockGeometryProperty (Src/flowfield_wrapper.cpp:291-623).
-int GeometryCode(int dim, const int n[3], const int p[3]) {
+int GeometryCode(int dim, const int n[3], const int p[3], int cut = 0) {
     int axis[3], sign[3];
-    const int k = NodeFaces(dim, n, p, axis, sign);
+    const int k = NodeFaces(dim, n, p, axis, sign, cut);
     auto face = [](int a, int s) { return 10 * (a + 1) + (s > 0 ? 0 : 1); };
     if (k == 0) return 0;
     if (k == 1) return face(axis[0], sign[0]);
@@ -533,6 +544,16 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
         const mplbgpu_block& src = d.blocks[order[i]];
         B.id = src.id;
         B.index = i;
+        B.cut = src.cut;
+        if (B.cut != 0) {
+            if (B.cut & ~((1 << (2 * P.dim)) - 1))
+                return fail(MPLBGPU_ERR_INVALID,
+                            "cut faces outside the block's dimension");
+            if (d.nconnections != 0 || swap)
+                return fail(MPLBGPU_ERR_UNSUPPORTED,
+                            "decomposed (cut) blocks take no connections "
+                            "and the two-array scheme");
+        }
         for (int a = 0; a < 3; a++) {
             B.n[a] = a < P.dim ? src.size[a] : 1;
             if (a < P.dim && B.n[a] < 2)
@@ -573,6 +594,15 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
             if (SurfaceFaces(bc.surface, sa, ss) < 1)
                 return fail(MPLBGPU_ERR_INVALID, "bad bounce-back surface");
         }
+        {
+            const int cut = P.blocks[blockIndex(bc.block)].cut;
+            int sa[2], ss[2];
+            const int nsf = SurfaceFaces(bc.surface, sa, ss);
+            for (int q = 0; q < nsf; q++)
+                if (cut >> FaceSurface(sa[q], ss[q]) & 1)
+                    return fail(MPLBGPU_ERR_INVALID,
+                                "boundary condition on a cut face");
+        }
     }
 
     // regions
@@ -606,7 +636,9 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
             // SetBoundaryNodeType, Src/flowfield_wrapper.cpp:625-788)
             bool bulk = true;
             for (int a = 0; a < P.dim; a++)
-                bulk = bulk && p[a] >= 1 && p[a] < B.n[a] - 1;
+                bulk = bulk &&
+                       (p[a] >= 1 || (B.cut >> FaceSurface(a, 0) & 1)) &&
+                       (p[a] < B.n[a] - 1 || (B.cut >> FaceSurface(a, 1) & 1));
             int vt = bulk ? kVtFluid : 0;
             for (int k = 0; k < d.nboundaries; k++) {
                 const mplbgpu_boundary& bc = d.boundaries[k];
@@ -631,10 +663,10 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                 if (InRange(p, rg)) vt = bc.vertex_type;
             }
             R.vt = vt;
-            R.vg = GeometryCode(P.dim, B.n, p);
+            R.vg = GeometryCode(P.dim, B.n, p, B.cut);
             R.fluidlike = FluidLike(vt) ? 1 : 0;
             int axis[3], sign[3];
-            const int nf = NodeFaces(P.dim, B.n, p, axis, sign);
+            const int nf = NodeFaces(P.dim, B.n, p, axis, sign, B.cut);
             // KerStream3D selection, Src/scheme_kernel.inc:1400-2051
             uint32_t pull = 0;
             for (int l = 0; l < P.Q; l++) {
@@ -742,7 +774,8 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                     const RegionInfo& R = B.region[r];
                     if (R.cls != kDeferred || !InRange(R.org, rg)) continue;
                     int axis[3], sign[3];
-                    const int nf = NodeFaces(P.dim, B.n, R.org, axis, sign);
+                    const int nf =
+                        NodeFaces(P.dim, B.n, R.org, axis, sign, B.cut);
                     RegionOp op;
                     if (bc.scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL)
                         op = MakeEqm(L, P.cs, nf, axis, sign, bc.given);

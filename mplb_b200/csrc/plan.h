@@ -82,6 +82,7 @@ struct DeferredOp {     // one boundary (definition order) on deferred nodes
 struct BlockPlan {
     int id;
     int index;          // position in id order
+    int cut;            // bit s: surface s continues in another context
     int n[3];
     int xoff;           // element index of x = 0 inside a row
     long long pitch;    // elements per row
