@@ -345,6 +345,9 @@ int lbmo_create(const mplbgpu_desc* d, lbm_oracle** out) {
           (d->space_dim == 3 && d->lattice == MPLBGPU_D3Q19)))
         return fail("lattice/dimension");
     if (d->nblocks < 1) return fail("no blocks");
+    for (int i = 0; i < d->nblocks; i++)
+        if (d->blocks[i].cut != 0)
+            return fail("decomposed (cut) blocks are not restated here");
     lbm_oracle* o = (lbm_oracle*)calloc(1, sizeof(lbm_oracle));
     o->dim = d->space_dim;
     o->Q = d->lattice;
