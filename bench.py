@@ -27,6 +27,7 @@ from its own sources against the sequential OPS stand-in, OpenMP over all
 host cores) on the same workload instead.
 """
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -70,6 +71,11 @@ def parse():
                         "cavities split over the ranks; cavities-warmstart: "
                         "the learned warm start experiment (minutes; 1 GPU)")
     p.add_argument("--epochs", type=int, default=200)
+    p.add_argument("--decomp", default="replicas",
+                   choices=["replicas", "slab"],
+                   help="N > 1 on the cavity: independent 256^3 replicas, or "
+                        "one 256 x 256 x 256N cavity cut into z slabs with "
+                        "a face exchange (NCCL) before every step")
     p.add_argument("--scheme", default="stream", choices=["stream", "swap"],
                    help="swap: the reference's one-array swap step "
                         "(Scheme_StreamCollision_Swap), half the memory")
@@ -322,6 +328,116 @@ def run_warmstart(args, rank, local):
     print(json.dumps(line))
 
 
+def run_slab(args, rank, world, local):
+    """One 256 x 256 x 256N cavity cut into N z slabs, one per GPU (weak
+    scaling: 256^3 nodes per GPU); before every step each rank exports the
+    populations leaving its slab through each cut face and swaps them with
+    its neighbour (NCCL send/recv), then imports the neighbour's into its
+    halo.  Timed on the device over the K steps including the exchanges,
+    max over ranks."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from mplb_b200 import config, slab
+    torch.cuda.set_device(local)
+    n = args.size
+    case = config.cavity(3, n, 0.05, re=400, precision=args.precision)
+    case = dataclasses.replace(case, block_sizes=[(n, n, n * world)])
+    group = None
+    if world > 1:
+        group = dist.new_group(backend="nccl",
+                               timeout=datetime.timedelta(seconds=300))
+    s = slab.SlabSolver(case, world, [rank],
+                        slab.DistExchange(group) if world > 1
+                        else slab.LocalExchange())
+    part = s.parts[0]
+    nodes = case.nodes()
+    local_nodes = slab.slab_case(case, world, rank).nodes()
+    s.init_uniform()
+    s.stream_collision(args.warmup)
+    part.synchronize()
+    launches0 = part.solver.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    s.stream_collision(args.steps)
+    part.synchronize()
+    ev1.record()
+    ev1.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = part.solver.launch_count() - launches0
+    ms_max = max_over_ranks(ms, world)
+    value = nodes * args.steps / (ms_max * 1e-3) / 1e6
+    step_kernel_ms = part.solver.last_step_ms()   # the last step's kernel
+    bpn = BYTES_PER_NODE[(case.precision, 3)]
+    achieved = bpn * local_nodes / (step_kernel_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    # end to end: initial fields from pinned host memory, K steps, moments
+    # back to pinned host memory
+    shp = slab.slab_case(case, world, rank).size3(0)[::-1]
+    pinned = [torch.empty(shp, dtype=torch.float64, pin_memory=True)
+              for _ in range(8)]
+    pinned[0].fill_(1.0)
+    for t in pinned[1:4]:
+        t.zero_()
+    lib = part.lib
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ptr = [t.data_ptr() for t in pinned]
+    part._check(lib.mplbgpu_init_macro(part.solver.h, 0, *ptr[:4]))
+    s.stream_collision(args.steps)
+    s.update_macro_vars()
+    part._check(lib.mplbgpu_download_macro(part.solver.h, 0, *ptr[4:]))
+    t1 = time.perf_counter()
+    barrier(world)
+    e2e_s = max_over_ranks(t1 - t0, world)
+    e2e = nodes * args.steps / e2e_s / 1e6
+    ok = bool(np.isfinite(float(pinned[4].sum())))
+    s.close()
+    if group is not None:
+        dist.destroy_process_group(group)
+    if not ok:
+        raise RuntimeError("non-finite density after the slab run")
+    if rank != 0:
+        return
+    face = 5 * n * n * (8 if case.precision == "fp64" else
+                        4 if case.precision == "fp32" else 2)
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPES[args.precision], "data": "synthetic",
+        "config": {"workload": f"3D lid-driven cavity D3Q19 {n} x {n} x "
+                               f"{n * world} {args.precision.upper()}, lid "
+                               "0.05 (lattice), Re 400, z slabs of "
+                               f"{n}^3 per GPU",
+                   "nodes_per_gpu": local_nodes,
+                   "parallelism": f"slab{world}",
+                   "exchange_bytes_per_step_per_cut": 2 * face,
+                   "l2": "population arrays larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_node": bpn,
+                     "traffic": None},
+        "e2e": {"value": e2e, "unit": "MLUPS",
+                "h2d_bytes_per_step": 4 * 8 * nodes / args.steps,
+                "d2h_bytes_per_step": 4 * 8 * nodes / args.steps},
+        "cpu_baseline": None,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args)
@@ -337,6 +453,9 @@ def main():
         return
     if args.workload == "cavities-warmstart":
         run_warmstart(args, rank, local)
+        return
+    if args.decomp == "slab" and args.workload == "cavity3d":
+        run_slab(args, rank, world, local)
         return
     if args.workload == "cavities":
         run_cavities(args, rank, world, local)
