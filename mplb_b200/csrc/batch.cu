@@ -164,9 +164,11 @@ int Grid(mplbgpu_batch* b, bool persistent) {
     if (persistent) {
         int maxres = 1;
         if (b->precision == MPLBGPU_FP64)
-            BatchLaunch<double>::MaxCoResident(b->tune.tile_nodes, &maxres);
+            BatchLaunch<double>::MaxCoResident(
+                b->tune.tile_nodes / BatchNodesPerThread<double>(), &maxres);
         else
-            BatchLaunch<float>::MaxCoResident(b->tune.tile_nodes, &maxres);
+            BatchLaunch<float>::MaxCoResident(
+                b->tune.tile_nodes / BatchNodesPerThread<float>(), &maxres);
         per = std::min(per, std::max(1, maxres));
     }
     return sms * per;
@@ -177,7 +179,7 @@ int LaunchChunk(mplbgpu_batch* b, int nsteps, bool macro_last) {
     const BatchDev d = MakeDev(b);
     T* P0 = static_cast<T*>(b->pop[0]);
     T* P1 = static_cast<T*>(b->pop[1]);
-    const int threads = b->tune.tile_nodes;
+    const int threads = b->tune.tile_nodes / BatchNodesPerThread<T>();
     if (b->tune.persistent) {
         const GridSync gs{b->sync_count, b->sync_gen, b->sync_err,
                           (long long)1 << 26};

@@ -93,6 +93,71 @@ __device__ __forceinline__ void BatchNode(const BatchDev& bd,
     }
 }
 
+// Two nodes of one cavity per thread, 32 apart (the FP32 form): both nodes'
+// loads are issued before either is computed, and each warp access covers
+// 256 contiguous bytes instead of 128.  Node kb is skipped when it lies
+// beyond the cavity (its loads then repeat node ka's).
+template <typename T, bool MACRO>
+__device__ __forceinline__ void BatchNodePair(const BatchDev& bd,
+                                              const PhysConst& pc,
+                                              const BatchCav& cv, int ka,
+                                              bool second,
+                                              const T* __restrict__ src,
+                                              T* __restrict__ dst) {
+    using L = Lattice<2>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int Q = 9;
+    const int n = cv.n;
+    const int nn = n * n;   // a cavity's populations fit in 32-bit offsets
+    const int kk[2] = {ka, second ? ka + 32 : ka};
+    const T* s = src + cv.base;
+    T* d = dst + cv.base;
+    C f[2][Q];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int k = kk[j];
+        const int y = n <= 1024 ? (int)(((float)k + 0.5f) * cv.ninv) : k / n;
+        const int x = k - y * n;
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const int sx = x - L::cx(i), sy = y - L::cy(i);
+            if (sx >= 0 && sx < n && sy >= 0 && sy < n) {
+                f[j][i] = P::Load(s, i * nn + sy * n + sx, i, pc);
+            } else {
+                C b = (C)0;
+                if (sy > n - 1) {
+                    if constexpr (P::kShifted) b = cv.lidbf[i];
+                    else b = cv.lidb[i];
+                }
+                f[j][i] = P::Load(s, L::opp(i) * nn + k, L::opp(i), pc) + b;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if (j == 1 && !second) break;
+        const int k = kk[j];
+        double rho, u[3];
+        MomentsCollideT<L, T>(f[j], pc, false, cv.omc, cv.omcf, rho, u);
+        Rng rng = SeedRng(pc.seed, cv.base + k);
+#pragma unroll
+        for (int i = 0; i < Q; i++) P::Store(d, i * nn + k, i, f[j][i], pc, rng);
+        if (MACRO) {
+            bd.macro[0][cv.mbase + k] = rho;
+            bd.macro[1][cv.mbase + k] = u[0];
+            bd.macro[2][cv.mbase + k] = u[1];
+        }
+    }
+}
+
+// Threads per CTA of the step kernels for a tile of `tile_nodes` nodes:
+// two nodes per thread in the FP32 form.
+template <typename T>
+__host__ __device__ constexpr int BatchNodesPerThread() {
+    return sizeof(T) < 8 ? 2 : 1;
+}
+
 template <typename T, bool MACRO>
 __device__ __forceinline__ void BatchSweep(const BatchDev& bd,
                                            const PhysConst& pc,
@@ -102,8 +167,19 @@ __device__ __forceinline__ void BatchSweep(const BatchDev& bd,
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int2 tile = bd.tiles[t];
         const BatchCav& cv = bd.cavs[tile.x];
-        const int k = tile.y + threadIdx.x;
-        if (k < cv.n * cv.n) BatchNode<T, MACRO>(bd, pc, cv, k, src, dst);
+        if constexpr (BatchNodesPerThread<T>() == 2) {
+            // warp w has nodes [64 w, 64 w + 64) of the tile, lane l the
+            // nodes 64 w + l and 64 w + 32 + l
+            const int ka = tile.y + (int)(threadIdx.x >> 5) * 64 +
+                           (int)(threadIdx.x & 31);
+            const int nn = cv.n * cv.n;
+            if (ka < nn)
+                BatchNodePair<T, MACRO>(bd, pc, cv, ka, ka + 32 < nn, src,
+                                        dst);
+        } else {
+            const int k = tile.y + threadIdx.x;
+            if (k < cv.n * cv.n) BatchNode<T, MACRO>(bd, pc, cv, k, src, dst);
+        }
     }
 }
 
