@@ -133,16 +133,22 @@ class Oracle:
         return vt, vg
 
 
-def run_reference(case, steps, kind="", workdir=None, program="ref_case"):
+def run_reference(case, steps, kind="", workdir=None, program="ref_case",
+                  json_path=None):
     """Runs oracle/_ref/{program}_{2d,3d}{kind}; returns dict with macro
     arrays per block, f per block and the residual history.  program
     "dropin_case" is the same driver with the B200 drop-in glue in place of
-    the reference's step."""
+    the reference's step.  json_path: run that case file as it is (the
+    reference's own JSON reader parses it) instead of case.to_json()."""
     exe = os.path.join(REF_DIR, f"{program}_{case.space_dim}d{kind}")
     tmp = workdir or tempfile.mkdtemp(prefix="mplbref_")
     cfg = os.path.join(tmp, "case.json")
-    with open(cfg, "w") as fh:
-        json.dump(case.to_json(), fh)
+    if json_path is not None:
+        with open(json_path) as src, open(cfg, "w") as fh:
+            fh.write(src.read())
+    else:
+        with open(cfg, "w") as fh:
+            json.dump(case.to_json(), fh)
     env = dict(os.environ, OPS_SHIM_QUIET="1")
     subprocess.run([exe, cfg, tmp, str(steps)], check=True, env=env)
     names = ["rho", "u", "v", "w"][:case.space_dim + 1]

@@ -32,3 +32,28 @@ def load(name):
         out["macro"][b] = [z[f"{n}_b{b}"] for n in vars_]
         out["f"][b] = z[f"f_b{b}"]
     return out
+
+
+def apps():
+    """The reference's own app case files, parsed and fingerprinted (made by
+    tests/golden/make_golden_apps.py): name -> (case, steps, digests)."""
+    with open(os.path.join(GOLDEN, "apps.json")) as fh:
+        d = json.load(fh)
+    return {k: (CaseConfig.from_json(v["case_json"]), v["steps"], v["digest"])
+            for k, v in d.items()}
+
+
+def fingerprint(case, f_of, macro_of):
+    """SHA-256 digests in the layout of make_golden_apps.fingerprint."""
+    import hashlib
+    names = ["rho", "u", "v", "w"][:case.space_dim + 1]
+
+    def dig(a):
+        return hashlib.sha256(np.ascontiguousarray(a, "<f8").tobytes()
+                              ).hexdigest()
+    out = {}
+    for b in case.block_ids:
+        out[f"f_b{b}"] = dig(f_of(b))
+        for n, a in zip(names, macro_of(b)):
+            out[f"{n}_b{b}"] = dig(a)
+    return out

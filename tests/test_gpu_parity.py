@@ -134,3 +134,16 @@ def test_divergence_is_detected(gpu_lib):
     s.upload_f(0, f)
     s.stream_collision(2)
     assert s.check_health() == abi.ERR_DIVERGED
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.apps()))
+def test_gpu_matches_reference_app_files(gpu_lib, name):
+    """The reference's own case files (Apps/*/*.json) through the JSON front
+    end on the GPU: bit for bit the reference's run of the file."""
+    case, steps, want = golden_cases.apps()[name]
+    s = Solver(case)
+    s.init_uniform()
+    s.stream_collision(steps)
+    s.update_macro_vars()
+    assert golden_cases.fingerprint(case, s.f, s.macro) == want
+    s.close()

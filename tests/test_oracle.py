@@ -134,3 +134,16 @@ def test_oracle_rejects_swap_outside_its_scope(oracle_mod):
     for case in bad:
         with pytest.raises(ValueError):
             oracle_mod.Oracle(case)
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.apps()))
+def test_oracle_matches_reference_app_files(oracle_mod, name):
+    """The reference's own case files (Apps/*/*.json), parsed by the JSON
+    front end: the oracle reproduces the reference's run of the file bit
+    for bit (digests of every block's f and moments)."""
+    case, steps, want = golden_cases.apps()[name]
+    o = oracle_mod.Oracle(case)
+    o.init_uniform()
+    o.step(steps)
+    o.update_macro()
+    assert golden_cases.fingerprint(case, o.f, o.macro) == want
