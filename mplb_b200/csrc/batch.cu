@@ -414,7 +414,8 @@ mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
     for (int i = 0; i < 9; i++) {
         pc.w[i] = w[L::wclass(i)];
         pc.wf[i] = (float)pc.w[i];
-        pc.winvf[i] = (float)(1.0 / pc.w[i]);
+        pc.winvf[i] = (float)(kHalfScale / pc.w[i]);
+        pc.wlf[i] = (float)(pc.w[i] / kHalfScale);
     }
     pc.seed = 1;
     if (BuildTiles(b) != MPLBGPU_OK) {

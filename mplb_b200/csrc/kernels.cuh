@@ -53,7 +53,8 @@ struct PhysConst {
     float tw_omf;        // tau omega / omega: the force term relative to
                          // the relaxation rate
     float wf[kMaxQ];
-    float winvf[kMaxQ];  // 1 / w_i
+    float winvf[kMaxQ];  // FP16 store scale kHalfScale / w_i
+    float wlf[kMaxQ];    // FP16 load scale w_i / kHalfScale
     uint32_t seed;       // per launch (FP16 stochastic rounding)
 };
 
@@ -148,14 +149,22 @@ struct Prec<float> {
     }
 };
 
-// FP16 stores round stochastically: the 13 float mantissa bits that FP16
-// drops are compared with a random draw, so increments far below one FP16
-// unit - a small body force per step - survive in expectation instead of
-// being rounded away every step.  Draws come from a per-thread xorshift32
-// generator seeded by hashing the node index with the step number.
+// FP16 stores round stochastically: 13 random bits are added to the 13
+// float mantissa bits that FP16 drops before truncating, so increments far
+// below one FP16 unit - a small body force per step - survive in
+// expectation instead of being rounded away every step.  The stored value
+// is kHalfScale h_i / w_i: h_i / w_i = f_i / w_i - 1 lies in [-1, 255)
+// for any population within 256 times its weight (a lattice Boltzmann state
+// stays within a few times it), so the scaled value stays in FP16's range
+// while values down to |h / w| = 2^-22 stay normal - the draw is added at the right bit
+// without testing for FP16 subnormals (below that the rounding is plain
+// truncation, 2^-32 in h / w).  Draws: one 32-bit hash of (node, step)
+// per node, and for population i the top 13 bits of its product with an
+// odd constant (a bijection of the hash, so each draw is uniform).
+constexpr float kHalfScale = 256.0f;
+
 struct Rng {
     uint32_t s;
-    uint32_t word;
 };
 
 __device__ __forceinline__ Rng SeedRng(uint32_t seed, long long node) {
@@ -166,27 +175,18 @@ __device__ __forceinline__ Rng SeedRng(uint32_t seed, long long node) {
     k ^= k >> 15;
     k *= 0x846ca68bu;
     k ^= k >> 16;
-    return Rng{k | 1u, 0u};
+    return Rng{k};
 }
 
 // 13 random bits for population i, aligned with the 13 mantissa bits that
-// FP16 drops (one xorshift32 step serves two populations).
-__device__ __forceinline__ uint32_t SrDraw(Rng& g, int i) {
-    if ((i & 1) == 0) {
-        g.s ^= g.s << 13;
-        g.s ^= g.s >> 17;
-        g.s ^= g.s << 5;
-        g.word = g.s;
-    }
-    return (i & 1) ? (g.word >> 19) : (g.word & 0x1fffu);
+// FP16 drops.
+__device__ __forceinline__ uint32_t SrDraw(const Rng& g, int i) {
+    const uint32_t m = 0x9e3779b1u * (uint32_t)(2 * i + 1) | 1u;
+    return (g.s * m) >> 19;
 }
 
 __device__ __forceinline__ __half StochasticHalf(float v, uint32_t r) {
-    const uint32_t bits = __float_as_uint(v);
-    // normal FP16 range (|v| >= 2^-14; stored values stay far below 65504);
-    // smaller values round to nearest
-    if (((bits >> 23) & 0xffu) < 113u) return __float2half_rn(v);
-    return __float2half_rz(__uint_as_float(bits + r));
+    return __float2half_rz(__uint_as_float(__float_as_uint(v) + r));
 }
 
 template <>
@@ -195,7 +195,7 @@ struct Prec<__half> {
     static constexpr bool kShifted = true;
     __device__ static __forceinline__ C Load(const __half* p, long long k,
                                              int i, const PhysConst& pc) {
-        return __half2float(p[k]) * pc.wf[i];
+        return __half2float(p[k]) * pc.wlf[i];
     }
     __device__ static __forceinline__ void Store(__half* p, long long k, int i,
                                                  C v, const PhysConst& pc,

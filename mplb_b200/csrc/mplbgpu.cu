@@ -397,7 +397,8 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
         pc.w[i] = P.w[i];
         pc.cff[i] = (float)P.cf[i];
         pc.wf[i] = (float)P.w[i];
-        pc.winvf[i] = P.w[i] > 0 ? (float)(1.0 / P.w[i]) : 0.0f;
+        pc.winvf[i] = P.w[i] > 0 ? (float)(kHalfScale / P.w[i]) : 0.0f;
+        pc.wlf[i] = (float)(P.w[i] / kHalfScale);
     }
     pc.csf = (float)P.cs;
     pc.omcf = (float)P.omc;
