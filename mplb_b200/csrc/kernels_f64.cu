@@ -7,11 +7,29 @@ namespace mplb {
 template struct Launch<2, double>;
 template struct Launch<3, double>;
 
+// Sum of v over the CTA (blockDim.x a multiple of 32): shuffles within each
+// warp, then over the warps' sums; the total is valid in thread 0.  `ws`
+// is 32 doubles of shared memory, reusable when this returns.
+__device__ __forceinline__ double BlockSum(double v, double* ws) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
 __global__ void ResidualPartialKernel(const double* __restrict__ q,
                                       double* __restrict__ qold, long long n,
                                       double* __restrict__ part) {
-    __shared__ double sd[256];
-    __shared__ double ss[256];
+    __shared__ double ws[32];
     double d = 0.0, s = 0.0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
@@ -21,26 +39,18 @@ __global__ void ResidualPartialKernel(const double* __restrict__ q,
         s = s + v * v;
         qold[t] = v;
     }
-    sd[threadIdx.x] = d;
-    ss[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            sd[threadIdx.x] = sd[threadIdx.x] + sd[threadIdx.x + w];
-            ss[threadIdx.x] = ss[threadIdx.x] + ss[threadIdx.x + w];
-        }
-        __syncthreads();
-    }
+    d = BlockSum(d, ws);
+    s = BlockSum(s, ws);
     if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = sd[0];
-        part[2 * blockIdx.x + 1] = ss[0];
+        part[2 * blockIdx.x] = d;
+        part[2 * blockIdx.x + 1] = s;
     }
 }
 
 __global__ void SumPartialKernel(const double* __restrict__ q, long long n,
                                  double* __restrict__ part,
                                  unsigned long long* __restrict__ bad) {
-    __shared__ double ss[256];
+    __shared__ double ws[32];
     double s = 0.0;
     unsigned long long nb = 0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -49,13 +59,8 @@ __global__ void SumPartialKernel(const double* __restrict__ q, long long n,
         s = s + v;
         if (!(v > 0.0) || !isfinite(v)) nb++;
     }
-    ss[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) ss[threadIdx.x] = ss[threadIdx.x] + ss[threadIdx.x + w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) part[blockIdx.x] = ss[0];
+    s = BlockSum(s, ws);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (nb) atomicAdd(bad, nb);
 }
 
@@ -69,7 +74,7 @@ template struct BatchLaunch<double>;
 
 __global__ void BatchResidualPartialKernel(BatchDev bd,
                                            double* __restrict__ part) {
-    __shared__ double sh[6][256];
+    __shared__ double ws[32];
     const int nt = *bd.ntiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const int2 tile = bd.tiles[t];
@@ -85,16 +90,10 @@ __global__ void BatchResidualPartialKernel(BatchDev bd,
                 bd.macro_old[m][cv.mbase + k] = q;
             }
         }
-        for (int j = 0; j < 6; j++) sh[j][threadIdx.x] = v[j];
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w)
-                for (int j = 0; j < 6; j++)
-                    sh[j][threadIdx.x] = sh[j][threadIdx.x] + sh[j][threadIdx.x + w];
-            __syncthreads();
+        for (int j = 0; j < 6; j++) {
+            const double sum = BlockSum(v[j], ws);
+            if (threadIdx.x == 0) part[(long long)t * 6 + j] = sum;
         }
-        if (threadIdx.x < 6) part[(long long)t * 6 + threadIdx.x] = sh[threadIdx.x][0];
-        __syncthreads();
     }
 }
 
