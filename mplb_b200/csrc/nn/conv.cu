@@ -313,6 +313,135 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     }
 }
 
+__global__ void __launch_bounds__(kConvThreads, 1)
+    WgradTKernel(const __grid_constant__ CUtensorMap tx,
+                 const __grid_constant__ CUtensorMap tdy, WgradTArgs a) {
+    constexpr uint32_t ATOM = 8192;   // 128 pixel rows x 32 channels
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = Align1024(smem_raw);
+    const int b_atoms = a.bn / 32;
+    const uint32_t stage_bytes = (4 + b_atoms) * ATOM;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + a.stages * stage_bytes);
+    uint64_t* empty = full + a.stages;
+    uint64_t* accum = empty + a.stages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+    volatile int* cta_err = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this CTA's M tile: atoms 4 blockIdx.x .. + 3 (atom = tap * ci_chunks
+    // + chunk); the last tile may hold fewer
+    const int atom0 = 4 * blockIdx.x;
+    const int m_atoms = min(4, a.n_atoms - atom0);
+    const uint32_t tx_bytes = (uint32_t)(m_atoms + b_atoms) * ATOM;
+    const int kb0 = blockIdx.y * a.kb_per_split;
+    const int nk = min(a.kb_total, kb0 + a.kb_per_split) - kb0;
+    if (nk <= 0 || m_atoms <= 0) return;   // uniform, before any allocation
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < a.stages; s++) {
+            BarInit(&full[s], 1);
+            BarInit(&empty[s], 1);
+        }
+        BarInit(accum, 1);
+        *cta_err = 0;
+        FenceBarrierInit();
+        PrefetchTmap(&tx);
+        PrefetchTmap(&tdy);
+    }
+    if (warp == 2) TmemAlloc(tmem_slot, a.tmem_cols);
+    FenceBeforeSync();
+    __syncthreads();
+    FenceAfterSync();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        int j = 0;
+        for (; j < nk; j++) {
+            const int s = j % a.stages;
+            if (j >= a.stages &&
+                !BarWait(&empty[s], ((j / a.stages) + 1) & 1, cta_err)) {
+                Flag(cta_err, a.err);
+                break;
+            }
+            const int g = kb0 + j;
+            const int img = g / a.tiles_per_img;
+            const int h0 = (g - img * a.tiles_per_img) * a.bh;
+            uint8_t* sa = smem + s * stage_bytes;
+            BarArriveExpectTx(&full[s], tx_bytes);
+            for (int m = 0; m < m_atoms; m++) {
+                const int at = atom0 + m;
+                const int tap = at / a.ci_chunks;
+                const int chunk = at - tap * a.ci_chunks;
+                int dh, dw;
+                TapOffset(a.taps, tap, dh, dw);
+                TmaLoad4D(sa + m * ATOM, &tx, &full[s], 32 * chunk, dw,
+                          h0 + dh, img);
+            }
+            for (int bt = 0; bt < b_atoms; bt++)
+                TmaLoad4D(sa + (4 + bt) * ATOM, &tdy, &full[s], 32 * bt, 0,
+                          h0, img);
+        }
+        for (int q = j > a.stages ? j - a.stages : 0; q < j; q++)
+            if (!BarWaitDrain(&full[q % a.stages], (q / a.stages) & 1))
+                Flag(cta_err, a.err);
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t idesc = InstrDescBf16(kTileM, a.bn, true, true);
+        const uint32_t base = SmemAddr(smem);
+        for (int j = 0; j < nk; j++) {
+            const int s = j % a.stages;
+            if (!BarWait(&full[s], (j / a.stages) & 1, cta_err)) {
+                Flag(cta_err, a.err);
+                break;
+            }
+            FenceAfterSync();
+            const uint32_t sa = base + s * stage_bytes;
+            const uint32_t sb = sa + 4 * ATOM;
+            // MN-major, 64-byte swizzle: rows of 32 channels per pixel, 8-row
+            // groups 512 B apart, atoms (32 M or N rows) 8 KiB apart; 16
+            // pixels per MMA
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                Mma(tmem, SmemDesc(sa + k * 1024, ATOM, 512, 64),
+                    SmemDesc(sb + k * 1024, ATOM, 512, 64), idesc,
+                    (j | k) != 0 ? 1u : 0u);
+            }
+            Commit(&empty[s]);
+        }
+        Commit(accum);
+    }
+    __syncwarp();
+
+    const bool acc_ok = BarWaitDrain(accum, 0);
+    FenceAfterSync();
+    if (!acc_ok && threadIdx.x == 0) Flag(cta_err, a.err);
+    const bool store = acc_ok && *cta_err == 0;
+    // TMEM lane = M row: atom (warp), channel lane of its chunk; columns are
+    // output channels
+    const int at = atom0 + warp;
+    const int tap = at / a.ci_chunks;
+    const int ci = 32 * (at - tap * a.ci_chunks) + lane;
+    const bool row_ok = warp < m_atoms && ci < a.cin;
+    for (int c = 0; c < a.bn; c += 16) {
+        float v[16];
+        TmemLoad16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+        if (!store || !row_ok) continue;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int co = c + i;
+            if (co < a.cout)
+                atomicAdd(a.dw + ((long long)co * a.taps + tap) * a.cin + ci,
+                          v[i]);
+        }
+    }
+
+    FenceBeforeSync();
+    __syncthreads();
+    if (warp == 2) {
+        FenceAfterSync();
+        TmemFree(tmem, a.tmem_cols);
+    }
+}
+
 }  // namespace nn
 }  // namespace mplb
 
@@ -454,6 +583,12 @@ cudaError_t SetSmemAttr() {
     return e;
 }
 
+cudaError_t SetWgradTSmemAttr() {
+    static cudaError_t e = cudaFuncSetAttribute(
+        WgradTKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemMax);
+    return e;
+}
+
 cudaError_t SetWgradSmemAttr() {
     static cudaError_t e = cudaFuncSetAttribute(
         WgradKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemMax);
@@ -543,6 +678,47 @@ bool LaunchWgrad(const View& dy, const View& x, int taps, float* dw,
         x.h != dy.h || x.w != dy.w) {
         err = "weight-gradient shapes do not match";
         return false;
+    }
+    if (dy.c <= 64) {
+        // few output channels: taps x input channels along M (WgradTKernel)
+        CUtensorMap tx, tdy;
+        if (!EncodeAct(&tx, x, 32, 64, err) || !EncodeAct(&tdy, dy, 32, 64, err))
+            return false;
+        WgradTArgs t{};
+        t.H = x.h;
+        t.W = x.w;
+        t.tiles_per_img = x.h * x.w / kTileM;
+        t.bh = kTileM / x.w;
+        t.taps = taps;
+        t.cout = dy.c;
+        t.cin = x.c;
+        t.ci_chunks = (x.c + 31) / 32;
+        t.n_atoms = taps * t.ci_chunks;
+        t.bn = 32 * ((dy.c + 31) / 32);
+        t.stages = 4;
+        t.tmem_cols = Pow2Cols(t.bn);
+        t.kb_total = x.nimg * t.tiles_per_img;
+        const int mtiles = (t.n_atoms + 3) / 4;
+        int splits = (2 * sm_count + mtiles - 1) / mtiles;
+        if (splits < 1) splits = 1;
+        if (splits > t.kb_total) splits = t.kb_total;
+        t.kb_per_split = (t.kb_total + splits - 1) / splits;
+        splits = (t.kb_total + t.kb_per_split - 1) / t.kb_per_split;
+        t.dw = dw;
+        t.err = err_dev;
+        const int smem = ResidencySafeSmem(WgradTSmemBytes(t.bn, t.stages),
+                                           t.tmem_cols);
+        cudaError_t e = SetWgradTSmemAttr();
+        if (e == cudaSuccess)
+            WgradTKernel<<<dim3(mtiles, splits), kConvThreads, smem, stream>>>(
+                tx, tdy, t);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            err = std::string("weight-gradient launch: ") +
+                  cudaGetErrorString(e);
+            return false;
+        }
+        return true;
     }
     CUtensorMap ta, tb;
     if (!EncodeAct(&ta, dy, 64, 128, err) || !EncodeAct(&tb, x, 64, 128, err))

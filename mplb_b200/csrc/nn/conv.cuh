@@ -77,10 +77,37 @@ struct WgradArgs {
     int* err;
 };
 
+// Weight gradient of layers with few output channels (cout <= 64), with the
+// roles of the operands swapped: M = 128 rows of (tap, 32-channel chunk of
+// the input) pairs - four "atoms", each one 32-channel TMA box of X at its
+// tap's shifted coordinates - N = the output channels (32 or 64, from
+// 32-channel boxes of dY), K = 128-pixel blocks split over CTAs.  Both
+// operands MN-major, swizzled by 64 bytes.  Padding M to 128 for 32 output
+// channels and N to 64 for 32 input channels, as WgradKernel does for
+// these layers, wasted 7/8 of the tensor work.
+struct WgradTArgs {
+    int H, W, tiles_per_img, bh;
+    int taps;
+    int cout, cin;         // dW is [cout][taps][cin]
+    int ci_chunks;         // 32-channel chunks of the input
+    int n_atoms;           // taps * ci_chunks
+    int bn;                // UMMA N: 32 * ceil(cout / 32)
+    int kb_total;          // 128-pixel blocks in the batch
+    int kb_per_split;
+    int stages;
+    int tmem_cols;
+    float* dw;
+    int* err;
+};
+
 template <int BK>
 __global__ void ConvKernel(const __grid_constant__ CUtensorMap ta,
                            const __grid_constant__ CUtensorMap tb,
                            ConvArgs a);
+
+__global__ void WgradTKernel(const __grid_constant__ CUtensorMap tx,
+                             const __grid_constant__ CUtensorMap tdy,
+                             WgradTArgs a);
 
 __global__ void WgradKernel(const __grid_constant__ CUtensorMap ta,
                             const __grid_constant__ CUtensorMap tb,
@@ -93,6 +120,10 @@ inline int ConvSmemBytes(int bk, int bn, int stages) {
 }
 inline int WgradSmemBytes(int b_atoms, int stages) {
     return 1024 + stages * ((2 + b_atoms) * 16384) + 256;
+}
+// WgradTKernel: per stage four 8 KiB X atoms and bn / 32 8 KiB dY atoms.
+inline int WgradTSmemBytes(int bn, int stages) {
+    return 1024 + stages * ((4 + bn / 32) * 8192) + 256;
 }
 
 }  // namespace nn

@@ -123,6 +123,10 @@ WGRAD_CASES = [
     (2, 32, 128, 384, 9, None),
     (1, 128, 16, 32, 1, None),
     (2, 32, 64, 96, 9, (192, 96)),
+    # few output channels: taps x input channels along M
+    (2, 128, 32, 96, 9, (96, 0)),
+    (3, 64, 64, 32, 9, (64, 32)),
+    (1, 32, 48, 160, 9, None),
 ]
 
 
