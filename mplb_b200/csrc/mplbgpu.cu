@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -533,9 +534,13 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
                             (cx + cy * B.pitch + cz * B.plane);
         }
         // 32-bit offsets from the node's own address: every access stays
-        // within one population array of Q * popstride elements
+        // within one population array of Q * popstride elements.  Blocks
+        // beyond 2^31 elements take the 64-bit kernels;
+        // MPLB_B200_WIDE_OFFSETS=1 selects them for any block, so that tests
+        // can check them against the 32-bit ones on small cases.
         const long long span = (long long)Q * B.popstride;
-        d.off32 = span < 0x7fffffffLL ? 1 : 0;
+        const char* wide = std::getenv("MPLB_B200_WIDE_OFFSETS");
+        d.off32 = span < 0x7fffffffLL && !(wide && wide[0] == '1') ? 1 : 0;
         for (int i = 0; i < kMaxQ; i++) {
             d.pull_off32[i] = d.off32 ? (int)d.pull_off[i] : 0;
             d.pop_off32[i] = d.off32 ? (int)d.pop_off[i] : 0;
