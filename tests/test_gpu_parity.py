@@ -4,6 +4,8 @@ FP64 results are compared bit for bit with the golden fixtures made by the
 reference itself and with the oracle (the C restatement) on the same
 inputs; residuals, whose reductions sum in a different order, within a
 relative 1e-12."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -53,6 +55,15 @@ ORACLE_CASES = {
     "lchannel_bb": (lambda: config.lchannel(leg=9, side=6, depth=4,
                                             wall="HalfwayBounceBack"), 40, 20),
     "lchannel_eqm": (lambda: config.lchannel(leg=14, side=9, depth=7), 50, 25),
+    # blocks of two nodes along an axis (no interior region)
+    "tiny3d_3x2x4": (lambda: dataclasses.replace(
+        config.cavity(3, 4, 0.05, re=50), block_sizes=[(3, 2, 4)]), 12, 4),
+    "tiny3d_2x2x2": (lambda: dataclasses.replace(
+        config.cavity(3, 2, 0.05, re=50), block_sizes=[(2, 2, 2)]), 12, 4),
+    "tiny2d_2x5": (lambda: dataclasses.replace(
+        config.cavity(2, 5, 0.05, re=50), block_sizes=[(2, 5)]), 12, 4),
+    "odd3d_37x5x3": (lambda: dataclasses.replace(
+        config.cavity(3, 37, 0.05, re=200), block_sizes=[(37, 5, 3)]), 20, 10),
     "cavity3d_edges": (lambda: config.cavity(
         3, 9, 0.05, re=100,
         order=("Front", "Left", "Right", "Top", "Bottom", "Back")), 30, 10),

@@ -49,6 +49,13 @@ REF_CASES = {
     # the reference's one-array swap step, force without the shifted
     # velocity
     "swap_box_force": (_swap_box, 33, 11),
+    # blocks of two nodes along an axis: no interior at all
+    "tiny3d_3x2x4": (lambda: dataclasses.replace(
+        config.cavity(3, 4, 0.05, re=50), block_sizes=[(3, 2, 4)]), 12, 4),
+    "tiny3d_2x2x2": (lambda: dataclasses.replace(
+        config.cavity(3, 2, 0.05, re=50), block_sizes=[(2, 2, 2)]), 12, 4),
+    "tiny2d_7x2": (lambda: dataclasses.replace(
+        config.cavity(2, 7, 0.05, re=50), block_sizes=[(7, 2)]), 12, 4),
     "cavity2d_lid_first": (lambda: config.cavity(
         2, 15, 0.1, re=30, order=("Top", "Left", "Right", "Bottom")), 120, 40),
     "lchannel_app_9": (lambda: config.lchannel_app(9), 50, 25),
