@@ -98,3 +98,21 @@ def test_diverged_cavity_is_reported_not_converged(gpu_lib):
     assert b.diverged.tolist() == [True, False]
     assert not conv[0] and np.isnan(res[0]) and steps[0] < 100000
     assert conv[1] and res[1] < 1e-8
+
+
+@pytest.mark.parametrize("tile", [128, 256])
+def test_batch_large_cavity_row_division(gpu_lib, tile):
+    """A cavity above 1024 nodes per side takes the integer-division row
+    index (the float reciprocal is exact only up to 1024): still bit for
+    bit the single-block run, next to small ones."""
+    specs = [CavitySpec(1030, 400.0, 0.05), CavitySpec(11, 50.0, 0.04)]
+    b = Batch(specs, "fp64")
+    b.set_tuning(tile_nodes=tile, persistent=0, chunk=2, ctas_per_sm=4)
+    b.init()
+    b.step(6)
+    got = b.macro()
+    for spec, g in zip(specs, got):
+        want, _ = single(spec, 6)
+        for a, w in zip(g, want):
+            assert np.array_equal(a, w), spec
+    b.close()
