@@ -189,6 +189,21 @@ __device__ __forceinline__ __half StochasticHalf(float v, uint32_t r) {
     return __float2half_rz(__uint_as_float(__float_as_uint(v) + r));
 }
 
+// 32 random bits for population i of a node pair.
+__device__ __forceinline__ uint32_t SrDraw32(const Rng& g, int i) {
+    return g.s * (0x9e3779b1u * (uint32_t)(2 * i + 1) | 1u);
+}
+
+// lo and hi to FP16 with the hardware's stochastic rounding (sm_100a
+// cvt.rs, random bits from r); lo in the low half of the result.
+__device__ __forceinline__ uint32_t StochasticHalf2(float lo, float hi,
+                                                    uint32_t r) {
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo),
+        "r"(r));
+    return d;
+}
+
 template <>
 struct Prec<__half> {
     using C = float;
@@ -750,6 +765,29 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
         }
     }
     const bool fl = b.center_fluid != 0;
+    if constexpr (std::is_same<T, __half>::value && G == 2) {
+        // FP16 pairs: both nodes collided, then population i of the two
+        // converted together by the hardware's stochastic rounding
+        // (cvt.rs.f16x2.f32 with 32 random bits per pair)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (valid[j]) MomentsCollideT<L, T>(f[j], pc, fl);
+        const Rng rg = SeedRng(pc.seed, node[first]);
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const uint32_t pair = StochasticHalf2(
+                f[0][i] * pc.winvf[i], f[1][i] * pc.winvf[i], SrDraw32(rg, i));
+            const long long k0 = O32 ? node[0] + b.pop_off32[i]
+                                     : OwnIndex(b, node[0], i);
+            const long long k1 = O32 ? node[1] + b.pop_off32[i]
+                                     : OwnIndex(b, node[1], i);
+            if (valid[0]) PopStore(dst + k0, __ushort_as_half(
+                                                 (unsigned short)(pair & 0xffffu)));
+            if (valid[1]) PopStore(dst + k1, __ushort_as_half(
+                                                 (unsigned short)(pair >> 16)));
+        }
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < G; j++) {
         if (!valid[j]) continue;
