@@ -149,18 +149,16 @@ struct Prec<float> {
     }
 };
 
-// FP16 stores round stochastically: 13 random bits are added to the 13
-// float mantissa bits that FP16 drops before truncating, so increments far
-// below one FP16 unit - a small body force per step - survive in
-// expectation instead of being rounded away every step.  The stored value
-// is kHalfScale h_i / w_i: h_i / w_i = f_i / w_i - 1 lies in [-1, 255)
-// for any population within 256 times its weight (a lattice Boltzmann state
-// stays within a few times it), so the scaled value stays in FP16's range
-// while values down to |h / w| = 2^-22 stay normal - the draw is added at the right bit
-// without testing for FP16 subnormals (below that the rounding is plain
-// truncation, 2^-32 in h / w).  Draws: one 32-bit hash of (node, step)
-// per node, and for population i the top 13 bits of its product with an
-// odd constant (a bijection of the hash, so each draw is uniform).
+// FP16 stores round stochastically, so increments far below one FP16 unit -
+// a small body force per step - survive in expectation instead of being
+// rounded away every step.  The rounding is the hardware's
+// (cvt.rs.f16x2.f32, sm_100a): two values per instruction, random bits from
+// a 32-bit word.  The stored value is kHalfScale h_i / w_i:
+// h_i / w_i = f_i / w_i - 1 lies in [-1, 255) for any population within 256
+// times its weight (a lattice Boltzmann state stays within a few times it),
+// so the scaled value stays in FP16's range.  Draws: one 32-bit hash of
+// (node, step) per node (or node pair), times an odd constant per
+// population (a bijection of the hash, so each draw is uniform).
 constexpr float kHalfScale = 256.0f;
 
 struct Rng {
@@ -178,30 +176,24 @@ __device__ __forceinline__ Rng SeedRng(uint32_t seed, long long node) {
     return Rng{k};
 }
 
-// 13 random bits for population i, aligned with the 13 mantissa bits that
-// FP16 drops.
-__device__ __forceinline__ uint32_t SrDraw(const Rng& g, int i) {
-    const uint32_t m = 0x9e3779b1u * (uint32_t)(2 * i + 1) | 1u;
-    return (g.s * m) >> 19;
-}
-
-__device__ __forceinline__ __half StochasticHalf(float v, uint32_t r) {
-    return __float2half_rz(__uint_as_float(__float_as_uint(v) + r));
-}
-
-// 32 random bits for population i of a node pair.
+// 32 random bits for population i.
 __device__ __forceinline__ uint32_t SrDraw32(const Rng& g, int i) {
     return g.s * (0x9e3779b1u * (uint32_t)(2 * i + 1) | 1u);
 }
 
-// lo and hi to FP16 with the hardware's stochastic rounding (sm_100a
-// cvt.rs, random bits from r); lo in the low half of the result.
+// lo and hi to FP16 with the hardware's stochastic rounding, random bits
+// from r; lo in the low half of the result.
 __device__ __forceinline__ uint32_t StochasticHalf2(float lo, float hi,
                                                     uint32_t r) {
     uint32_t d;
     asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo),
         "r"(r));
     return d;
+}
+
+__device__ __forceinline__ __half StochasticHalf(float v, uint32_t r) {
+    return __ushort_as_half(
+        (unsigned short)(StochasticHalf2(v, 0.0f, r) & 0xffffu));
 }
 
 template <>
@@ -215,7 +207,7 @@ struct Prec<__half> {
     __device__ static __forceinline__ void Store(__half* p, long long k, int i,
                                                  C v, const PhysConst& pc,
                                                  Rng& rng) {
-        PopStore(p + k, StochasticHalf(v * pc.winvf[i], SrDraw(rng, i)));
+        PopStore(p + k, StochasticHalf(v * pc.winvf[i], SrDraw32(rng, i)));
     }
 };
 
