@@ -629,12 +629,13 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
     const int dim = ctx->plan.dim;
     const size_t nodes = (size_t)B->nodes();
     const double* src[4] = {rho, u, v, w};
-    std::vector<double> fill(nodes);
+    std::vector<double> fill;   // host staging only for fields not given
     for (int m = 0; m < dim + 1; m++) {
         if (src[m]) {
             CK(cudaMemcpyAsync(b->macro[m], src[m], nodes * sizeof(double),
                                cudaMemcpyHostToDevice, ctx->stream));
         } else {
+            fill.resize(nodes);
             std::fill(fill.begin(), fill.end(), m == 0 ? 1.0 : 0.0);
             CK(cudaMemcpyAsync(b->macro[m], fill.data(), nodes * sizeof(double),
                                cudaMemcpyHostToDevice, ctx->stream));
