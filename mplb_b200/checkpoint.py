@@ -11,6 +11,8 @@ contiguous, halo excluded) with the suffix ``.f64``, plus one JSON manifest
 
     save(solver, directory, step)        -> manifest path
     restart(case, directory, step, lib)  -> Solver positioned after `step`
+    save_slabs / restart_slabs           -> the same for a run split into
+                                            slabs (files of the whole block)
 
 A restart uploads each block's f (``mplbgpu_upload_f``); the next step then
 continues bit for bit as the uninterrupted run would.
@@ -87,6 +89,27 @@ def save(solver: Solver, directory: str, step: int) -> str:
     """Checkpoint of a running solver (its current f per block)."""
     return write(directory, solver.case, step,
                  {b: solver.f(b) for b in solver.case.block_ids})
+
+
+def save_slabs(solver, directory: str, step: int) -> str:
+    """Checkpoint of a slab-decomposed run held by this process (every
+    slab), in the files of the undivided block: it restarts as the whole
+    block or as slabs."""
+    if len(solver.parts) != solver.nparts:
+        raise ValueError("every slab must be held by this process")
+    bid = solver.case.block_ids[0]
+    return write(directory, solver.case, step, {bid: solver.f()})
+
+
+def restart_slabs(case, parts: int, directory: str, step: int, lib=None):
+    """A slab-decomposed solver (all slabs in this process) holding the
+    checkpointed f of the undivided block."""
+    from . import slab
+    fields = read(directory, case, step)
+    s = slab.SlabSolver(case, parts, list(range(parts)), slab.LocalExchange(),
+                        lib)
+    s.upload_f(fields[case.block_ids[0]])
+    return s
 
 
 def restart(case, directory: str, step: int, lib=None) -> Solver:

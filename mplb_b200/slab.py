@@ -239,6 +239,18 @@ class SlabSolver:
         for p in self.parts:
             p.solver.init_uniform()
 
+    def upload_f(self, f):
+        """The distributions of the whole block (nz, ny, nx, Q); each slab
+        held here takes its part (restart)."""
+        f = np.asarray(f)
+        axis = self.case.space_dim - 1
+        n = self.case.block_sizes[0][axis]
+        bounds = slab_bounds(n, self.nparts)
+        for p in self.parts:
+            lo, hi = bounds[p.index]
+            part = f[lo:hi] if self.join_axis == 0 else f[:, lo:hi]
+            p.solver.upload_f(p.bid, np.ascontiguousarray(part))
+
     def stream_collision(self, n=1):
         """n steps; the faces cross before each step."""
         for _ in range(int(n)):

@@ -132,3 +132,28 @@ def test_slab_ranks_through_torch_distributed(gpu_lib):
                           w.f(0))
     np.testing.assert_allclose(got[0][1], rw[0], rtol=1e-12)
     w.close()
+
+
+def test_slab_checkpoint_round_trips_with_the_whole_block(gpu_lib, tmp_path):
+    """Slabs checkpoint into the whole block's files and restart from them
+    either way, bit for bit the uninterrupted whole-block run."""
+    from mplb_b200 import checkpoint
+    case = config.cavity(3, 18, 0.05, re=100)
+    w = Solver(case)
+    w.init_uniform()
+    w.stream_collision(21)
+    want = w.f(0)
+    w.close()
+    s = slab.SlabSolver(case, 3, [0, 1, 2], slab.LocalExchange())
+    s.init_uniform()
+    s.stream_collision(7)
+    checkpoint.save_slabs(s, str(tmp_path), 7)
+    s.close()
+    r = checkpoint.restart(case, str(tmp_path), 7)      # as the whole block
+    r.stream_collision(7)
+    checkpoint.save(r, str(tmp_path), 14)
+    r.close()
+    s2 = checkpoint.restart_slabs(case, 2, str(tmp_path), 14)   # as 2 slabs
+    s2.stream_collision(7)
+    assert np.array_equal(s2.f(), want)
+    s2.close()
