@@ -354,11 +354,67 @@ __device__ __forceinline__ void CollideF64(double* f, const PhysConst& pc,
 }
 
 // Shifted forms: h = f - w.  rho = 1 + sum h, j = sum CS c h (sum c w = 0).
-template <typename L>
-__device__ __forceinline__ void MomentsShifted(const float* h,
-                                               const PhysConst& pc,
-                                               bool fluidlike, float& drho,
-                                               float u[3]) {
+//
+// The arithmetic is written once over V = float (one node) or V = float2
+// (two nodes: sm_100a's paired FP32 instructions, one instruction for both
+// nodes), every operation rounded explicitly (no contraction left to the
+// compiler), so a node gives the same bits alone or in a pair.
+template <typename V>
+struct VOps;
+
+template <>
+struct VOps<float> {
+    __device__ static __forceinline__ float add(float a, float b) {
+        return __fadd_rn(a, b);
+    }
+    __device__ static __forceinline__ float sub(float a, float b) {
+        return __fsub_rn(a, b);
+    }
+    __device__ static __forceinline__ float mul(float a, float b) {
+        return __fmul_rn(a, b);
+    }
+    __device__ static __forceinline__ float fma(float a, float b, float c) {
+        return __fmaf_rn(a, b, c);
+    }
+    __device__ static __forceinline__ float neg(float a) { return -a; }
+    __device__ static __forceinline__ float splat(float c) { return c; }
+    __device__ static __forceinline__ float rcp(float a) {
+        return __frcp_rn(a);
+    }
+};
+
+template <>
+struct VOps<float2> {
+    __device__ static __forceinline__ float2 add(float2 a, float2 b) {
+        return __fadd2_rn(a, b);
+    }
+    __device__ static __forceinline__ float2 sub(float2 a, float2 b) {
+        return __fadd2_rn(a, neg(b));
+    }
+    __device__ static __forceinline__ float2 mul(float2 a, float2 b) {
+        return __fmul2_rn(a, b);
+    }
+    __device__ static __forceinline__ float2 fma(float2 a, float2 b,
+                                                 float2 c) {
+        return __ffma2_rn(a, b, c);
+    }
+    __device__ static __forceinline__ float2 neg(float2 a) {
+        return make_float2(-a.x, -a.y);
+    }
+    __device__ static __forceinline__ float2 splat(float c) {
+        return make_float2(c, c);
+    }
+    __device__ static __forceinline__ float2 rcp(float2 a) {
+        return make_float2(__frcp_rn(a.x), __frcp_rn(a.y));
+    }
+};
+
+template <typename L, typename V>
+__device__ __forceinline__ void MomentsShiftedV(const V* h,
+                                                const PhysConst& pc,
+                                                bool fluidlike, V& drho,
+                                                V u[3]) {
+    using O = VOps<V>;
     constexpr int Q = L::Q;
     // Opposite populations are combined first: h_i + h_opp(i) cancels the
     // large odd parts (exactly, by Sterbenz's lemma, when they dominate) and
@@ -370,19 +426,25 @@ __device__ __forceinline__ void MomentsShifted(const float* h,
     drho = h[0];
 #pragma unroll
     for (int i = 1; i < Q; i++)
-        if (i < L::opp(i)) drho += h[i] + h[L::opp(i)];
-    const float rinv = __frcp_rn(1.0f + drho);
+        if (i < L::opp(i)) drho = O::add(drho, O::add(h[i], h[L::opp(i)]));
+    const V rinv = O::rcp(O::add(O::splat(1.0f), drho));
 #pragma unroll
     for (int a = 0; a < L::D; a++) {
-        float s = 0.0f;
+        V s = O::splat(0.0f);
+        bool first = true;
 #pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (comp<L>(i, a) > 0) s += h[i] - h[L::opp(i)];
-        s = pc.csf * s * rinv;
-        if (pc.force_vel && fluidlike) s += pc.hdtaf[a];
+        for (int i = 0; i < Q; i++) {
+            if (comp<L>(i, a) > 0) {
+                const V d = O::sub(h[i], h[L::opp(i)]);
+                s = first ? d : O::add(s, d);
+                first = false;
+            }
+        }
+        s = O::mul(O::mul(O::splat(pc.csf), s), rinv);
+        if (pc.force_vel && fluidlike) s = O::add(s, O::splat(pc.hdtaf[a]));
         u[a] = s;
     }
-    if (L::D == 2) u[2] = 0.0f;
+    if (L::D == 2) u[2] = O::splat(0.0f);
 }
 
 // feq_i - w_i = w_i [(rho - 1) + rho (cu + (cu^2 - u^2) / 2)], computed
@@ -402,70 +464,118 @@ __device__ __forceinline__ void MomentsShifted(const float* h,
 // error after 5e4 steps of a channel spinning up); with the projection BGK
 // conserves mass and momentum to the final rounding.  m_i is small, so the
 // sums over opposite pairs are accurate to its own ulp.
-template <typename L>
-__device__ __forceinline__ void CollideShifted(float* h, const PhysConst& pc,
-                                               bool fluidlike, float drho,
-                                               const float u[3], float omc) {
+template <typename L, typename V>
+__device__ __forceinline__ void CollideShiftedV(V* h, const PhysConst& pc,
+                                                bool fluidlike, V drho,
+                                                const V u[3], float omc) {
+    using O = VOps<V>;
     constexpr int Q = L::Q;
-    const float rho = 1.0f + drho;
-    const float hr = 0.5f * rho;   // rest population: w (drho - rho u^2 / 2)
-    const float cu0 = pc.csf * u[0], cu1 = pc.csf * u[1], cu2 = pc.csf * u[2];
-    const float u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const V rho = O::add(O::splat(1.0f), drho);
+    const V hr = O::mul(O::splat(0.5f), rho);   // rest: w (drho - rho u^2 / 2)
+    const V csf = O::splat(pc.csf);
+    const V cu0 = O::mul(csf, u[0]), cu1 = O::mul(csf, u[1]),
+            cu2 = O::mul(csf, u[2]);
+    const V u2 = O::fma(u[0], u[0], O::fma(u[1], u[1], O::mul(u[2], u[2])));
+    const V half = O::splat(0.5f);
     // m_i = h_i - heq_i.  heq is evaluated whole for each direction (the
     // pair i, opp(i) shares cu^2 - u^2 only): splitting it into an even and
     // an odd part rounded separately biases the stress it carries, which a
     // channel spinning up shows as a 10x larger velocity error.
-    float m[Q];
-    m[0] = fmaf(-pc.wf[0], fmaf(-hr, u2, drho), h[0]);
-    float m0 = m[0], mv0 = 0.0f, mv1 = 0.0f, mv2 = 0.0f;
+    V m[Q];
+    m[0] = O::fma(O::splat(-pc.wf[0]), O::fma(O::neg(hr), u2, drho), h[0]);
+    V m0 = m[0], mv0 = O::splat(0.0f), mv1 = O::splat(0.0f),
+      mv2 = O::splat(0.0f);
 #pragma unroll
     for (int i = 1; i < Q; i++) {
         if (i > L::opp(i)) continue;
         const int j = L::opp(i);
-        float cu = 0.0f;
-        if (L::cx(i) > 0) cu += cu0;
-        if (L::cx(i) < 0) cu -= cu0;
-        if (L::cy(i) > 0) cu += cu1;
-        if (L::cy(i) < 0) cu -= cu1;
-        if (L::cz(i) > 0) cu += cu2;
-        if (L::cz(i) < 0) cu -= cu2;
-        const float y = fmaf(cu, cu, -u2);
-        m[i] = fmaf(-pc.wf[i], fmaf(rho, fmaf(0.5f, y, cu), drho), h[i]);
-        m[j] = fmaf(-pc.wf[j], fmaf(rho, fmaf(0.5f, y, -cu), drho), h[j]);
-        m0 += m[i] + m[j];
-        const float d = m[i] - m[j];
-        if (L::cx(i) > 0) mv0 += d;
-        if (L::cx(i) < 0) mv0 -= d;
-        if (L::cy(i) > 0) mv1 += d;
-        if (L::cy(i) < 0) mv1 -= d;
-        if (L::cz(i) > 0) mv2 += d;
-        if (L::cz(i) < 0) mv2 -= d;
+        V cu = O::splat(0.0f);
+        bool first = true;
+        const V comps[3] = {cu0, cu1, cu2};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const int c = comp<L>(i, a);
+            if (c == 0 || a >= L::D) continue;
+            const V t = c > 0 ? comps[a] : O::neg(comps[a]);
+            cu = first ? t : O::add(cu, t);
+            first = false;
+        }
+        const V y = O::fma(cu, cu, O::neg(u2));
+        m[i] = O::fma(O::splat(-pc.wf[i]),
+                      O::fma(rho, O::fma(half, y, cu), drho), h[i]);
+        m[j] = O::fma(O::splat(-pc.wf[j]),
+                      O::fma(rho, O::fma(half, y, O::neg(cu)), drho), h[j]);
+        m0 = O::add(m0, O::add(m[i], m[j]));
+        const V d = O::sub(m[i], m[j]);
+        if (L::cx(i) > 0) mv0 = O::add(mv0, d);
+        if (L::cx(i) < 0) mv0 = O::sub(mv0, d);
+        if (L::cy(i) > 0) mv1 = O::add(mv1, d);
+        if (L::cy(i) < 0) mv1 = O::sub(mv1, d);
+        if (L::cz(i) > 0) mv2 = O::add(mv2, d);
+        if (L::cz(i) < 0) mv2 = O::sub(mv2, d);
     }
     if (pc.force_vel && fluidlike) {
-        mv0 += rho * pc.hdta_csf[0];
-        mv1 += rho * pc.hdta_csf[1];
-        mv2 += rho * pc.hdta_csf[2];
+        mv0 = O::fma(rho, O::splat(pc.hdta_csf[0]), mv0);
+        mv1 = O::fma(rho, O::splat(pc.hdta_csf[1]), mv1);
+        mv2 = O::fma(rho, O::splat(pc.hdta_csf[2]), mv2);
     }
-    mv0 *= 3.0f;
-    mv1 *= 3.0f;
-    mv2 *= 3.0f;
+    const V three = O::splat(3.0f);
+    mv0 = O::mul(mv0, three);
+    mv1 = O::mul(mv1, three);
+    mv2 = O::mul(mv2, three);
     // g_i = h_i + omega (w_i (M0 + 3 c_i . M) - m_i + F_i / omega), with
     // F_i = w_i CS c_i.a tau omega rho: one rounding at the size of h_i.
-    const float om = 1.0f - omc;
+    const V om = O::splat(1.0f - omc);
     const bool force = pc.force && fluidlike;
-    const float fr = pc.tw_omf * rho;
+    const V fr = O::mul(O::splat(pc.tw_omf), rho);
 #pragma unroll
     for (int i = 0; i < Q; i++) {
-        float cm = m0;
-        if (L::cx(i) > 0) cm += mv0;
-        if (L::cx(i) < 0) cm -= mv0;
-        if (L::cy(i) > 0) cm += mv1;
-        if (L::cy(i) < 0) cm -= mv1;
-        if (L::cz(i) > 0) cm += mv2;
-        if (L::cz(i) < 0) cm -= mv2;
-        float t = fmaf(pc.wf[i], cm, -m[i]);
-        if (force) t = fmaf(fr, pc.wcff[i], t);
-        h[i] = fmaf(om, t, h[i]);
+        V cm = m0;
+        if (L::cx(i) > 0) cm = O::add(cm, mv0);
+        if (L::cx(i) < 0) cm = O::sub(cm, mv0);
+        if (L::cy(i) > 0) cm = O::add(cm, mv1);
+        if (L::cy(i) < 0) cm = O::sub(cm, mv1);
+        if (L::cz(i) > 0) cm = O::add(cm, mv2);
+        if (L::cz(i) < 0) cm = O::sub(cm, mv2);
+        V t = O::fma(O::splat(pc.wf[i]), cm, O::neg(m[i]));
+        if (force) t = O::fma(fr, O::splat(pc.wcff[i]), t);
+        h[i] = O::fma(om, t, h[i]);
+    }
+}
+
+template <typename L>
+__device__ __forceinline__ void MomentsShifted(const float* h,
+                                               const PhysConst& pc,
+                                               bool fluidlike, float& drho,
+                                               float u[3]) {
+    MomentsShiftedV<L, float>(h, pc, fluidlike, drho, u);
+}
+
+template <typename L>
+__device__ __forceinline__ void CollideShifted(float* h, const PhysConst& pc,
+                                               bool fluidlike, float drho,
+                                               const float u[3], float omc) {
+    CollideShiftedV<L, float>(h, pc, fluidlike, drho, u, omc);
+}
+
+// Moments and collision of two nodes at once (paired FP32 instructions);
+// bit for bit what MomentsCollideT does to each of them alone.
+template <typename L>
+__device__ __forceinline__ void MomentsCollidePair(float* ha, float* hb,
+                                                   const PhysConst& pc,
+                                                   bool fluidlike,
+                                                   float omcf) {
+    constexpr int Q = L::Q;
+    float2 h[Q];
+#pragma unroll
+    for (int i = 0; i < Q; i++) h[i] = make_float2(ha[i], hb[i]);
+    float2 drho, u[3];
+    MomentsShiftedV<L, float2>(h, pc, fluidlike, drho, u);
+    CollideShiftedV<L, float2>(h, pc, fluidlike, drho, u, omcf);
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        ha[i] = h[i].x;
+        hb[i] = h[i].y;
     }
 }
 
@@ -583,11 +693,12 @@ __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
 // Fused step over one block.  kModeStep writes g^{n+1}; kModeMacro and
 // kModeF recompute the current f = post-boundary populations from the
 // previous g and write moments or f (FP64, dense) instead.
-// The shifted forms hold two interior nodes per thread (PureNodeGroup):
-// 6 CTAs of 128 threads per SM (<= 85 registers) keeps both nodes in
-// registers; 8 CTAs (64 registers) spilled and measured no faster.
+// The shifted forms hold two interior nodes per thread (PureNodeGroup) and
+// collide them with paired FP32 instructions: 5 CTAs of 128 threads per SM
+// (<= 102 registers) keeps the register pairs with almost no spills (at 6
+// CTAs the paired form spilled and lost 17 % in FP32).
 #ifndef MPLB_LP_MIN_BLOCKS
-#define MPLB_LP_MIN_BLOCKS 6
+#define MPLB_LP_MIN_BLOCKS 5
 #endif
 // The FP64 form holds 19 doubles per node; 5 CTAs per SM (<= 102 registers)
 // keeps it spill-free with 20 warps of loads in flight.
@@ -757,13 +868,15 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
         }
     }
     const bool fl = b.center_fluid != 0;
+    // shifted forms: the two nodes collide together (paired FP32
+    // instructions); a node outside the row computes on its copy of the
+    // other's values and is not stored
+    constexpr bool kPair = P::kShifted && G == 2;
+    if constexpr (kPair) MomentsCollidePair<L>(f[0], f[1], pc, fl, pc.omcf);
     if constexpr (std::is_same<T, __half>::value && G == 2) {
-        // FP16 pairs: both nodes collided, then population i of the two
-        // converted together by the hardware's stochastic rounding
-        // (cvt.rs.f16x2.f32 with 32 random bits per pair)
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-            if (valid[j]) MomentsCollideT<L, T>(f[j], pc, fl);
+        // FP16 pairs: population i of the two converted together by the
+        // hardware's stochastic rounding (cvt.rs.f16x2.f32 with 32 random
+        // bits per pair)
         const Rng rg = SeedRng(pc.seed, node[first]);
 #pragma unroll
         for (int i = 0; i < Q; i++) {
@@ -783,7 +896,7 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
 #pragma unroll
     for (int j = 0; j < G; j++) {
         if (!valid[j]) continue;
-        MomentsCollideT<L, T>(f[j], pc, fl);
+        if constexpr (!kPair) MomentsCollideT<L, T>(f[j], pc, fl);
         Rng rg = SeedRng(pc.seed, node[j]);
         if constexpr (O32) {
             T* pd = dst + node[j];

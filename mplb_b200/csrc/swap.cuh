@@ -165,10 +165,12 @@ __device__ __forceinline__ void SwapInteriorGroup(const BlockDev& b,
         for (int j = 0; j < G; j++) v[j][k] = P::Load(p[j], off(k), k, pc);
     }
     const bool fl = b.center_fluid != 0;
+    constexpr bool kPair = P::kShifted && G == 2;
+    if constexpr (kPair) MomentsCollidePair<L>(v[0], v[1], pc, fl, pc.omcf);
 #pragma unroll
     for (int j = 0; j < G; j++) {
         if (!valid[j]) continue;
-        MomentsCollideT<L, T>(v[j], pc, fl);
+        if constexpr (!kPair) MomentsCollideT<L, T>(v[j], pc, fl);
         Rng rg = SeedRng(pc.seed, node[j]);
 #pragma unroll
         for (int k = 0; k < Q; k++)
