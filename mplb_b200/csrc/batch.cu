@@ -37,8 +37,8 @@ struct mplbgpu_batch {
     int cur = 0;                       // pop[cur] holds the latest g
     double* macro[3] = {nullptr, nullptr, nullptr};
     double* macro_old[3] = {nullptr, nullptr, nullptr};
-    int2* tiles_all = nullptr;
-    int2* tiles_active = nullptr;
+    int4* tiles_all = nullptr;
+    int4* tiles_active = nullptr;
     int* ntiles_dev = nullptr;
     int ntiles_all = 0;
     int ntiles_active = 0;
@@ -104,13 +104,17 @@ void DropGraphs(mplbgpu_batch* b) {
 
 int BuildTiles(mplbgpu_batch* b) {
     const int tn = b->tune.tile_nodes;
-    std::vector<int2> tiles;
+    std::vector<int4> tiles;
+    const long long unit = 128 / (b->precision == MPLBGPU_FP64 ? 8 : 4);
     b->first_tile.assign(b->cav.size(), 0);
     b->ntile.assign(b->cav.size(), 0);
     for (size_t c = 0; c < b->cav.size(); c++) {
         const long long nn = (long long)b->cav[c].n * b->cav[c].n;
         b->first_tile[c] = (int)tiles.size();
-        for (long long k = 0; k < nn; k += tn) tiles.push_back(make_int2((int)c, (int)k));
+        // cavity offsets are multiples of 128 bytes (mplbgpu_batch_create)
+        const int base = (int)(b->hcav[c].base / unit);
+        for (long long k = 0; k < nn; k += tn)
+            tiles.push_back(make_int4((int)c, (int)k, b->cav[c].n, base));
         b->ntile[c] = (int)tiles.size() - b->first_tile[c];
     }
     cudaFree(b->tiles_all);
@@ -119,10 +123,10 @@ int BuildTiles(mplbgpu_batch* b) {
     b->tiles_all = b->tiles_active = nullptr;
     b->part = nullptr;
     b->ntiles_all = (int)tiles.size();
-    BCK(cudaMalloc(&b->tiles_all, tiles.size() * sizeof(int2)));
-    BCK(cudaMalloc(&b->tiles_active, tiles.size() * sizeof(int2)));
+    BCK(cudaMalloc(&b->tiles_all, tiles.size() * sizeof(int4)));
+    BCK(cudaMalloc(&b->tiles_active, tiles.size() * sizeof(int4)));
     BCK(cudaMalloc(&b->part, tiles.size() * 6 * sizeof(double)));
-    BCK(cudaMemcpy(b->tiles_all, tiles.data(), tiles.size() * sizeof(int2),
+    BCK(cudaMemcpy(b->tiles_all, tiles.data(), tiles.size() * sizeof(int4),
                    cudaMemcpyHostToDevice));
     DropGraphs(b);
     return MPLBGPU_OK;
@@ -135,7 +139,7 @@ int UploadActive(mplbgpu_batch* b) {
     for (int c : b->active) {
         ranges.push_back(make_int4(c, pos, b->ntile[c], 0));
         BCK(cudaMemcpyAsync(b->tiles_active + pos, b->tiles_all + b->first_tile[c],
-                            b->ntile[c] * sizeof(int2), cudaMemcpyDeviceToDevice,
+                            b->ntile[c] * sizeof(int4), cudaMemcpyDeviceToDevice,
                             b->stream));
         pos += b->ntile[c];
     }
@@ -201,7 +205,8 @@ int LaunchChunk(mplbgpu_batch* b, int nsteps, bool macro_last) {
             T* dst = (b->cur ^ (s & 1)) == 0 ? P1 : P0;
             cudaError_t e = BatchLaunch<T>::Step(macro_last && s == nsteps - 1,
                                                  grid, threads, b->stream, d,
-                                                 b->pc, src, dst);
+                                                 b->pc, b->ntiles_active, src,
+                                                 dst);
             b->launches++;
             b->pc.seed += 1;
             if (e != cudaSuccess)
@@ -374,6 +379,10 @@ mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
         const long long nn = (long long)cv.n * cv.n;
         base += ((9 * nn + align - 1) / align) * align;
         mbase += nn;
+    }
+    if (base / align > 0x7fffffffLL) {   // tiles hold the offset in 32 bits
+        delete b;
+        return BErr(nullptr, MPLBGPU_ERR_INVALID, "batch too large");
     }
     b->pop_elems = base;
     b->total_nodes = mbase;

@@ -32,7 +32,11 @@ struct BatchCav {
 
 struct BatchDev {
     const BatchCav* cavs;
-    const int2* tiles;      // active tiles: (cavity, first node)
+    // active tiles: (cavity, first node, nodes per side, element offset of
+    // the cavity in 128-byte units), so a tile's population addresses wait
+    // on the tile's own load alone and the cavity's constants load beside
+    // the populations
+    const int4* tiles;
     const int* ntiles;      // number of active tiles (device word)
     int tile_nodes;         // nodes per tile = threads per CTA
     double* macro[3];       // rho, u, v of every cavity, packed
@@ -50,22 +54,22 @@ struct GridSync {           // bounded grid-wide barrier state
 template <typename T, bool MACRO>
 __device__ __forceinline__ void BatchNode(const BatchDev& bd,
                                           const PhysConst& pc,
-                                          const BatchCav& cv, int k,
+                                          const BatchCav& cv, int n,
+                                          long long base, float ninv, int k,
                                           const T* __restrict__ src,
                                           T* __restrict__ dst) {
     using L = Lattice<2>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = 9;
-    const int n = cv.n;
     const long long nn = (long long)n * n;
     // k / n without an integer division: (k + 1/2) / n is at least 1/(2n)
     // from an integer and the float product is off by less than
     // (k + 1/2) / n * 2^-22, so truncating it is exact while n <= 1024
-    const int y = n <= 1024 ? (int)(((float)k + 0.5f) * cv.ninv) : k / n;
+    const int y = n <= 1024 ? (int)(((float)k + 0.5f) * ninv) : k / n;
     const int x = k - y * n;
-    const T* s = src + cv.base;
-    T* d = dst + cv.base;
+    const T* s = src + base;
+    T* d = dst + base;
     C f[Q];
 #pragma unroll
     for (int i = 0; i < Q; i++) {
@@ -83,7 +87,7 @@ __device__ __forceinline__ void BatchNode(const BatchDev& bd,
     }
     double rho, u[3];
     MomentsCollideT<L, T>(f, pc, false, cv.omc, cv.omcf, rho, u);
-    Rng rng = SeedRng(pc.seed, cv.base + k);
+    Rng rng = SeedRng(pc.seed, base + k);
 #pragma unroll
     for (int i = 0; i < Q; i++) P::Store(d, i * nn + k, i, f[i], pc, rng);
     if (MACRO) {
@@ -100,24 +104,24 @@ __device__ __forceinline__ void BatchNode(const BatchDev& bd,
 template <typename T, bool MACRO>
 __device__ __forceinline__ void BatchNodePair(const BatchDev& bd,
                                               const PhysConst& pc,
-                                              const BatchCav& cv, int ka,
-                                              bool second,
+                                              const BatchCav& cv, int n,
+                                              long long base, float ninv,
+                                              int ka, bool second,
                                               const T* __restrict__ src,
                                               T* __restrict__ dst) {
     using L = Lattice<2>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = 9;
-    const int n = cv.n;
     const int nn = n * n;   // a cavity's populations fit in 32-bit offsets
     const int kk[2] = {ka, second ? ka + 32 : ka};
-    const T* s = src + cv.base;
-    T* d = dst + cv.base;
+    const T* s = src + base;
+    T* d = dst + base;
     C f[2][Q];
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         const int k = kk[j];
-        const int y = n <= 1024 ? (int)(((float)k + 0.5f) * cv.ninv) : k / n;
+        const int y = n <= 1024 ? (int)(((float)k + 0.5f) * ninv) : k / n;
         const int x = k - y * n;
 #pragma unroll
         for (int i = 0; i < Q; i++) {
@@ -140,7 +144,7 @@ __device__ __forceinline__ void BatchNodePair(const BatchDev& bd,
         const int k = kk[j];
         double rho, u[3];
         MomentsCollideT<L, T>(f[j], pc, false, cv.omc, cv.omcf, rho, u);
-        Rng rng = SeedRng(pc.seed, cv.base + k);
+        Rng rng = SeedRng(pc.seed, base + k);
 #pragma unroll
         for (int i = 0; i < Q; i++) P::Store(d, i * nn + k, i, f[j][i], pc, rng);
         if (MACRO) {
@@ -160,35 +164,42 @@ __host__ __device__ constexpr int BatchNodesPerThread() {
 
 template <typename T, bool MACRO>
 __device__ __forceinline__ void BatchSweep(const BatchDev& bd,
-                                           const PhysConst& pc,
+                                           const PhysConst& pc, int nt,
                                            const T* __restrict__ src,
                                            T* __restrict__ dst) {
-    const int nt = *bd.ntiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const int2 tile = bd.tiles[t];
+        const int4 tile = bd.tiles[t];
         const BatchCav& cv = bd.cavs[tile.x];
+        const int n = tile.z;
+        const int nn = n * n;
+        const long long base = (long long)tile.w * (long long)(128 / sizeof(T));
+        // the correctly rounded 1 / n, as the host computes it
+        const float ninv = __frcp_rn((float)n);
         if constexpr (BatchNodesPerThread<T>() == 2) {
             // warp w has nodes [64 w, 64 w + 64) of the tile, lane l the
             // nodes 64 w + l and 64 w + 32 + l
             const int ka = tile.y + (int)(threadIdx.x >> 5) * 64 +
                            (int)(threadIdx.x & 31);
-            const int nn = cv.n * cv.n;
             if (ka < nn)
-                BatchNodePair<T, MACRO>(bd, pc, cv, ka, ka + 32 < nn, src,
-                                        dst);
+                BatchNodePair<T, MACRO>(bd, pc, cv, n, base, ninv, ka,
+                                        ka + 32 < nn, src, dst);
         } else {
             const int k = tile.y + threadIdx.x;
-            if (k < cv.n * cv.n) BatchNode<T, MACRO>(bd, pc, cv, k, src, dst);
+            if (k < nn)
+                BatchNode<T, MACRO>(bd, pc, cv, n, base, ninv, k, src, dst);
         }
     }
 }
 
 // One step over every active tile (a CUDA graph replays a chunk of these).
+// `nt` is the active tile count when the launch was made (one-step graphs
+// are captured again when it changes), so the tile loads need not wait for
+// the device word.
 template <typename T, bool MACRO>
 __global__ void __launch_bounds__(256)
-    BatchStepKernel(BatchDev bd, PhysConst pc, const T* __restrict__ src,
-                    T* __restrict__ dst) {
-    BatchSweep<T, MACRO>(bd, pc, src, dst);
+    BatchStepKernel(BatchDev bd, PhysConst pc, int nt,
+                    const T* __restrict__ src, T* __restrict__ dst) {
+    BatchSweep<T, MACRO>(bd, pc, nt, src, dst);
 }
 
 // Grid-wide barrier with a bounded wait: thread 0 of each CTA arrives and
@@ -233,13 +244,14 @@ __global__ void __launch_bounds__(256)
                           int macro_last, GridSync gs) {
     unsigned my_gen = 0;
     if (threadIdx.x == 0) my_gen = atomicAdd(gs.gen, 0u);
+    const int nt = *bd.ntiles;
     for (int s = 0; s < nsteps; s++) {
         const T* src = (s & 1) ? b : a;
         T* dst = (s & 1) ? a : b;
         if (macro_last && s == nsteps - 1)
-            BatchSweep<T, true>(bd, pc, src, dst);
+            BatchSweep<T, true>(bd, pc, nt, src, dst);
         else
-            BatchSweep<T, false>(bd, pc, src, dst);
+            BatchSweep<T, false>(bd, pc, nt, src, dst);
         if (s + 1 < nsteps && !GridBarrier(gs, my_gen)) return;
         pc.seed += 1;
     }
@@ -263,13 +275,13 @@ __global__ void BatchResidualFinalKernel(BatchDev bd,
 // as the first StreamCollision would do, into `a`.
 template <typename T>
 __global__ void BatchInitKernel(BatchDev bd, PhysConst pc,
-                                const int2* __restrict__ alltiles, int ntiles,
+                                const int4* __restrict__ alltiles, int ntiles,
                                 T* __restrict__ a) {
     using L = Lattice<2>;
     using P = Prec<T>;
     using C = typename P::C;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int2 tile = alltiles[t];
+        const int4 tile = alltiles[t];
         const BatchCav& cv = bd.cavs[tile.x];
         const int k = tile.y + threadIdx.x;
         if (k >= cv.n * cv.n) continue;
@@ -314,12 +326,14 @@ namespace mplb {
 template <typename T>
 struct BatchLaunch {
     static cudaError_t Step(bool macro, int grid, int threads, cudaStream_t s,
-                            const BatchDev& bd, const PhysConst& pc,
+                            const BatchDev& bd, const PhysConst& pc, int nt,
                             const T* src, T* dst) {
         if (macro)
-            BatchStepKernel<T, true><<<grid, threads, 0, s>>>(bd, pc, src, dst);
+            BatchStepKernel<T, true><<<grid, threads, 0, s>>>(bd, pc, nt, src,
+                                                              dst);
         else
-            BatchStepKernel<T, false><<<grid, threads, 0, s>>>(bd, pc, src, dst);
+            BatchStepKernel<T, false><<<grid, threads, 0, s>>>(bd, pc, nt, src,
+                                                               dst);
         return cudaGetLastError();
     }
     static cudaError_t Persistent(int grid, int threads, cudaStream_t s,
@@ -340,7 +354,7 @@ struct BatchLaunch {
     }
     static cudaError_t Init(int grid, int threads, cudaStream_t s,
                             const BatchDev& bd, const PhysConst& pc,
-                            const int2* alltiles, int ntiles, T* a) {
+                            const int4* alltiles, int ntiles, T* a) {
         BatchInitKernel<T><<<grid, threads, 0, s>>>(bd, pc, alltiles, ntiles,
                                                     a);
         return cudaGetLastError();

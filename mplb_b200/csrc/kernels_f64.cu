@@ -77,7 +77,7 @@ __global__ void BatchResidualPartialKernel(BatchDev bd,
     __shared__ double ws[32];
     const int nt = *bd.ntiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const int2 tile = bd.tiles[t];
+        const int4 tile = bd.tiles[t];
         const BatchCav& cv = bd.cavs[tile.x];
         const int k = tile.y + threadIdx.x;
         double v[6] = {0, 0, 0, 0, 0, 0};
