@@ -457,6 +457,10 @@ mplbgpu_status mplbgpu_batch_set_tuning(mplbgpu_batch* b,
     if (!b || !t) return MPLBGPU_ERR_INVALID;
     if (t->tile_nodes != 64 && t->tile_nodes != 128 && t->tile_nodes != 256)
         return BErr(b, MPLBGPU_ERR_INVALID, "tile_nodes must be 64, 128 or 256");
+    if (b->precision != MPLBGPU_FP64 &&
+        t->tile_nodes < 32 * BatchNodesPerThread<float>())
+        return BErr(b, MPLBGPU_ERR_INVALID,
+                    "tile_nodes too small for the FP32 form's nodes per thread");
     if (t->chunk < 2 || (t->chunk & 1))
         return BErr(b, MPLBGPU_ERR_INVALID, "chunk must be even and >= 2");
     if (t->ctas_per_sm < 1 || t->ctas_per_sm > 32)

@@ -97,29 +97,31 @@ __device__ __forceinline__ void BatchNode(const BatchDev& bd,
     }
 }
 
-// Two nodes of one cavity per thread, 32 apart (the FP32 form): both nodes'
-// loads are issued before either is computed, and each warp access covers
-// 256 contiguous bytes instead of 128.  Node kb is skipped when it lies
-// beyond the cavity (its loads then repeat node ka's).
-template <typename T, bool MACRO>
-__device__ __forceinline__ void BatchNodePair(const BatchDev& bd,
-                                              const PhysConst& pc,
-                                              const BatchCav& cv, int n,
-                                              long long base, float ninv,
-                                              int ka, bool second,
-                                              const T* __restrict__ src,
-                                              T* __restrict__ dst) {
+// G nodes of one cavity per thread, 32 apart (the FP32 form): all of their
+// loads are issued before any node is computed, and each warp access covers
+// 32 G contiguous values.  Nodes beyond the cavity are skipped (their loads
+// repeat node ka's).
+template <typename T, bool MACRO, int G>
+__device__ __forceinline__ void BatchNodeGroup(const BatchDev& bd,
+                                               const PhysConst& pc,
+                                               const BatchCav& cv, int n,
+                                               long long base, float ninv,
+                                               int ka,
+                                               const T* __restrict__ src,
+                                               T* __restrict__ dst) {
     using L = Lattice<2>;
     using P = Prec<T>;
     using C = typename P::C;
     constexpr int Q = 9;
     const int nn = n * n;   // a cavity's populations fit in 32-bit offsets
-    const int kk[2] = {ka, second ? ka + 32 : ka};
+    int kk[G];
+#pragma unroll
+    for (int j = 0; j < G; j++) kk[j] = ka + 32 * j < nn ? ka + 32 * j : ka;
     const T* s = src + base;
     T* d = dst + base;
-    C f[2][Q];
+    C f[G][Q];
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
+    for (int j = 0; j < G; j++) {
         const int k = kk[j];
         const int y = n <= 1024 ? (int)(((float)k + 0.5f) * ninv) : k / n;
         const int x = k - y * n;
@@ -139,8 +141,8 @@ __device__ __forceinline__ void BatchNodePair(const BatchDev& bd,
         }
     }
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
-        if (j == 1 && !second) break;
+    for (int j = 0; j < G; j++) {
+        if (j > 0 && ka + 32 * j >= nn) break;
         const int k = kk[j];
         double rho, u[3];
         MomentsCollideT<L, T>(f[j], pc, false, cv.omc, cv.omcf, rho, u);
@@ -155,11 +157,15 @@ __device__ __forceinline__ void BatchNodePair(const BatchDev& bd,
     }
 }
 
-// Threads per CTA of the step kernels for a tile of `tile_nodes` nodes:
-// two nodes per thread in the FP32 form.
+#ifndef MPLB_BATCH_GROUP
+#define MPLB_BATCH_GROUP 2
+#endif
+
+// Nodes per thread of the step kernels (threads per CTA = tile nodes / this):
+// MPLB_BATCH_GROUP in the FP32 form, one in FP64.
 template <typename T>
 __host__ __device__ constexpr int BatchNodesPerThread() {
-    return sizeof(T) < 8 ? 2 : 1;
+    return sizeof(T) < 8 ? MPLB_BATCH_GROUP : 1;
 }
 
 template <typename T, bool MACRO>
@@ -175,14 +181,15 @@ __device__ __forceinline__ void BatchSweep(const BatchDev& bd,
         const long long base = (long long)tile.w * (long long)(128 / sizeof(T));
         // the correctly rounded 1 / n, as the host computes it
         const float ninv = __frcp_rn((float)n);
-        if constexpr (BatchNodesPerThread<T>() == 2) {
-            // warp w has nodes [64 w, 64 w + 64) of the tile, lane l the
-            // nodes 64 w + l and 64 w + 32 + l
-            const int ka = tile.y + (int)(threadIdx.x >> 5) * 64 +
+        constexpr int G = BatchNodesPerThread<T>();
+        if constexpr (G > 1) {
+            // warp w has nodes [32 G w, 32 G (w + 1)) of the tile, lane l
+            // the nodes 32 G w + l + 32 j
+            const int ka = tile.y + (int)(threadIdx.x >> 5) * (32 * G) +
                            (int)(threadIdx.x & 31);
             if (ka < nn)
-                BatchNodePair<T, MACRO>(bd, pc, cv, n, base, ninv, ka,
-                                        ka + 32 < nn, src, dst);
+                BatchNodeGroup<T, MACRO, G>(bd, pc, cv, n, base, ninv, ka,
+                                            src, dst);
         } else {
             const int k = tile.y + threadIdx.x;
             if (k < nn)
