@@ -258,12 +258,15 @@ typedef struct {
 } mplbgpu_cavity;
 
 typedef struct {
-    int tile_nodes;  /* nodes per tile = threads per CTA: 64, 128 or 256 */
+    int tile_nodes;  /* nodes per tile: 64, 128 or 256; a CTA has one
+                        thread per node in FP64 and one per two nodes in
+                        FP32 */
     int persistent;  /* 1: one cooperative launch per chunk of steps with a
                         bounded grid barrier between steps; 0: one launch
                         per step, a chunk replayed from a CUDA graph */
     int chunk;       /* steps per chunk (even) */
-    int ctas_per_sm; /* CTAs per SM of the grid-stride launches */
+    int ctas_per_sm; /* CTAs per SM of the persistent launches (at most
+                        the co-resident count) */
 } mplbgpu_batch_tuning;
 
 typedef struct mplbgpu_batch mplbgpu_batch;

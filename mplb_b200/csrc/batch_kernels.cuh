@@ -38,7 +38,7 @@ struct BatchDev {
     // the populations
     const int4* tiles;
     const int* ntiles;      // number of active tiles (device word)
-    int tile_nodes;         // nodes per tile = threads per CTA
+    int tile_nodes;         // nodes per tile
     double* macro[3];       // rho, u, v of every cavity, packed
     double* macro_old[3];
 };
