@@ -1,0 +1,83 @@
+"""Seeded random single-block cases for parity checks: block shapes from
+two nodes to a few dozen per axis, every boundary surface defined in a
+random order, walls moving in random directions (normal components too,
+so some walls are inlets), an optional pressure outlet, optional
+periodic axes, an optional first-order body force with or without the
+force-shifted velocity moments, random relaxation time and initial state.
+Each case is small enough for the reference's CPU build to run in well
+under a second."""
+import math
+
+import numpy as np
+
+from mplb_b200 import config
+
+SQRT3 = math.sqrt(3.0)
+FACES = {2: ("Left", "Right", "Top", "Bottom"),
+         3: ("Left", "Right", "Top", "Bottom", "Front", "Back")}
+# surfaces paired across each axis (x, y, z)
+AXES = (("Left", "Right"), ("Bottom", "Top"), ("Back", "Front"))
+
+SEEDS = list(range(24))
+
+
+def random_case(seed: int):
+    """(case, steps) for one seed; check period = half the steps."""
+    rng = np.random.default_rng(1000 + seed)
+    dim = 2 if seed % 2 == 0 else 3
+    hi = 17 if dim == 2 else 9
+    size = tuple(int(rng.integers(2, hi)) for _ in range(dim))
+    mesh = 1.0 / (max(size) - 1)
+    dt = mesh / SQRT3
+    tau_l = float(rng.uniform(0.52, 1.3))
+    mt = ("Variable_U", "Variable_V", "Variable_W")[:dim]
+
+    # periodic axes: x in a third of the cases, z in a third of the 3D ones
+    periodic = []
+    if rng.random() < 1 / 3:
+        periodic.append(0)
+    if dim == 3 and rng.random() < 1 / 3:
+        periodic.append(2)
+    faces = [f for f in FACES[dim]
+             if not any(f in AXES[a] for a in periodic)]
+    outlet = faces[int(rng.integers(len(faces)))] \
+        if rng.random() < 0.3 else None
+    # every surface, periodic ones included, in a random definition order
+    order = list(FACES[dim])
+    rng.shuffle(order)
+    bounds = []
+    for f in order:
+        if f not in faces:
+            bounds.append(config.BoundaryDef(0, f, "MDPeriodic", "MDPeriodic"))
+        elif f == outlet:
+            bounds.append(config.BoundaryDef(
+                0, f, "ExtrapolPressure1ST", "OutLet",
+                (float(rng.uniform(0.99, 1.01)),), ("Variable_Rho",)))
+        else:
+            u = tuple(float(v) for v in SQRT3 * rng.uniform(-0.04, 0.04, dim))
+            bounds.append(config.BoundaryDef(0, f, "EQMDiffuseRefl", "Wall",
+                                             u, mt))
+    conns = []
+    for a in periodic:
+        lo, hi_face = AXES[a]
+        conns.append(config.ConnectionDef(0, lo, 0, hi_face, "MDPeriodic"))
+        conns.append(config.ConnectionDef(0, hi_face, 0, lo, "MDPeriodic"))
+
+    force = rng.random() < 0.5
+    accel = (0.0, 0.0, 0.0)
+    if force:
+        g = rng.uniform(-1e-4, 1e-4, 3) * mesh / (dt * dt)
+        accel = tuple(float(v) for v in g[:dim]) + (0.0,) * (3 - dim)
+    rho0 = float(rng.uniform(0.98, 1.02))
+    u0 = tuple(float(v) for v in SQRT3 * rng.uniform(-0.02, 0.02, 3))
+    steps = int(rng.integers(8, 31))
+    case = config.CaseConfig(
+        case_name=f"random{seed}", space_dim=dim, block_ids=[0],
+        block_names=["Box"], block_sizes=[size], mesh_size=mesh,
+        tau_ref=config.lattice_tau_to_tauref(tau_l, dt), boundaries=bounds,
+        connections=conns,
+        force_velocity=bool(force and rng.random() < 0.5),
+        body_force="BodyForce_1st" if force else "BodyForce_None",
+        accel=accel, initial=(rho0,) + u0[:dim] + (0.0,) * (3 - dim),
+        check_period=max(1, steps // 2))
+    return case, steps

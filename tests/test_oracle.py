@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import golden_cases
+import random_cases
 from mplb_b200 import config
 
 
@@ -154,3 +155,19 @@ def test_oracle_matches_reference_app_files(oracle_mod, name):
     o.step(steps)
     o.update_macro()
     assert golden_cases.fingerprint(case, o.f, o.macro) == want
+
+
+@pytest.mark.parametrize("seed", random_cases.SEEDS)
+def test_oracle_matches_reference_random_cases(oracle_mod, seed):
+    """Seeded random boxes (shapes, definition orders, moving and inflowing
+    walls, outlets, periodic axes, body forces): the oracle is the
+    reference bit for bit."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    case, steps = random_cases.random_case(seed)
+    ref = oracle_mod.run_reference(case, steps)
+    o, hist = run_oracle(oracle_mod, case, steps)
+    for got, want in zip(o.macro(0), ref["macro"][0]):
+        assert np.array_equal(got, want)
+    assert np.array_equal(o.f(0), ref["f"][0])
+    assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
