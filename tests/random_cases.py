@@ -81,3 +81,80 @@ def random_case(seed: int):
         accel=accel, initial=(rho0,) + u0[:dim] + (0.0,) * (3 - dim),
         check_period=max(1, steps // 2))
     return case, steps
+
+
+MULTI_SEEDS = list(range(12))
+
+
+def random_two_blocks(seed: int):
+    """(case, steps): two blocks joined through VirtualBoundary connections
+    along a random axis (block 0 below, block 1 above), equal extents
+    across the joint; every other surface of both blocks a moving wall, an
+    outlet or periodic, all defined in one random order."""
+    rng = np.random.default_rng(5000 + seed)
+    dim = 2 if seed % 2 == 0 else 3
+    hi = 13 if dim == 2 else 8
+    axis = int(rng.integers(dim))
+    base = [int(rng.integers(2, hi)) for _ in range(dim)]
+    sizes = []
+    for _ in range(2):
+        s = list(base)
+        s[axis] = int(rng.integers(2, hi))
+        sizes.append(tuple(s))
+    mesh = 1.0 / (max(max(s) for s in sizes) - 1)
+    dt = mesh / SQRT3
+    tau_l = float(rng.uniform(0.52, 1.3))
+    mt = ("Variable_U", "Variable_V", "Variable_W")[:dim]
+    lo_face, hi_face = AXES[axis]
+    # one periodic axis other than the joint's in a third of the cases
+    others = [a for a in range(dim) if a != axis]
+    periodic = int(rng.choice(others)) if rng.random() < 1 / 3 else None
+    items = [(b, f) for b in (0, 1) for f in FACES[dim]]
+    rng.shuffle(items)
+    outlet = None
+    if rng.random() < 0.4:
+        cand = [(b, f) for b, f in items
+                if not (b == 0 and f == hi_face) and not (b == 1 and f == lo_face)
+                and (periodic is None or f not in AXES[periodic])]
+        outlet = cand[int(rng.integers(len(cand)))]
+    bounds = []
+    for b, f in items:
+        if (b == 0 and f == hi_face) or (b == 1 and f == lo_face):
+            bounds.append(config.BoundaryDef(b, f, "None", "VirtualBoundary"))
+        elif periodic is not None and f in AXES[periodic]:
+            bounds.append(config.BoundaryDef(b, f, "MDPeriodic", "MDPeriodic"))
+        elif (b, f) == outlet:
+            bounds.append(config.BoundaryDef(
+                b, f, "ExtrapolPressure1ST", "OutLet",
+                (float(rng.uniform(0.99, 1.01)),), ("Variable_Rho",)))
+        else:
+            u = tuple(float(v) for v in SQRT3 * rng.uniform(-0.04, 0.04, dim))
+            bounds.append(config.BoundaryDef(b, f, "EQMDiffuseRefl", "Wall",
+                                             u, mt))
+    conns = [config.ConnectionDef(0, hi_face, 1, lo_face, "VirtualBoundary"),
+             config.ConnectionDef(1, lo_face, 0, hi_face, "VirtualBoundary")]
+    if periodic is not None:
+        p_lo, p_hi = AXES[periodic]
+        for b in (0, 1):
+            conns += [config.ConnectionDef(b, p_lo, b, p_hi, "MDPeriodic"),
+                      config.ConnectionDef(b, p_hi, b, p_lo, "MDPeriodic")]
+    start = {0: [0.0] * dim, 1: [0.0] * dim}
+    start[1][axis] = sizes[0][axis] * mesh
+    force = rng.random() < 0.5
+    accel = (0.0, 0.0, 0.0)
+    if force:
+        g = rng.uniform(-1e-4, 1e-4, 3) * mesh / (dt * dt)
+        accel = tuple(float(v) for v in g[:dim]) + (0.0,) * (3 - dim)
+    rho0 = float(rng.uniform(0.98, 1.02))
+    u0 = tuple(float(v) for v in SQRT3 * rng.uniform(-0.02, 0.02, 3))
+    steps = int(rng.integers(8, 25))
+    case = config.CaseConfig(
+        case_name=f"random2b{seed}", space_dim=dim, block_ids=[0, 1],
+        block_names=["Low", "High"], block_sizes=sizes, mesh_size=mesh,
+        tau_ref=config.lattice_tau_to_tauref(tau_l, dt), boundaries=bounds,
+        connections=conns, start_pos=start,
+        force_velocity=bool(force and rng.random() < 0.5),
+        body_force="BodyForce_1st" if force else "BodyForce_None",
+        accel=accel, initial=(rho0,) + u0[:dim] + (0.0,) * (3 - dim),
+        check_period=max(1, steps // 2))
+    return case, steps

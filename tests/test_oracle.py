@@ -171,3 +171,20 @@ def test_oracle_matches_reference_random_cases(oracle_mod, seed):
         assert np.array_equal(got, want)
     assert np.array_equal(o.f(0), ref["f"][0])
     assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
+
+
+@pytest.mark.parametrize("seed", random_cases.MULTI_SEEDS)
+def test_oracle_matches_reference_random_two_blocks(oracle_mod, seed):
+    """Seeded random pairs of blocks joined through VirtualBoundary
+    connections (halo transfer between blocks, edge nodes of the joint):
+    the oracle is the reference bit for bit."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    case, steps = random_cases.random_two_blocks(seed)
+    ref = oracle_mod.run_reference(case, steps)
+    o, hist = run_oracle(oracle_mod, case, steps)
+    for b in case.block_ids:
+        for got, want in zip(o.macro(b), ref["macro"][b]):
+            assert np.array_equal(got, want)
+        assert np.array_equal(o.f(b), ref["f"][b])
+    assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
