@@ -158,3 +158,41 @@ def random_two_blocks(seed: int):
         accel=accel, initial=(rho0,) + u0[:dim] + (0.0,) * (3 - dim),
         check_period=max(1, steps // 2))
     return case, steps
+
+
+SWAP_SEEDS = list(range(8))
+
+
+def random_swap_box(seed: int):
+    """(case, steps) for the one-array swap scheme: a 3D box (the scheme's
+    scope: one block, every surface an EQMDiffuseRefl wall) with random
+    shape, wall velocities, definition order, body force and initial
+    state."""
+    rng = np.random.default_rng(9000 + seed)
+    size = tuple(int(rng.integers(3, 12)) for _ in range(3))
+    mesh = 1.0 / (max(size) - 1)
+    dt = mesh / SQRT3
+    tau_l = float(rng.uniform(0.52, 1.3))
+    mt = ("Variable_U", "Variable_V", "Variable_W")
+    order = list(FACES[3])
+    rng.shuffle(order)
+    bounds = [config.BoundaryDef(
+        0, f, "EQMDiffuseRefl", "Wall",
+        tuple(float(v) for v in SQRT3 * rng.uniform(-0.04, 0.04, 3)), mt)
+        for f in order]
+    force = rng.random() < 0.5
+    accel = (0.0, 0.0, 0.0)
+    if force:
+        accel = tuple(float(v) for v in
+                      rng.uniform(-1e-4, 1e-4, 3) * mesh / (dt * dt))
+    rho0 = float(rng.uniform(0.98, 1.02))
+    u0 = tuple(float(v) for v in SQRT3 * rng.uniform(-0.02, 0.02, 3))
+    steps = int(rng.integers(8, 31))
+    case = config.CaseConfig(
+        case_name=f"randomswap{seed}", space_dim=3, block_ids=[0],
+        block_names=["Box"], block_sizes=[size], mesh_size=mesh,
+        tau_ref=config.lattice_tau_to_tauref(tau_l, dt), boundaries=bounds,
+        body_force="BodyForce_1st" if force else "BodyForce_None",
+        accel=accel, initial=(rho0,) + u0, check_period=max(1, steps // 2),
+        scheme="Scheme_StreamCollision_Swap")
+    return case, steps

@@ -188,3 +188,18 @@ def test_oracle_matches_reference_random_two_blocks(oracle_mod, seed):
             assert np.array_equal(got, want)
         assert np.array_equal(o.f(b), ref["f"][b])
     assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
+
+
+@pytest.mark.parametrize("seed", random_cases.SWAP_SEEDS)
+def test_oracle_matches_reference_random_swap_boxes(oracle_mod, seed):
+    """Seeded random boxes under the one-array swap scheme: the oracle's
+    swap step is the reference's bit for bit."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    case, steps = random_cases.random_swap_box(seed)
+    ref = oracle_mod.run_reference(case, steps)
+    o, hist = run_oracle(oracle_mod, case, steps)
+    for got, want in zip(o.macro(0), ref["macro"][0]):
+        assert np.array_equal(got, want)
+    assert np.array_equal(o.f(0), ref["f"][0])
+    assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
