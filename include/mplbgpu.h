@@ -161,7 +161,9 @@ typedef struct {
 typedef struct mplbgpu_ctx mplbgpu_ctx;
 
 /* Builds node classification, boundary tables and halo plans, allocates the
- * device state (Partition + DefineScheme + PrepareFlowField). */
+ * device state (Partition + DefineScheme + PrepareFlowField).  The
+ * description is checked before the device is looked for: a bad one gives
+ * MPLBGPU_ERR_INVALID / _UNSUPPORTED even where there is no GPU. */
 mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out);
 mplbgpu_status mplbgpu_destroy(mplbgpu_ctx* ctx);
 

@@ -377,13 +377,15 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     mplbgpu_ctx* ctx = nullptr;
     if (!desc || !out) return SetErr(nullptr, MPLBGPU_ERR_INVALID, "null argument");
     *out = nullptr;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
-        return SetErr(nullptr, MPLBGPU_ERR_NO_DEVICE, "no CUDA device");
+    // the description is checked before the device (the plan is host
+    // work), so a host without a GPU still tells a bad description apart
     std::unique_ptr<mplbgpu_ctx> c(new mplbgpu_ctx);
     std::string err;
     int rc = BuildPlan(*desc, &c->plan, &err);
     if (rc != MPLBGPU_OK) return SetErr(nullptr, rc, err);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        return SetErr(nullptr, MPLBGPU_ERR_NO_DEVICE, "no CUDA device");
     ctx = c.get();
     const Plan& P = c->plan;
     PhysConst& pc = c->pc;
