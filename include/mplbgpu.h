@@ -273,7 +273,8 @@ typedef struct {
 
 typedef struct mplbgpu_batch mplbgpu_batch;
 
-/* precision: MPLBGPU_FP64 or MPLBGPU_FP32_SHIFTED. */
+/* precision: MPLBGPU_FP64 or MPLBGPU_FP32_SHIFTED.  The cavities are checked
+ * before the device is looked for. */
 mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
                                     int precision, mplbgpu_batch** out);
 mplbgpu_status mplbgpu_batch_destroy(mplbgpu_batch* b);

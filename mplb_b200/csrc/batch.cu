@@ -336,9 +336,6 @@ mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
     if (precision != MPLBGPU_FP64 && precision != MPLBGPU_FP32_SHIFTED)
         return BErr(nullptr, MPLBGPU_ERR_UNSUPPORTED,
                     "batched cavities run in FP64 or shifted FP32");
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
-        return BErr(nullptr, MPLBGPU_ERR_NO_DEVICE, "no CUDA device");
     b = new mplbgpu_batch;
     b->precision = precision;
     b->cav.assign(cavities, cavities + ncav);
@@ -383,6 +380,12 @@ mplbgpu_status mplbgpu_batch_create(const mplbgpu_cavity* cavities, int ncav,
     if (base / align > 0x7fffffffLL) {   // tiles hold the offset in 32 bits
         delete b;
         return BErr(nullptr, MPLBGPU_ERR_INVALID, "batch too large");
+    }
+    // the cavities are checked before the device is looked for
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        delete b;
+        return BErr(nullptr, MPLBGPU_ERR_NO_DEVICE, "no CUDA device");
     }
     b->pop_elems = base;
     b->total_nodes = mbase;

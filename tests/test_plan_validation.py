@@ -187,3 +187,38 @@ def test_reference_app_files_accepted(lib):
     for name, (case, _, _) in apps.items():
         rc, msg = create(lib, case)
         assert accepted(rc), (name, rc, msg)
+
+
+def batch_create(lib, cavs, precision="fp32"):
+    arr = (abi.Cavity * max(len(cavs), 1))()
+    for i, (n, lid_u, tau_ref) in enumerate(cavs):
+        arr[i].n, arr[i].lid_u, arr[i].tau_ref = n, lid_u, tau_ref
+    h = ctypes.c_void_p()
+    rc = lib.mplbgpu_batch_create(arr, len(cavs), abi.PRECISIONS[precision],
+                                  ctypes.byref(h))
+    msg = lib.mplbgpu_batch_last_error(None).decode()
+    if rc == abi.OK:
+        lib.mplbgpu_batch_destroy(h)
+    return rc, msg
+
+
+@pytest.mark.parametrize("cavs,precision,code,words", [
+    ([], "fp32", abi.ERR_INVALID, "no cavities"),
+    ([(64, 0.05, 0.01)], "fp16", abi.ERR_UNSUPPORTED, "FP64 or shifted FP32"),
+    ([(64, 0.05, 0.01), (2, 0.05, 0.01)], "fp32", abi.ERR_INVALID,
+     "cavity side"),
+    ([(46341, 0.05, 0.01)], "fp64", abi.ERR_INVALID, "cavity side"),
+    ([(64, 0.05, -1.0)], "fp32", abi.ERR_INVALID, "tau_ref"),
+])
+def test_batch_rejected(lib, cavs, precision, code, words):
+    rc, msg = batch_create(lib, cavs, precision)
+    assert rc == code and words in msg, (rc, msg)
+
+
+def test_batch_accepted(lib):
+    from mplb_b200.batch import cavity_set
+    specs = cavity_set(64)
+    cavs = [(s.n, 3 ** 0.5 * s.lid, s.tau_ref) for s in specs]
+    for p in ("fp32", "fp64"):
+        rc, msg = batch_create(lib, cavs, p)
+        assert accepted(rc), (p, rc, msg)
