@@ -891,22 +891,23 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
             if (valid[1]) PopStore(dst + k1, __ushort_as_half(
                                                  (unsigned short)(pair >> 16)));
         }
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int j = 0; j < G; j++) {
-        if (!valid[j]) continue;
-        if constexpr (!kPair) MomentsCollideT<L, T>(f[j], pc, fl);
-        Rng rg = SeedRng(pc.seed, node[j]);
-        if constexpr (O32) {
-            T* pd = dst + node[j];
+        for (int j = 0; j < G; j++) {
+            if (!valid[j]) continue;
+            if constexpr (!kPair) MomentsCollideT<L, T>(f[j], pc, fl);
+            Rng rg = SeedRng(pc.seed, node[j]);
+            if constexpr (O32) {
+                T* pd = dst + node[j];
 #pragma unroll
-            for (int i = 0; i < Q; i++)
-                P::Store(pd, b.pop_off32[i], i, f[j][i], pc, rg);
-        } else {
+                for (int i = 0; i < Q; i++)
+                    P::Store(pd, b.pop_off32[i], i, f[j][i], pc, rg);
+            } else {
 #pragma unroll
-            for (int i = 0; i < Q; i++)
-                P::Store(dst, OwnIndex(b, node[j], i), i, f[j][i], pc, rg);
+                for (int i = 0; i < Q; i++)
+                    P::Store(dst, OwnIndex(b, node[j], i), i, f[j][i], pc,
+                             rg);
+            }
         }
     }
 }

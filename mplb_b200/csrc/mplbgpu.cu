@@ -374,7 +374,6 @@ int FaceCopy(mplbgpu_ctx* ctx, size_t bi, const FaceDev& fd, bool exp,
 extern "C" {
 
 mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
-    mplbgpu_ctx* ctx = nullptr;
     if (!desc || !out) return SetErr(nullptr, MPLBGPU_ERR_INVALID, "null argument");
     *out = nullptr;
     // the description is checked before the device (the plan is host
@@ -386,7 +385,6 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
         return SetErr(nullptr, MPLBGPU_ERR_NO_DEVICE, "no CUDA device");
-    ctx = c.get();
     const Plan& P = c->plan;
     PhysConst& pc = c->pc;
     pc.cs = P.cs;
