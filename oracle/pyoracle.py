@@ -6,8 +6,8 @@
   reference's own sources built against the sequential OPS stand-in) on a
   case written in the reference's JSON format.
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
-this module.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg and
+reference arm (`--impl reference`) use this module.
 """
 import ctypes
 import json
