@@ -202,9 +202,13 @@ class CaseConfig:
         i = 0
         while js.get(f"BoundaryCondition{i}") is not None:
             bc = js[f"BoundaryCondition{i}"]
+            # the reference's files spell it "EQMDiffuseREfl"
+            sch = bc["BoundaryScheme"]
+            if sch == "EQMDiffuseREfl":
+                sch = "EQMDiffuseRefl"
             bounds.append(BoundaryDef(
                 block=int(bc["BlockIndex"]), surface=bc["BoundarySurface"],
-                scheme=bc["BoundaryScheme"], vertex_type=bc["BoundaryType"],
+                scheme=sch, vertex_type=bc["BoundaryType"],
                 given=tuple(float(v) for v in bc.get("GivenVars", [])),
                 macro_types=tuple(bc.get("MacroVarTypesatBoundary", []))))
             i += 1
