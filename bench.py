@@ -65,8 +65,16 @@ def parse():
     p.add_argument("--precision", default="fp64",
                    choices=["fp64", "fp32", "fp16"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--min-time", type=float, default=1.0,
+                   help="seconds of timed work: the K-step timed region is "
+                        "repeated until this much has run, so that the clock "
+                        "sampler sees the load (0: one repetition)")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the FP32/FP16 runs of the same case that the "
+                        "FP64 line reports beside its own")
     p.add_argument("--workload", default="cavity3d",
-                   choices=["cavity3d", "cavities", "cavities-warmstart"],
+                   choices=["cavity3d", "cavities", "cavities-warmstart",
+                            "precision", "lchannel"],
                    help="cavities: throughput of the 4,096 batched D2Q9 "
                         "cavities split over the ranks; cavities-warmstart: "
                         "the learned warm start experiment (minutes; 1 GPU)")
@@ -75,6 +83,10 @@ def parse():
                         "(its first ones; 4,096 is the workload, fewer "
                         "make a small case for profiling)")
     p.add_argument("--epochs", type=int, default=200)
+    p.add_argument("--lsteps", type=int, default=10000,
+                   help="lchannel: steps (checks every 1,000)")
+    p.add_argument("--quick", action="store_true",
+                   help="precision: small channels instead of the full ones")
     p.add_argument("--decomp", default="replicas",
                    choices=["replicas", "slab"],
                    help="N > 1 on the cavity: independent 256^3 replicas, or "
@@ -198,6 +210,33 @@ def barrier(world):
         dist.barrier()
 
 
+def repeat_timed(run_k, world, min_s=1.0, max_reps=2000):
+    """Times run_k() - exactly K steps between a barrier and a device
+    synchronize, returning its device milliseconds - again and again until
+    at least min_s seconds of timed work have run, so that the clock
+    sampler (200 ms period) sees the load.  Every rank runs the same number
+    of repetitions (fixed from the slowest rank's first one).  Returns the
+    per-repetition max-over-ranks device times."""
+    first = max_over_ranks(run_k(), world)
+    reps = int(min(max_reps, max(1, -(-min_s * 1e3 // max(first, 1e-3)))))
+    times = [first]
+    for _ in range(reps - 1):
+        times.append(max_over_ranks(run_k(), world))
+    return times
+
+
+def cpu_model():
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True,
+                             timeout=10).stdout
+    except (OSError, subprocess.SubprocessError):
+        return None
+    for line in out.splitlines():
+        if line.startswith("Model name:"):
+            return line.split(":", 1)[1].strip()
+    return None
+
+
 def max_over_ranks(v, world):
     if world <= 1:
         return v
@@ -208,14 +247,33 @@ def max_over_ranks(v, world):
     return float(t.item())
 
 
+def cavity_config(args, world, nodes):
+    """The `config` of the cavity workload's line (both arms)."""
+    swap = args.scheme == "swap"
+    return {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
+                        f"{args.precision.upper()}, lid 0.05 (lattice), "
+                        "Re 400" + (", swap scheme (one array)" if swap
+                                    else ""),
+            "nodes_per_gpu": nodes, "parallelism": f"replicas{world}",
+            "l2": "population arrays of 0.7-2.7 GB each, larger than L2"}
+
+
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU implementation of the step (oracle/_ref: its
+    sources against the sequential OPS stand-in, OpenMP over every host
+    core) on the same case, the same config and warm-up; K steps, or fewer
+    where K would take more than a few minutes (the line says how many)."""
     case = workload(args.size, "fp64", args.scheme)
     swap = args.scheme == "swap"
     step_name = "SwapStreamCollision" if swap else "StreamCollision"
     if rank != 0:
         return
-    res = cpu_reference(case, max(1, min(args.warmup, 1)), args.steps,
-                        budget_s=120)
+    if args.precision != "fp64":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference computes in FP64 only; its arm "
+                          "runs with --precision fp64"}))
+        return
+    res = cpu_reference(case, args.warmup, args.steps, budget_s=150)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference CPU build (oracle/_ref) not present"}))
@@ -226,19 +284,17 @@ def run_reference_arm(args, rank, world):
         "metric": METRIC if not swap else METRIC[:-1] +
         ", one-array swap scheme)", "value": mlups,
         "unit": "MLUPS", "n_gpus": args.gpus, "steps": n,
-        "warmup": 1, "ms_per_step": secs / n * 1e3,
+        "warmup": args.warmup, "ms_per_step": secs / n * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
-                               "FP64, lid 0.05, Re 400" +
-                               (", swap scheme (one array)" if swap else ""),
-                   "nodes": case.nodes()},
+        "config": cavity_config(args, world, case.nodes()),
         "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads,
-                         "kind": "reference",
+                         "kind": "reference", "cpu_model": cpu_model(),
                          "sample": f"{n} {step_name} steps of the "
-                                   f"{args.size}^3 cavity after 1 warm-up "
-                                   "step (reference sources + sequential "
-                                   "OPS stand-in, OpenMP)"},
+                                   f"{args.size}^3 cavity after "
+                                   f"{args.warmup} warm-up steps (reference "
+                                   "sources + sequential OPS stand-in, "
+                                   "OpenMP)"},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -252,27 +308,37 @@ def run_cavities(args, rank, world, local):
     every cavity after W warm-up steps, CUDA events on each batch's stream,
     max over ranks."""
     import torch
-    from mplb_b200.batch import Batch, cavity_set, shard
+    from mplb_b200.batch import Batch, autotune, cavity_set, shard
     torch.cuda.set_device(local)
     specs = cavity_set(args.cavities)
     mine = [specs[i] for i in shard(specs, rank, world)]
     b = Batch(mine, "fp32")
-    b.set_tuning(tile_nodes=128, persistent=0, chunk=50, ctas_per_sm=8)
+    # the autotuner times every candidate on this rank's cavities and
+    # leaves the fastest set (a fresh choice: the cache is not consulted)
+    tuned = autotune(b, steps=200, force=True,
+                     cache=os.path.join(tempfile.mkdtemp(), "tuning.json"))
     b.init()
     b.step(max(args.warmup, 50))
     s0 = b.stats()
+
+    def run_k():
+        barrier(world)
+        a = b.stats()
+        b.step(args.steps)        # CUDA events on the batch's stream
+        z = b.stats()
+        barrier(world)
+        return z["device_ms"] - a["device_ms"]
+
     clocks = ClockSampler(local)
     clocks.start()
-    barrier(world)
-    b.step(args.steps)
-    barrier(world)
+    times = repeat_timed(run_k, world, args.min_time)
     clk = clocks.stop()
     s1 = b.stats()
-    ms = max_over_ranks(s1["device_ms"] - s0["device_ms"], world)
+    ms = statistics.median(times)
     total_nodes = sum(s.n * s.n for s in specs)
     value = total_nodes * args.steps / (ms * 1e-3) / 1e6
     peak, peak_kind = measured_peaks()
-    launches = s1["launches"] - s0["launches"]
+    launches = (s1["launches"] - s0["launches"]) // len(times)
     b.close()
     if rank != 0:
         return
@@ -292,10 +358,16 @@ def run_cavities(args, rank, world, local):
                    "nodes": total_nodes,
                    "parallelism": f"cavities split over {world} GPU(s) "
                                   "(LPT on nodes)"},
+        "timing": {"repetitions": len(times),
+                   "statistic": "median over repetitions of K timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "bytes_per_node": 72,
                      "traffic": None},
+        "tuning": tuned["tuning"],
+        "autotune": [{"mlups": round(r["mlups"], 1),
+                      **{k: v for k, v in r.items() if k != "mlups"}}
+                     for r in tuned["all"]],
         "clocks": clk, "gpu_launches": launches}))
 
 
@@ -332,6 +404,196 @@ def run_warmstart(args, rank, local):
         "clocks": clk,
     }
     print(json.dumps(line))
+
+
+def interface_continuity(s):
+    """Per interface of the L-channel (inlet leg | corner across x, corner |
+    outlet leg across y) and per moment: the largest jump between the two
+    blocks' nodes that face each other across the joint, and the largest
+    difference between the same layer and the next one inside the first
+    block (the size of one grid spacing's change where nothing is joined).
+    A jump of the order of the in-block difference is a continuous field."""
+    import numpy as np
+    m = [s.macro(b) for b in (0, 1, 2)]
+    names = ["rho", "u", "v", "w"]
+    out = {}
+    for label, a, b, axis in (("inlet_leg|corner", 0, 1, 2),
+                              ("corner|outlet_leg", 1, 2, 1)):
+        rec = {}
+        for q, name in enumerate(names):
+            qa, qb = m[a][q], m[b][q]
+            last = np.take(qa, -1, axis=axis)
+            prev = np.take(qa, -2, axis=axis)
+            first = np.take(qb, 0, axis=axis)
+            rec[name] = {"jump": float(np.abs(first - last).max()),
+                         "in_block": float(np.abs(last - prev).max())}
+        out[label] = rec
+    return out
+
+
+def run_lchannel(args, rank, local):
+    """The 3-block L-channel (384 x 128 x 128 inlet leg, 128^3 corner,
+    128 x 384 x 128 outlet leg = 14,680,064 nodes; D3Q19 BGK, tau_L 0.6,
+    z-periodic, EQMDiffuseRefl walls, pressure outlet rho = 1) with the
+    inlet at u_x = 0.03 lattice units plus a seeded uniform +-1 %
+    perturbation per node (seed 20261203), from rest, for --lsteps steps
+    (10,000) in periods of 1,000.  Device time of the steps (CUDA events
+    on the library's stream; the check-period work outside it) gives the
+    MLUPS; at each check: total mass (FP64 sum of rho), the residual and
+    the continuity of the moments across the two block joints."""
+    import torch
+    from mplb_b200 import Solver, config
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    case = config.lchannel(precision=args.precision)
+    k, comps = config.inlet_perturbation(case, seed=20261203, amplitude=0.01)
+    s = Solver(case)
+    s.set_boundary_velocity(k, *comps)
+    s.init_uniform()
+    nodes = case.nodes()
+    mass0 = s.mass()
+    cp = 1000
+    launches0 = s.launch_count()
+    device_ms, history = 0.0, []
+    clocks = ClockSampler(local)
+    clocks.start()
+    done = 0
+    while done < args.lsteps:
+        n = min(cp, args.lsteps - done)
+        s.stream_collision(n)
+        device_ms += s.last_step_ms()
+        done += n
+        s.update_macro_vars()
+        mass = s.mass()
+        res, _ = s.calc_residual_error(n)
+        history.append({"step": done, "mass": mass,
+                        "mass_change": mass - mass0,
+                        "residual": res,
+                        "continuity": interface_continuity(s)})
+    clk = clocks.stop()
+    launches = s.launch_count() - launches0
+    s.close()
+    value = nodes * args.lsteps / (device_ms * 1e-3) / 1e6
+    bpn = BYTES_PER_NODE[(args.precision, 3)]
+    achieved = bpn * nodes / (device_ms / args.lsteps * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": "MLUPS (3-block D3Q19 L-channel, 14,680,064 nodes)",
+        "value": value, "unit": "MLUPS", "n_gpus": 1,
+        "steps": args.lsteps, "warmup": 0,
+        "ms_per_step": device_ms / args.lsteps, "higher_is_better": True,
+        "scaling": "none", "vs_baseline": None,
+        "dtype": DTYPES[args.precision], "data": "synthetic",
+        "config": {"workload": "L-channel: 384x128x128 inlet leg, 128^3 "
+                               "corner, 128x384x128 outlet leg, tau_L 0.6, "
+                               "z-periodic, inlet u_x 0.03 (lattice) "
+                               "+-1 % per node (seed 20261203), outlet "
+                               "rho 1, from rest",
+                   "nodes": nodes, "parallelism": "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_node": bpn,
+                     "traffic": None},
+        "mass_initial": mass0,
+        "history": history,
+        "clocks": clk,
+        "gpu_launches": launches,
+        "launches_per_step": launches / args.lsteps,
+    }
+    print(json.dumps(line))
+
+
+# --- precision study of the storage forms (forced channels) --------------
+SQRT3 = 3.0 ** 0.5
+
+
+def analytic_u(ny, g, tau, wall):
+    import numpy as np
+    """Lattice-unit profile: walls half a spacing outside the first/last
+    node for halfway bounce-back (H = ny), on the first/last node for
+    EQMDiffuseRefl (H = ny - 1)."""
+    nu = (tau - 0.5) / 3.0
+    if wall == "HalfwayBounceBack":
+        y = np.arange(ny) + 0.5
+        h = ny
+    else:
+        y = np.arange(ny, dtype=float)
+        h = ny - 1
+    return g / (2.0 * nu) * y * (h - y)
+
+
+def rel(a, b):
+    import numpy as np
+    d = a - b
+    nb = np.linalg.norm(b)
+    mb = np.abs(b).max()
+    return (float(np.linalg.norm(d) / nb) if nb > 0 else float("nan"),
+            float(np.abs(d).max() / mb) if mb > 0 else float("nan"))
+
+
+def run_channel(dim, nx, ny, nz, steps, precision, wall, g=1e-6, tau=0.8):
+    from mplb_b200 import Solver, config
+    case = config.poiseuille(dim, nx, ny, nz, g_lattice=g, tau_lattice=tau,
+                             wall=wall, precision=precision)
+    import numpy as np
+    ua = analytic_u(ny, g, tau, wall) * SQRT3
+    shape = (nz, ny, nx) if dim == 3 else (1, ny, nx)
+    start = "analytic" if ua.max() / SQRT3 < 0.3 else "rest"
+    u0 = np.broadcast_to(ua[None, :, None], shape) if start == "analytic" \
+        else 0.0
+    with Solver(case) as s:
+        s.init_macro(0, 1.0, u0, 0.0, 0.0 if dim == 3 else None)
+        s.stream_collision(steps)
+        ms = s.last_step_ms()
+        s.update_macro_vars()
+        m = s.macro(0)
+    mlups = case.nodes() * steps / (ms * 1e-3) / 1e6
+    return m, mlups, ua, start
+
+
+def run_precision(args):
+    """Body-force Poiseuille channels (D2Q9 4096 x 1024 for 50,000 steps and
+    D3Q19 512 x 256 x 256 for 10,000 steps; tau_L = 0.8, g_L = 1e-6 along x;
+    walls at y-min/y-max, periodic in x and z) in the FP64 form (bit-
+    identical to the reference), the shifted FP32 form and the FP16-storage
+    form.  The channels' viscous times H^2/nu (10^7 and 6.6 x 10^5 steps)
+    are far longer than the prescribed runs: where the analytic profile is
+    subsonic (the 3D channel, peak 0.082 lattice units) the flow starts
+    from it and the error against it measures discretisation and storage
+    error; the 2D profile would peak at 1.31 lattice units, so that channel
+    starts from rest.  One JSON line per run: relative L2 and max errors of
+    rho and u against the FP64 form, of u against the profile, and the
+    device-time MLUPS.  --quick runs small channels."""
+    quick = args.quick
+    runs = [(2, 4096, 1024, 1, 50000), (3, 512, 256, 256, 10000)]
+    if quick:
+        runs = [(2, 256, 64, 1, 4000), (3, 64, 32, 32, 1000)]
+    for dim, nx, ny, nz, steps in runs:
+        for wall in ("HalfwayBounceBack", "EQMDiffuseRefl"):
+            ref, ref_mlups, ua, start = run_channel(dim, nx, ny, nz, steps,
+                                                    "fp64", wall)
+            for prec in ("fp64", "fp32", "fp16"):
+                if prec == "fp64":
+                    m, mlups = ref, ref_mlups
+                else:
+                    m, mlups, _, _ = run_channel(dim, nx, ny, nz, steps,
+                                                 prec, wall)
+                u = m[1]
+                import numpy as np
+                prof = u.mean(axis=(0, 2)) / SQRT3
+                line = {
+                    "study": "precision", "dim": dim,
+                    "grid": [nx, ny] + ([nz] if dim == 3 else []),
+                    "steps": steps, "wall": wall, "precision": prec,
+                    "start": start,
+                    "mlups": mlups,
+                    "rho_vs_fp64": rel(m[0], ref[0]),
+                    "u_vs_fp64": rel(u, ref[1]),
+                    "u_vs_analytic": rel(prof, ua / SQRT3),
+                }
+                print(json.dumps(line), flush=True)
+
 
 
 def run_slab(args, rank, world, local):
@@ -460,6 +722,15 @@ def main():
     if args.workload == "cavities-warmstart":
         run_warmstart(args, rank, local)
         return
+    if args.workload == "lchannel":
+        run_lchannel(args, rank, local)
+        return
+    if args.workload == "precision":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            run_precision(args)
+        return
     if args.decomp == "slab" and args.workload == "cavity3d":
         run_slab(args, rank, world, local)
         return
@@ -477,29 +748,53 @@ def main():
     swap = args.scheme == "swap"
 
     # --- device-resident timing ------------------------------------------
-    s = Solver(case, lib)
-    s.init_uniform()
-    s.stream_collision(args.warmup)
-    s.synchronize()
-    launches0 = s.launch_count()
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier(world)
-    torch.cuda.synchronize()
-    s.stream_collision(args.steps)     # CUDA events on the library's stream
-    torch.cuda.synchronize()
-    barrier(world)
-    clk = clocks.stop()
-    ms = s.last_step_ms()
-    launches = s.launch_count() - launches0
-    ms_max = max_over_ranks(ms, world)
+    def device_run(prec):
+        """K steps of the cavity in storage form `prec`, repeated for at
+        least a second under the clock sampler; returns (median device ms of
+        K steps, launches per K steps, clocks, per-repetition ms)."""
+        c = workload(args.size, prec, args.scheme)
+        s = Solver(c, lib)
+        s.init_uniform()
+        s.stream_collision(args.warmup)
+        s.synchronize()
+        launches0 = s.launch_count()
+
+        def run_k():
+            barrier(world)
+            torch.cuda.synchronize()
+            s.stream_collision(args.steps)   # CUDA events on its stream
+            ms = s.last_step_ms()            # waits for the K steps
+            barrier(world)
+            return ms
+
+        clocks = ClockSampler(local)
+        clocks.start()
+        times = repeat_timed(run_k, world, args.min_time)
+        clk = clocks.stop()
+        launches = (s.launch_count() - launches0) // len(times)
+        s.close()
+        return statistics.median(times), launches, clk, times
+
+    ms_max, launches, clk, times = device_run(args.precision)
     value = world * nodes * args.steps / (ms_max * 1e-3) / 1e6
-    kernel_ms = ms / args.steps          # one kernel launch per step
+    kernel_ms = ms_max / args.steps      # one kernel launch per step
     bpn = BYTES_PER_NODE[(case.precision, 3)]
     achieved = bpn * nodes / (kernel_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    s.close()
-    del s
+    forms = {}
+    if args.precision == "fp64" and not args.no_forms:
+        # the shifted forms of the same case (precision target: FP32 at
+        # >= 1.8x the FP64 node rate)
+        for prec, key in (("fp32", "fp32_shifted"), ("fp16", "fp16_storage")):
+            fms, _, fclk, _ = device_run(prec)
+            fb = BYTES_PER_NODE[(prec, 3)]
+            fach = fb * nodes / (fms / args.steps * 1e-3) / 1e9
+            fv = world * nodes * args.steps / (fms * 1e-3) / 1e6
+            forms[key] = {"value": fv, "unit": "MLUPS",
+                          "ms_per_step": fms / args.steps,
+                          "vs_fp64": fv / value, "bytes_per_node": fb,
+                          "achieved_gbs": fach, "frac": fach / peak,
+                          "dtype": DTYPES[prec], "sm_mhz": fclk["sm_mhz"]}
 
     # --- end to end through the C ABI with host buffers ------------------
     shp = (nz, ny, nx)
@@ -537,13 +832,19 @@ def main():
         res = cpu_reference(case, 1, 5, budget_s=25)
         if res is not None:
             mlups, n, threads, secs = res
+            name = "SwapStreamCollision" if swap else "StreamCollision"
             cpu = {"value": mlups, "unit": "MLUPS", "cores": threads,
-                   "kind": "reference",
-                   "sample": f"{n} {'SwapStreamCollision' if swap else 'StreamCollision'} "
-                             f"steps of the same "
-                             f"{args.size}^3 cavity after 1 warm-up step "
-                             "(reference sources + sequential OPS stand-in, "
-                             "OpenMP)"}
+                   "kind": "reference", "cpu_model": cpu_model(),
+                   "sample": f"{n} {name} steps of the same {args.size}^3 "
+                             "cavity after 1 warm-up step (reference "
+                             "sources + sequential OPS stand-in, OpenMP)"}
+            one = cpu_reference(case, 1, 2, budget_s=10, threads=1)
+            if one is not None:
+                m1, n1, _, _ = one
+                cpu["single_thread"] = {
+                    "value": m1, "unit": "MLUPS", "cores": 1,
+                    "sample": f"{n1} {name} steps after 1 warm-up step "
+                              "(the same build without OpenMP: OPS seq)"}
     metric = METRIC if not swap else METRIC[:-1] + ", one-array swap scheme)"
     traffic = (TRAFFIC_PER_NODE[(case.precision, 3)] * nodes
                if (case.precision, 3) in TRAFFIC_PER_NODE and not swap
@@ -554,13 +855,11 @@ def main():
         "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": DTYPES[args.precision], "data": "synthetic",
-        "config": {"workload": f"3D lid-driven cavity D3Q19 {args.size}^3 "
-                               f"{args.precision.upper()}, lid 0.05 "
-                               "(lattice), Re 400" +
-                               (", swap scheme (one array)" if swap else ""),
-                   "nodes_per_gpu": nodes, "parallelism": f"replicas{world}",
-                   "l2": "population arrays of 0.7-2.7 GB each, larger "
-                         "than L2"},
+        "config": cavity_config(args, world, nodes),
+        "timing": {"repetitions": len(times),
+                   "statistic": "median over repetitions of K timed steps",
+                   "ms_per_step_min": min(times) / args.steps,
+                   "ms_per_step_max": max(times) / args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
@@ -573,6 +872,8 @@ def main():
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if forms:
+        line["forms"] = forms
     print(json.dumps(line))
 
 

@@ -241,6 +241,16 @@ def _cache_key(batch: Batch) -> str:
     return f"{name}|{batch.precision}|{h[:12]}"
 
 
+def default_candidates():
+    """Tile size x launch style (x CTAs per SM, which only the persistent
+    launch uses)."""
+    graph = [dict(tile_nodes=t, persistent=0, chunk=50, ctas_per_sm=8)
+             for t in (64, 128, 256)]
+    persistent = [dict(tile_nodes=t, persistent=1, chunk=50, ctas_per_sm=k)
+                  for t in (128, 256) for k in (4, 8)]
+    return graph + persistent
+
+
 def autotune(batch: Batch, steps: int = 200, cache: str = DEFAULT_CACHE,
              candidates=None, force=False):
     """Times each candidate tuning on `batch` (from its initial state) and
@@ -254,9 +264,7 @@ def autotune(batch: Batch, steps: int = 200, cache: str = DEFAULT_CACHE,
         batch.set_tuning(**table[key]["tuning"])
         return table[key]
     if candidates is None:
-        candidates = [dict(tile_nodes=t, persistent=p, chunk=c, ctas_per_sm=k)
-                      for t in (128, 256) for p in (0, 1)
-                      for c in (50,) for k in (4, 8)]
+        candidates = default_candidates()
     results = []
     for cand in candidates:
         batch.set_tuning(**cand)

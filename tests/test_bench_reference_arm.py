@@ -7,6 +7,7 @@ import os
 import socket
 import subprocess
 import sys
+import types
 
 import pytest
 
@@ -39,9 +40,13 @@ def test_reference_line_keys(scheme):
     assert d["impl"] == "reference"
     assert d["unit"] == "MLUPS" and d["value"] > 0
     assert d["higher_is_better"] is True
-    assert 1 <= d["steps"] <= 3 and d["warmup"] >= 1
+    assert d["steps"] == 3 and d["warmup"] == 1
     assert d["ms_per_step"] > 0
-    assert d["config"]["nodes"] == 20 ** 3
+    # the same config as the B200 arm's line for the same arguments
+    import bench
+    args = types.SimpleNamespace(size=20, scheme=scheme, precision="fp64")
+    assert d["config"] == bench.cavity_config(args, 1, 20 ** 3)
+    assert d["cpu_baseline"]["sample"].count("1 warm-up") == 1
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1
     assert cb["value"] == d["value"]
