@@ -50,9 +50,13 @@ struct lbm_oracle {
     oblock* b;
     int nbc;
     mplbgpu_boundary* bc;
+    double** bc_field; /* per boundary: (u, v, w) per node of its range or
+                          NULL (a new-build extension of GivenVars) */
     int nhalo;
     ohalo* halo;
 };
+
+static oblock* find_block(lbm_oracle* o, int id);
 
 static char g_err[256];
 const char* lbmo_error(void) { return g_err; }
@@ -412,6 +416,7 @@ int lbmo_create(const mplbgpu_desc* d, lbm_oracle** out) {
     o->nbc = d->nboundaries;
     o->bc = (mplbgpu_boundary*)calloc((size_t)(o->nbc + 1),
                                       sizeof(mplbgpu_boundary));
+    o->bc_field = (double**)calloc((size_t)(o->nbc + 1), sizeof(double*));
     for (int i = 0; i < o->nbc; i++) {
         o->bc[i] = d->boundaries[i];
         if (!valid_surface(o->dim, o->bc[i].surface)) {
@@ -569,9 +574,42 @@ void lbmo_destroy(lbm_oracle* o) {
         free(b->vg);
     }
     free(o->b);
+    for (int i = 0; i < o->nbc; i++) free(o->bc_field[i]);
+    free(o->bc_field);
     free(o->bc);
     free(o->halo);
     free(o);
+}
+
+int lbmo_boundary_extent(lbm_oracle* o, int boundary, int ext[3]) {
+    if (boundary < 0 || boundary >= o->nbc) return fail("unknown boundary");
+    oblock* b = find_block(o, o->bc[boundary].block);
+    if (!b) return fail("unknown block");
+    int r[6];
+    surface_range(o, b, o->bc[boundary].surface, r);
+    for (int a = 0; a < 3; a++) ext[a] = r[2 * a + 1] - r[2 * a];
+    return 0;
+}
+
+int lbmo_set_boundary_velocity(lbm_oracle* o, int boundary, const double* u,
+                               const double* v, const double* w) {
+    int ext[3];
+    if (lbmo_boundary_extent(o, boundary, ext) != 0) return -1;
+    const int s = o->bc[boundary].scheme;
+    if (s != MPLBGPU_BC_EQM_DIFFUSE_REFL && s != MPLBGPU_BC_HALFWAY_BOUNCE_BACK)
+        return fail("per-node velocity on a boundary without a wall kernel");
+    if (o->swap) return fail("per-node velocity under the swap scheme");
+    free(o->bc_field[boundary]);
+    o->bc_field[boundary] = NULL;
+    if (!u && !v && !w) return 0;
+    const size_t cnt = (size_t)ext[0] * ext[1] * ext[2];
+    double* f = (double*)calloc(3 * cnt, sizeof(double));
+    const double* src[3] = {u, v, o->dim == 3 ? w : NULL};
+    for (int c = 0; c < 3; c++)
+        if (src[c])
+            for (size_t k = 0; k < cnt; k++) f[3 * k + c] = src[c][k];
+    o->bc_field[boundary] = f;
+    return 0;
 }
 
 static oblock* find_block(lbm_oracle* o, int id) {
@@ -674,14 +712,27 @@ int lbmo_set_f(lbm_oracle* o, int block, const double* f) {
 }
 
 /* KerCutCellEQMDiffuseRefl(3D), Src/boundary_kernel.inc:534-613,1184-1276 */
+/* Wall velocity of node (i, j, k) of range r: the boundary's uniform
+ * GivenVars, or its entry of a per-node field over the range (x fastest;
+ * not in the reference, whose GivenVars are uniform). */
+static const double* wall_velocity(const double* given, const double* field,
+                                   const int r[6], int i, int j, int k) {
+    if (!field) return given;
+    const size_t idx = ((size_t)(k - r[4]) * (size_t)(r[3] - r[2]) +
+                        (size_t)(j - r[2])) * (size_t)(r[1] - r[0]) +
+                       (size_t)(i - r[0]);
+    return &field[3 * idx];
+}
+
 static void bc_eqm(lbm_oracle* o, oblock* b, const int r[6],
-                   const double* given) {
+                   const double* given, const double* field) {
     const double CS = o->cs;
     const int D = o->dim, Q = o->Q;
-    const double u = given[0], v = given[1], w = D == 3 ? given[2] : 0.0;
     for (int k = r[4]; k < r[5]; k++)
         for (int j = r[2]; j < r[3]; j++)
             for (int i = r[0]; i < r[1]; i++) {
+                const double* g = wall_velocity(given, field, r, i, j, k);
+                const double u = g[0], v = g[1], w = D == 3 ? g[2] : 0.0;
                 const size_t p = pidx(b, i, j, k);
                 const int vg = b->vg[p];
                 double* f = &b->f[p * Q];
@@ -838,7 +889,8 @@ static int surface_sides(int s, int axis[2], int side[2]) {
  * faces takes the node's own post-collision opposite population plus
  * 2 w_l (c_l . u_wall); the wall sits half a spacing beyond the face. */
 static void bc_halfway_bb(lbm_oracle* o, oblock* b, const int r[6],
-                          int surface, const double* given) {
+                          int surface, const double* given,
+                          const double* field) {
     const double CS = o->cs;
     const int D = o->dim, Q = o->Q;
     int axis[2], side[2];
@@ -848,6 +900,7 @@ static void bc_halfway_bb(lbm_oracle* o, oblock* b, const int r[6],
             for (int i = r[0]; i < r[1]; i++) {
                 const size_t p = pidx(b, i, j, k);
                 const int x[3] = {i, j, k};
+                const double* g = wall_velocity(given, field, r, i, j, k);
                 for (int l = 0; l < Q; l++) {
                     int beyond = 0;
                     for (int q = 0; q < nf; q++) {
@@ -855,9 +908,9 @@ static void bc_halfway_bb(lbm_oracle* o, oblock* b, const int r[6],
                         beyond |= side[q] ? (s > b->n[axis[q]] - 1) : (s < 0);
                     }
                     if (!beyond) continue;
-                    double cu = CS * o->xi[l * D] * given[0] +
-                                CS * o->xi[l * D + 1] * given[1];
-                    if (D == 3) cu = cu + CS * o->xi[l * D + 2] * given[2];
+                    double cu = CS * o->xi[l * D] * g[0] +
+                                CS * o->xi[l * D + 1] * g[1];
+                    if (D == 3) cu = cu + CS * o->xi[l * D + 2] * g[2];
                     b->f[p * Q + l] =
                         b->fs[p * Q + o->opp[l]] + 2.0 * o->w[l] * cu;
                 }
@@ -970,13 +1023,14 @@ static void one_step(lbm_oracle* o) {
         surface_range(o, b, bc->surface, r);
         switch (bc->scheme) {
             case MPLBGPU_BC_EQM_DIFFUSE_REFL:
-                bc_eqm(o, b, r, bc->given);
+                bc_eqm(o, b, r, bc->given, o->bc_field[i]);
                 break;
             case MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST:
                 bc_extrapol(o, b, r, bc->surface, bc->given[0]);
                 break;
             case MPLBGPU_BC_HALFWAY_BOUNCE_BACK:
-                bc_halfway_bb(o, b, r, bc->surface, bc->given);
+                bc_halfway_bb(o, b, r, bc->surface, bc->given,
+                              o->bc_field[i]);
                 break;
             default:
                 break; /* TreatBlockBoundary3D: no kernel dispatched */
@@ -1093,7 +1147,8 @@ static void swap_step(lbm_oracle* o) {
         const mplbgpu_boundary* bc = &o->bc[i];
         int r[6];
         surface_range(o, b, bc->surface, r);
-        if (bc->scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL) bc_eqm(o, b, r, bc->given);
+        if (bc->scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL)
+            bc_eqm(o, b, r, bc->given, NULL);
     }
 }
 

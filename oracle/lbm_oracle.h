@@ -36,6 +36,12 @@ int lbmo_residual(lbm_oracle* o, int check_period, double* per_var,
 int lbmo_get_macro(lbm_oracle* o, int block, double* rho, double* u,
                    double* v, double* w);
 int lbmo_get_f(lbm_oracle* o, int block, double* f);
+/* Per-node wall velocity of an EQMDiffuseRefl / halfway bounce-back
+ * boundary over its surface range (x fastest; NULL components zero, all
+ * NULL: back to GivenVars), as mplbgpu_set_boundary_velocity. */
+int lbmo_boundary_extent(lbm_oracle* o, int boundary, int ext[3]);
+int lbmo_set_boundary_velocity(lbm_oracle* o, int boundary, const double* u,
+                               const double* v, const double* w);
 /* Node type / geometry property of one block's interior nodes. */
 int lbmo_get_node_info(lbm_oracle* o, int block, int* node_type,
                        int* geometry);

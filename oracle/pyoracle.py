@@ -20,7 +20,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liblbmoracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-REF_ROOT = "/root/reference"
+# where the reference's sources are (only needed to build oracle/_ref)
+REF_ROOT = os.environ.get("MPLB_REFERENCE_ROOT", "/root/reference")
 
 
 def build_restatement():
@@ -43,7 +44,8 @@ def build_reference():
     """Builds oracle/_ref from the reference sources (only where they are)."""
     if not os.path.isdir(os.path.join(REF_ROOT, "Src")):
         return False
-    subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref",
+                    f"REF_ROOT={REF_ROOT}"], check=True)
     return True
 
 
@@ -65,6 +67,8 @@ class Oracle:
         L.lbmo_get_macro.argtypes = [vp, ip, vp, vp, vp, vp]
         L.lbmo_get_f.argtypes = [vp, ip, vp]
         L.lbmo_get_node_info.argtypes = [vp, ip, vp, vp]
+        L.lbmo_boundary_extent.argtypes = [vp, ip, vp]
+        L.lbmo_set_boundary_velocity.argtypes = [vp, ip, vp, vp, vp]
         self.case = case
         desc, self._keep = case.to_desc()
         self._desc = desc
@@ -98,6 +102,20 @@ class Oracle:
     def set_f(self, block, f):
         f = np.ascontiguousarray(f, np.float64)
         self.lib.lbmo_set_f(self.h, block, f.ctypes.data)
+
+    def boundary_extent(self, boundary):
+        ext = (ctypes.c_int * 3)()
+        if self.lib.lbmo_boundary_extent(self.h, boundary, ext) != 0:
+            raise ValueError(self.lib.lbmo_error().decode())
+        return tuple(ext)
+
+    def set_boundary_velocity(self, boundary, u=None, v=None, w=None):
+        nx, ny, nz = self.boundary_extent(boundary)
+        arrs = [None if a is None else np.ascontiguousarray(
+            np.broadcast_to(a, (nz, ny, nx)), np.float64) for a in (u, v, w)]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        if self.lib.lbmo_set_boundary_velocity(self.h, boundary, *ptrs) != 0:
+            raise ValueError(self.lib.lbmo_error().decode())
 
     def step(self, n=1):
         self.lib.lbmo_step(self.h, n)

@@ -57,3 +57,17 @@ def fingerprint(case, f_of, macro_of):
         for n, a in zip(names, macro_of(b)):
             out[f"{n}_b{b}"] = dig(a)
     return out
+
+
+def bench_cases():
+    """The benchmark workloads at reduced size run by the reference (made
+    by tests/golden/make_golden_bench.py): name -> (case, steps, residual
+    history [(step, max, per-variable)], digests)."""
+    with open(os.path.join(GOLDEN, "bench_cases.json")) as fh:
+        d = json.load(fh)
+    out = {}
+    for k, v in d.items():
+        case = CaseConfig.from_json(v["case_json"])
+        case.check_period = v["check_period"]
+        out[k] = (case, v["steps"], v["residual"], v["digest"])
+    return out

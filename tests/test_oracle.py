@@ -91,7 +91,7 @@ def test_oracle_corner_populations_are_stale(oracle_mod):
     f0 = o.f(0)[0, 0, 0].copy()
     o.step(25)
     f = o.f(0)[0, 0, 0]
-    from mplb_b200.csrc_tables import D3Q19_C
+    from csrc_tables import D3Q19_C
     stale = [i for i, c in enumerate(D3Q19_C) if c != (0, 0, 0)
              and all(v >= 0 for v in c)]
     assert len(stale) == 6
@@ -203,3 +203,33 @@ def test_oracle_matches_reference_random_swap_boxes(oracle_mod, seed):
         assert np.array_equal(got, want)
     assert np.array_equal(o.f(0), ref["f"][0])
     assert [h[0] for h in hist] == [r[1] for r in ref["residual"]]
+
+
+@pytest.mark.parametrize("name", ["lchannel_app_9", "cavity2d_lid_first",
+                                  "poiseuille3d"])
+def test_parallel_parity_build_is_the_parity_build(oracle_mod, name):
+    """ref_case_*_par (the parity build with OpenMP over loops without
+    reductions, used for the full-size reference runs) gives the bits of
+    the sequential parity build."""
+    if not oracle_mod.reference_available("_par"):
+        pytest.skip("reference build (oracle/_ref) not present")
+    build, steps, cp = REF_CASES[name]
+    case = build()
+    case.check_period = cp
+    seq = oracle_mod.run_reference(case, steps)
+    par = oracle_mod.run_reference(case, steps, kind="_par")
+    for b in case.block_ids:
+        for got, want in zip(par["macro"][b], seq["macro"][b]):
+            assert np.array_equal(got, want)
+        assert np.array_equal(par["f"][b], seq["f"][b])
+    assert par["residual"] == seq["residual"]
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.bench_cases()))
+def test_oracle_matches_reference_bench_cases(oracle_mod, name):
+    """The benchmark cavity at 64^3 (300 steps) and the L-channel at
+    96/32/32 (200 steps), fingerprinted from the reference's own run."""
+    case, steps, residual, want = golden_cases.bench_cases()[name]
+    o, hist = run_oracle(oracle_mod, case, steps)
+    assert golden_cases.fingerprint(case, o.f, o.macro) == want
+    assert [h[0] for h in hist] == [r[1] for r in residual]
