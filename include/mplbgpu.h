@@ -178,11 +178,34 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
                                   const double* rho, const double* u,
                                   const double* v, const double* w);
 
-/* Replaces the distributions of one block (restart from saved f). */
+/* Replaces the distributions of one block (restart from saved f).  The
+ * context's step count is left as it is; a restart sets it with
+ * mplbgpu_set_step. */
 mplbgpu_status mplbgpu_upload_f(mplbgpu_ctx* ctx, int block, const double* f);
 
-/* nsteps calls of StreamCollision(). */
+/* nsteps calls of StreamCollision().  The kernels are queued on the
+ * context's stream and the call returns without waiting for them (a launch
+ * error is returned at once; a fault during the steps is returned by the
+ * next call that waits: a download, residual, mass, health check,
+ * mplbgpu_synchronize or mplbgpu_last_step_ms).  Calling it once per time
+ * step, as StreamCollision() is called, costs no host round trip. */
 mplbgpu_status mplbgpu_step(mplbgpu_ctx* ctx, int nsteps);
+
+/* One step in two calls, for decomposed blocks whose cut faces come from
+ * another GPU: mplbgpu_step_begin queues the part of the step that reads
+ * no halo layer (the interior of every block whose rows are longer than
+ * two 32-byte sectors), mplbgpu_step_finish the rest (shell rows, row
+ * edges, deferred boundary nodes, block-to-block halos).  Between the two
+ * only mplbgpu_export_face / mplbgpu_import_face are accepted (other calls
+ * return MPLBGPU_ERR_STATE), so a face transfer on another stream overlaps
+ * the interior's computation when the import waits for it.  begin + finish
+ * is one mplbgpu_step(ctx, 1), bit for bit.  Two-array scheme only. */
+mplbgpu_status mplbgpu_step_begin(mplbgpu_ctx* ctx);
+mplbgpu_status mplbgpu_step_finish(mplbgpu_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for ordering a caller's own
+ * work (a face transfer, an event) with the context's. */
+mplbgpu_status mplbgpu_get_stream(mplbgpu_ctx* ctx, void** stream);
 
 /* Moments of the current f into the context's macro fields
  * (UpdateMacroVars3D / UpdateMacroVars). */
@@ -229,6 +252,25 @@ mplbgpu_status mplbgpu_import_face(mplbgpu_ctx* ctx, int block, int surface,
 mplbgpu_status mplbgpu_residual_sums(mplbgpu_ctx* ctx, double* diff,
                                      double* sum);
 
+/* Wall velocity per node for one boundary: no counterpart in the
+ * reference, whose BlockBoundary carries one uniform GivenVars per surface
+ * (Src/boundary.h:85-93); used for an inlet with a perturbed velocity
+ * profile.  `boundary` indexes desc.boundaries (definition order) and must
+ * be an EQMDiffuseRefl or halfway bounce-back boundary.  The arrays hold
+ * one value (MPLB units, like GivenVars) per node of the boundary's
+ * surface range (Block::BoundarySurfaceRange, Src/block.cpp:17-97, the
+ * range its kernel runs over), x fastest then y then z, extent from
+ * mplbgpu_boundary_extent; NULL components are zero, all three NULL go
+ * back to the uniform given values.  Each node's wall constants are then
+ * evaluated from its own velocity in the operation order of the uniform
+ * case, so a field of equal values steps bit for bit as `given` does.
+ * Not available under the swap scheme (MPLBGPU_ERR_UNSUPPORTED). */
+mplbgpu_status mplbgpu_boundary_extent(mplbgpu_ctx* ctx, int boundary,
+                                       int ext[3]);
+mplbgpu_status mplbgpu_set_boundary_velocity(mplbgpu_ctx* ctx, int boundary,
+                                             const double* u, const double* v,
+                                             const double* w);
+
 /* FP64 sum of rho over all nodes of all blocks, from the current f. */
 mplbgpu_status mplbgpu_mass(mplbgpu_ctx* ctx, double* mass);
 
@@ -236,13 +278,22 @@ mplbgpu_status mplbgpu_mass(mplbgpu_ctx* ctx, double* mass);
  * MPLBGPU_OK or MPLBGPU_ERR_DIVERGED. */
 mplbgpu_status mplbgpu_check_health(mplbgpu_ctx* ctx);
 
+/* Number of steps the current state has taken: 0 after
+ * mplbgpu_init_macro, advanced by mplbgpu_step; a restart from saved f
+ * sets it to the checkpoint's step (the reference's CurrentTimeStep,
+ * Src/model.cpp:299-309).  The FP16 storage form draws its stochastic
+ * rounding from it, so a restarted FP16 run takes the draws of the
+ * uninterrupted one. */
+mplbgpu_status mplbgpu_set_step(mplbgpu_ctx* ctx, long long step);
+
 /* Waits for all work issued on the context's stream. */
 mplbgpu_status mplbgpu_synchronize(mplbgpu_ctx* ctx);
 
 /* Number of kernel launches the context has issued since creation. */
 long long mplbgpu_launch_count(const mplbgpu_ctx* ctx);
 
-/* Device time of the most recent mplbgpu_step call's kernels (ms). */
+/* Device time of the most recent mplbgpu_step call's kernels (ms); waits
+ * for them to finish. */
 mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms);
 
 /* ---------------------------------------------------------------------
@@ -265,7 +316,11 @@ typedef struct {
                         FP32 */
     int persistent;  /* 1: one cooperative launch per chunk of steps with a
                         bounded grid barrier between steps; 0: one launch
-                        per step, a chunk replayed from a CUDA graph */
+                        per step (one CTA per tile), a chunk replayed from
+                        a CUDA graph; 2: the same with a grid of the CTAs
+                        that fit on the device whose warps walk the tiles,
+                        each loading its next piece of work before
+                        computing the current one */
     int chunk;       /* steps per chunk (even) */
     int ctas_per_sm; /* CTAs per SM of the persistent launches (at most
                         the co-resident count) */
@@ -283,6 +338,14 @@ mplbgpu_status mplbgpu_batch_set_tuning(mplbgpu_batch* b,
                                         const mplbgpu_batch_tuning* t);
 mplbgpu_status mplbgpu_batch_get_tuning(mplbgpu_batch* b,
                                         mplbgpu_batch_tuning* t);
+/* Polls a grid barrier of the persistent launch makes before it gives up
+ * (default 2^26, several seconds): the kernel then records an error and
+ * returns, and the step or run call reports MPLBGPU_ERR_TIMEOUT; the batch
+ * is then uninitialised (MPLBGPU_ERR_STATE until mplbgpu_batch_init), its
+ * fields being a mix of steps.  Small limits let a test exercise that
+ * path. */
+mplbgpu_status mplbgpu_batch_set_wait_limit(mplbgpu_batch* b,
+                                            long long polls);
 /* Initial macroscopic fields of every cavity, packed cavity after cavity
  * (n*n values each, y slowest), in host or device memory; NULL means
  * rho = 1 / u = v = 0.  f = feq, every cavity active again. */
@@ -319,9 +382,9 @@ mplbgpu_status mplbgpu_batch_stats(mplbgpu_batch* b, double* device_ms,
  * variable; q_old is overwritten with q.  Per-CTA partial sums go to a
  * fixed 512 KiB device array inside the library (held on every GPU that
  * loads it until exit), which limits n to MPLBGPU_NOALLOC_MAX_NODES; larger
- * n is rejected with MPLBGPU_ERR_INVALID.  The first call on a device looks
- * up that array's address for the current device; make it before any
- * stream capture.  Work is queued on `stream` (a cudaStream_t, NULL for the
+ * n is rejected with MPLBGPU_ERR_INVALID.  The first call in a CUDA context
+ * (in practice, the first call on each device) looks up that array's
+ * address in the current context; make it before any stream capture.  Work is queued on `stream` (a cudaStream_t, NULL for the
  * default stream).  All calls share the array: calls that overlap on the
  * GPU race. */
 #define MPLBGPU_NOALLOC_MAX_NODES 16777216LL

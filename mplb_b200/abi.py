@@ -141,6 +141,15 @@ _SIGNATURES = {
     "mplbgpu_residual_sums": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p]),
     "mplbgpu_check_health": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_step_begin": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_step_finish": (ctypes.c_int, [ctypes.c_void_p]),
+    "mplbgpu_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mplbgpu_set_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "mplbgpu_boundary_extent": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_void_p]),
+    "mplbgpu_set_boundary_velocity": (ctypes.c_int, [
+        ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p]),
     "mplbgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "mplbgpu_launch_count": (ctypes.c_longlong, [ctypes.c_void_p]),
     "mplbgpu_last_step_ms": (ctypes.c_int, [ctypes.c_void_p,
@@ -152,6 +161,8 @@ _SIGNATURES = {
     "mplbgpu_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "mplbgpu_batch_set_tuning": (ctypes.c_int, [ctypes.c_void_p,
                                                 ctypes.c_void_p]),
+    "mplbgpu_batch_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p,
+                                                    ctypes.c_longlong]),
     "mplbgpu_batch_get_tuning": (ctypes.c_int, [ctypes.c_void_p,
                                                 ctypes.c_void_p]),
     "mplbgpu_batch_init": (ctypes.c_int, [ctypes.c_void_p] +

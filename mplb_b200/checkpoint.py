@@ -14,7 +14,9 @@ contiguous, halo excluded) with the suffix ``.f64``, plus one JSON manifest
     save_slabs / restart_slabs           -> the same for a run split into
                                             slabs (files of the whole block)
 
-A restart uploads each block's f (``mplbgpu_upload_f``); the next step then
+A restart uploads each block's f (``mplbgpu_upload_f``) and positions the
+run at the checkpoint's step (``mplbgpu_set_step``: check periods and the
+FP16 form's rounding draws continue from there); in FP64 the next step then
 continues bit for bit as the uninterrupted run would.
 """
 import json
@@ -69,6 +71,9 @@ def read(directory: str, case, step: int) -> Dict[int, np.ndarray]:
     if man.get("format") != FORMAT or man["q"] != case.q or \
             man["space_dim"] != case.space_dim:
         raise ValueError("checkpoint does not match the case")
+    if man.get("precision", "fp64") != getattr(case, "precision", "fp64"):
+        raise ValueError(f"checkpoint was written by a {man['precision']} "
+                         f"run, the case is {case.precision}")
     out = {}
     for b in case.block_ids:
         ent = man["blocks"].get(str(b))
@@ -109,6 +114,7 @@ def restart_slabs(case, parts: int, directory: str, step: int, lib=None):
     s = slab.SlabSolver(case, parts, list(range(parts)), slab.LocalExchange(),
                         lib)
     s.upload_f(fields[case.block_ids[0]])
+    s.set_step(step)
     return s
 
 
@@ -118,4 +124,5 @@ def restart(case, directory: str, step: int, lib=None) -> Solver:
     s = Solver(case, lib)
     for b in case.block_ids:
         s.upload_f(b, fields[b])
+    s.set_step(step)
     return s

@@ -436,6 +436,54 @@ def lchannel(leg: int = 384, side: int = 128, depth: int = 128,
         check_period=check_period)
 
 
+def inlet_index(case: CaseConfig) -> int:
+    """Position in the boundary list (definition order) of the case's one
+    boundary with vertex type Inlet."""
+    idx = [k for k, b in enumerate(case.boundaries) if b.vertex_type == "Inlet"]
+    if len(idx) != 1:
+        raise ValueError("the case has no single Inlet boundary")
+    return idx[0]
+
+
+def face_extent(case: CaseConfig, k: int) -> Tuple[int, int, int]:
+    """(nx, ny, nz) of the node range of face boundary k (Left/Right: one
+    x layer, Bottom/Top: one y layer, Back/Front: one z layer)."""
+    bc = case.boundaries[k]
+    nx, ny, nz = case.size3(bc.block)
+    axis = {"Left": 0, "Right": 0, "Bottom": 1, "Top": 1, "Back": 2,
+            "Front": 2}.get(bc.surface)
+    if axis is None:
+        raise ValueError(f"boundary {k} is not a face")
+    ext = [nx, ny, nz]
+    ext[axis] = 1
+    return tuple(ext)
+
+
+def inlet_perturbation(case: CaseConfig, seed: int = 20261203,
+                       amplitude: float = 0.01):
+    """Per-node inlet velocity (MPLB units) for the case's Inlet face: the
+    boundary's given velocity with its normal component scaled by
+    1 + e, e uniform in [-amplitude, amplitude] per node, drawn from
+    numpy's PCG64 generator seeded with `seed` in node order (x fastest,
+    then y, then z).  Returns (boundary index, (u, v, w)) with arrays of
+    shape (nz, ny, nx) over the face.  The reference takes one uniform
+    velocity per boundary (GivenVars), so this is an extension of it."""
+    import numpy as np
+    k = inlet_index(case)
+    nx, ny, nz = face_extent(case, k)
+    bc = case.boundaries[k]
+    g = list(bc.given) + [0.0] * (3 - len(bc.given))
+    axis = {"Left": 0, "Right": 0, "Bottom": 1, "Top": 1, "Back": 2,
+            "Front": 2}[bc.surface]
+    e = np.random.default_rng(seed).uniform(-amplitude, amplitude,
+                                            size=(nz, ny, nx))
+    comps = [np.full((nz, ny, nx), g[a]) for a in range(3)]
+    comps[axis] = g[axis] * (1.0 + e)
+    if case.space_dim == 2:
+        comps[2] = None
+    return k, tuple(comps)
+
+
 def poiseuille(dim: int, nx: int, ny: int, nz: int = 1,
                g_lattice: float = 1e-6, tau_lattice: float = 0.8,
                wall: str = "EQMDiffuseRefl", precision: str = "fp64",

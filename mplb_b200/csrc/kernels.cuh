@@ -84,6 +84,9 @@ struct BlockDev {
     // region PURE); center_fluid: the interior is fluid-like
     int split;
     int center_fluid;
+    // the split step runs as EdgeStepKernel + PipeStepKernel (rows longer
+    // than two 32-byte sectors)
+    int pipe;
     // per region: class (bits 0-1) and fluid-like flag (bit 2); the pulled
     // and the stale populations (copies of RegionInfo::pull / ::stale)
     uint8_t rflags[kNumRegions];
@@ -630,14 +633,131 @@ __device__ __forceinline__ void MomentsCollideT(typename Prec<T>::C* f,
     MomentsCollideT<L, T>(f, pc, fluidlike, pc.omc, pc.omcf, rho, u);
 }
 
+// Wall velocity of node (x, y, z) under an operation with a per-node field
+// (u, v, w per node of the boundary's surface range, x fastest).
+template <typename L>
+__device__ __forceinline__ void FieldVelocity(const RegionOp& op, int x, int y,
+                                              int z, double uw[3]) {
+    const long long k =
+        ((long long)(z - op.forg[2]) * op.fext[1] + (y - op.forg[1])) *
+            op.fext[0] +
+        (x - op.forg[0]);
+    const double* p = op.field + 3 * k;
+    uw[0] = p[0];
+    uw[1] = p[1];
+    uw[2] = L::D == 3 ? p[2] : 0.0;
+}
+
+// (CS c_l) . u_w, the reference's order (cx u + cy v) + cz w with
+// cx = CS * XI (Src/boundary_kernel.inc:1218-1231).
+template <typename L>
+__device__ __forceinline__ double WallCu(double CS, int l, const double uw[3]) {
+    const double cx = CS * (double)L::cx(l);
+    const double cy = CS * (double)L::cy(l);
+    if constexpr (L::D == 3) {
+        const double cz = CS * (double)L::cz(l);
+        return cx * uw[0] + cy * uw[1] + cz * uw[2];
+    } else {
+        return cx * uw[0] + cy * uw[1];
+    }
+}
+
+// CalcBGKFeq(l, rho, u, T = 1, order 2) / (w_l rho): the bracket of
+// Src/model_host_device.h:34-82 in its operation order.
+template <typename L>
+__device__ __forceinline__ double FeqBracket(double CS, int l,
+                                             const double u[3]) {
+    const double T = 1;
+    const double XI0 = L::cx(l), XI1 = L::cy(l);
+    double cu, c2, u2;
+    if constexpr (L::D == 2) {
+        cu = (CS * XI0 * u[0] + CS * XI1 * u[1]);
+        c2 = (CS * XI0 * CS * XI0 + CS * XI1 * CS * XI1);
+        u2 = u[0] * u[0] + u[1] * u[1];
+    } else {
+        const double XI2 = L::cz(l);
+        cu = (CS * XI0 * u[0] + CS * XI1 * u[1] + CS * XI2 * u[2]);
+        c2 = (CS * XI0 * CS * XI0 + CS * XI1 * CS * XI1 +
+              CS * XI2 * CS * XI2);
+        u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    }
+    const double cu2 = cu * cu;
+    return 1.0 + cu + 0.5 * (cu2 - u2 + (T - 1.0) * (c2 - L::D));
+}
+
+// EQMDiffuseRefl with the wall velocity of this node (a per-node field,
+// no counterpart in the reference, whose GivenVars are uniform): the
+// kernel's wall constants evaluated per node, FP64 in the reference's
+// operation order (the same values the uniform path takes from the plan).
+template <typename L, typename T>
+__device__ __noinline__ void ApplyEqmField(typename Prec<T>::C* f,
+                                           const RegionOp& op,
+                                           const PhysConst& pc, int x, int y,
+                                           int z) {
+    constexpr int Q = L::Q;
+    double uw[3];
+    FieldVelocity<L>(op, x, y, z, uw);
+    double deltaRho = 0.0, rhoParallel = 0.0;
+#pragma unroll
+    for (int l = 0; l < Q; l++) {
+        if (op.out_mask >> l & 1u)
+            deltaRho = deltaRho + (2.0 * pc.w[l]) * WallCu<L>(pc.cs, l, uw);
+        if (op.par_mask >> l & 1u)
+            rhoParallel =
+                rhoParallel + (pc.w[l] * 1.0) * FeqBracket<L>(pc.cs, l, uw);
+    }
+    const double denom = 1.0 - deltaRho - rhoParallel;
+    if constexpr (Prec<T>::kShifted) {
+        float sin = 0.0f;
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.in_mask >> i & 1u) sin += f[i];
+        const float inv = 1.0f / (float)denom;
+        const float drw = ((float)(2.0 * op.win - denom) + 2.0f * sin) * inv;
+        const float rhoWall = 1.0f + drw;
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            if (op.par_mask >> i & 1u) {
+                const double a = FeqBracket<L>(pc.cs, i, uw);
+                f[i] = pc.wf[i] * ((float)(a - 1.0) + drw * (float)a);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.out_mask >> i & 1u)
+                f[i] = f[L::opp(i)] + 2.0f * rhoWall * pc.wf[i] *
+                                          (float)WallCu<L>(pc.cs, i, uw);
+    } else {
+        double rhoIn = 0.0;
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.in_mask >> i & 1u) rhoIn = rhoIn + f[i];
+        const double rhoWall = (2.0 * rhoIn) / denom;
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.par_mask >> i & 1u)
+                f[i] = (pc.w[i] * rhoWall) * FeqBracket<L>(pc.cs, i, uw);
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.out_mask >> i & 1u)
+                f[i] = f[L::opp(i)] +
+                       ((2.0 * rhoWall) * pc.w[i]) * WallCu<L>(pc.cs, i, uw);
+    }
+}
+
 // EQMDiffuseRefl (KerCutCellEQMDiffuseRefl3D, Src/boundary_kernel.inc:
 // 1184-1276) with the wall constants precomputed per region.  Shifted
 // forms use sum_in f = sum_in h + sum_in w and w_opp(i) = w_i.
 template <typename L, typename T>
 __device__ __forceinline__ void ApplyEqm(typename Prec<T>::C* f,
                                          const RegionOp& op,
-                                         const PhysConst& pc) {
+                                         const PhysConst& pc, int x, int y,
+                                         int z) {
     constexpr int Q = L::Q;
+    if (op.field != nullptr) {
+        ApplyEqmField<L, T>(f, op, pc, x, y, z);
+        return;
+    }
     if constexpr (Prec<T>::kShifted) {
         // rhoWall - 1 and w_i (rhoWall a_i - 1) without cancellation
         float sin = 0.0f;
@@ -679,9 +799,23 @@ __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
                                          const RegionOp& op,
                                          const PhysConst& pc,
                                          const T* __restrict__ src,
-                                         const BlockDev& b, long long node) {
+                                         const BlockDev& b, long long node,
+                                         int x, int y, int z) {
     constexpr int Q = L::Q;
     using P = Prec<T>;
+    if (op.field != nullptr) {
+        // wall velocity of this node: 2 w_i (c_i . u_w) as the plan forms it
+        double uw[3];
+        FieldVelocity<L>(op, x, y, z, uw);
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+            if (op.out_mask >> i & 1u)
+                f[i] = P::Load(src, L::opp(i) * b.popstride + node, L::opp(i),
+                               pc) +
+                       (typename P::C)((2.0 * pc.w[i]) *
+                                       WallCu<L>(pc.cs, i, uw));
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < Q; i++)
         if (op.out_mask >> i & 1u)
@@ -764,8 +898,9 @@ __device__ __forceinline__ void StepNode(const BlockDev& b,
         }
         for (int k = 0; k < R.nops; k++) {
             const RegionOp& op = b.ops[R.op[k]];
-            if (op.kind == kOpEqm) ApplyEqm<L, T>(f, op, pc);
-            else if (op.kind == kOpHbb) ApplyHbb<L, T>(f, op, pc, src, b, node);
+            if (op.kind == kOpEqm) ApplyEqm<L, T>(f, op, pc, x, y, z);
+            else if (op.kind == kOpHbb)
+                ApplyHbb<L, T>(f, op, pc, src, b, node, x, y, z);
         }
     }
     const bool fl = (rf & 4) != 0;
@@ -831,6 +966,95 @@ __host__ __device__ constexpr int SplitGroup() {
     return sizeof(T) < 8 ? MPLB_LP_GROUP : 1;
 }
 
+// G interior nodes of one row held by one thread: their populations, their
+// element indices and which of them are stored.
+template <int D, typename T, int G>
+struct NodeGroup {
+    typename Prec<T>::C f[G][Lattice<D>::Q];
+    long long node[G];
+    bool valid[G];
+    int first;   // first valid node (the one a node group's seed follows)
+};
+
+// Loads the pulled populations of every node of the group (an invalid node
+// loads a valid node's values and is not stored).
+template <int D, typename T, bool O32, int G>
+__device__ __forceinline__ void GroupLoad(const BlockDev& b,
+                                          const PhysConst& pc,
+                                          const T* __restrict__ src,
+                                          NodeGroup<D, T, G>& n) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    constexpr int Q = L::Q;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+#pragma unroll
+        for (int j = 0; j < G; j++) {
+            if constexpr (O32)
+                n.f[j][i] = P::Load(src + n.node[j], b.pull_off32[i], i, pc);
+            else
+                n.f[j][i] = P::Load(src, PullIndex<L>(b, n.node[j], i), i, pc);
+        }
+    }
+}
+
+// Moments, collision and stores of the valid nodes of a loaded group.
+template <int D, typename T, bool O32, int G>
+__device__ __forceinline__ void GroupFinish(const BlockDev& b,
+                                            const PhysConst& pc,
+                                            T* __restrict__ dst,
+                                            NodeGroup<D, T, G>& n) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    constexpr int Q = L::Q;
+    const bool fl = b.center_fluid != 0;
+    // shifted forms: the two nodes collide together (paired FP32
+    // instructions); a node outside the row computes on its copy of the
+    // other's values and is not stored
+    constexpr bool kPair = P::kShifted && G == 2;
+    if constexpr (kPair) MomentsCollidePair<L>(n.f[0], n.f[1], pc, fl, pc.omcf);
+    if constexpr (std::is_same<T, __half>::value && G == 2) {
+        // FP16 pairs: population i of the two converted together by the
+        // hardware's stochastic rounding (cvt.rs.f16x2.f32 with 32 random
+        // bits per pair)
+        const Rng rg = SeedRng(pc.seed, n.node[n.first]);
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const uint32_t pair = StochasticHalf2(n.f[0][i] * pc.winvf[i],
+                                                  n.f[1][i] * pc.winvf[i],
+                                                  SrDraw32(rg, i));
+            const long long k0 = O32 ? n.node[0] + b.pop_off32[i]
+                                     : OwnIndex(b, n.node[0], i);
+            const long long k1 = O32 ? n.node[1] + b.pop_off32[i]
+                                     : OwnIndex(b, n.node[1], i);
+            if (n.valid[0])
+                PopStore(dst + k0,
+                         __ushort_as_half((unsigned short)(pair & 0xffffu)));
+            if (n.valid[1])
+                PopStore(dst + k1,
+                         __ushort_as_half((unsigned short)(pair >> 16)));
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < G; j++) {
+            if (!n.valid[j]) continue;
+            if constexpr (!kPair) MomentsCollideT<L, T>(n.f[j], pc, fl);
+            Rng rg = SeedRng(pc.seed, n.node[j]);
+            if constexpr (O32) {
+                T* pd = dst + n.node[j];
+#pragma unroll
+                for (int i = 0; i < Q; i++)
+                    P::Store(pd, b.pop_off32[i], i, n.f[j][i], pc, rg);
+            } else {
+#pragma unroll
+                for (int i = 0; i < Q; i++)
+                    P::Store(dst, OwnIndex(b, n.node[j], i), i, n.f[j][i], pc,
+                             rg);
+            }
+        }
+    }
+}
+
 // The G nodes x0 + 32 j (j < G) of one interior row; nodes outside
 // [1, n0 - 2] load from the first valid one and are not stored.
 template <int D, typename T, bool O32, int G>
@@ -839,77 +1063,21 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
                                               const T* __restrict__ src,
                                               T* __restrict__ dst, int x0,
                                               int y, int z) {
-    using L = Lattice<D>;
-    using P = Prec<T>;
-    using C = typename P::C;
-    constexpr int Q = L::Q;
-    bool valid[G];
-    int first = -1;
+    NodeGroup<D, T, G> n;
+    n.first = -1;
 #pragma unroll
     for (int j = 0; j < G; j++) {
         const int x = x0 + 32 * j;
-        valid[j] = x >= 1 && x <= b.n[0] - 2;
-        if (valid[j] && first < 0) first = j;
+        n.valid[j] = x >= 1 && x <= b.n[0] - 2;
+        if (n.valid[j] && n.first < 0) n.first = j;
     }
-    if (first < 0) return;
-    long long node[G];
+    if (n.first < 0) return;
 #pragma unroll
     for (int j = 0; j < G; j++)
-        node[j] = NodeIndexT<D, O32>(b, x0 + 32 * (valid[j] ? j : first), y, z);
-    C f[G][Q];
-#pragma unroll
-    for (int i = 0; i < Q; i++) {
-#pragma unroll
-        for (int j = 0; j < G; j++) {
-            if constexpr (O32)
-                f[j][i] = P::Load(src + node[j], b.pull_off32[i], i, pc);
-            else
-                f[j][i] = P::Load(src, PullIndex<L>(b, node[j], i), i, pc);
-        }
-    }
-    const bool fl = b.center_fluid != 0;
-    // shifted forms: the two nodes collide together (paired FP32
-    // instructions); a node outside the row computes on its copy of the
-    // other's values and is not stored
-    constexpr bool kPair = P::kShifted && G == 2;
-    if constexpr (kPair) MomentsCollidePair<L>(f[0], f[1], pc, fl, pc.omcf);
-    if constexpr (std::is_same<T, __half>::value && G == 2) {
-        // FP16 pairs: population i of the two converted together by the
-        // hardware's stochastic rounding (cvt.rs.f16x2.f32 with 32 random
-        // bits per pair)
-        const Rng rg = SeedRng(pc.seed, node[first]);
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const uint32_t pair = StochasticHalf2(
-                f[0][i] * pc.winvf[i], f[1][i] * pc.winvf[i], SrDraw32(rg, i));
-            const long long k0 = O32 ? node[0] + b.pop_off32[i]
-                                     : OwnIndex(b, node[0], i);
-            const long long k1 = O32 ? node[1] + b.pop_off32[i]
-                                     : OwnIndex(b, node[1], i);
-            if (valid[0]) PopStore(dst + k0, __ushort_as_half(
-                                                 (unsigned short)(pair & 0xffffu)));
-            if (valid[1]) PopStore(dst + k1, __ushort_as_half(
-                                                 (unsigned short)(pair >> 16)));
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < G; j++) {
-            if (!valid[j]) continue;
-            if constexpr (!kPair) MomentsCollideT<L, T>(f[j], pc, fl);
-            Rng rg = SeedRng(pc.seed, node[j]);
-            if constexpr (O32) {
-                T* pd = dst + node[j];
-#pragma unroll
-                for (int i = 0; i < Q; i++)
-                    P::Store(pd, b.pop_off32[i], i, f[j][i], pc, rg);
-            } else {
-#pragma unroll
-                for (int i = 0; i < Q; i++)
-                    P::Store(dst, OwnIndex(b, node[j], i), i, f[j][i], pc,
-                             rg);
-            }
-        }
-    }
+        n.node[j] = NodeIndexT<D, O32>(
+            b, x0 + 32 * (n.valid[j] ? j : n.first), y, z);
+    GroupLoad<D, T, O32, G>(b, pc, src, n);
+    GroupFinish<D, T, O32, G>(b, pc, dst, n);
 }
 
 // Rows of interior nodes handled per x-face block of SplitStepKernel.
@@ -1007,6 +1175,137 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                 D == 3 ? 1 + k.r / ny : 0);
 }
 
+// ---------------------------------------------------------------------------
+// Software-pipelined step, two launches (blocks whose interior region is
+// PURE and whose rows are longer than two sectors):
+//   EdgeStepKernel : the shell rows (y or z on the block boundary) and the
+//                    first and last S nodes of every interior row, S the
+//                    values of one 32-byte sector (4 FP64, 8 FP32, 16
+//                    FP16), one node per thread (StepNode: the x faces'
+//                    boundary programmes run here);
+//   PipeStepKernel : x in [S, n0 - S) of every interior row as warp tasks
+//                    of 32 G nodes in a persistent grid.  Each warp walks
+//                    its tasks holding two register sets: the next task's
+//                    populations are loaded before the current task is
+//                    collided and stored, so the warp's loads stay in
+//                    flight while it computes (a one-task warp waits for
+//                    its loads, then computes with none in flight).
+// The two launches share no 32-byte sector of any population row: a sector
+// written in part by one and in part by the other costs a read-modify-write
+// in HBM when the parts do not meet in L2.
+template <typename T>
+__host__ __device__ constexpr int SectorNodes() {
+    return 32 / (int)sizeof(T);
+}
+
+struct PipeGeom {
+    int xs, xe;       // x range of the pipelined tasks, [xs, xe)
+    int tpr;          // tasks per interior row
+    int ny;           // interior rows per z plane (n1 - 2)
+    long long rows;   // interior rows
+    long long tasks;  // tpr * rows
+};
+
+// Pipelined CTAs per SM: two register sets of a node group.
+#ifndef MPLB_PIPE_MIN_BLOCKS
+#define MPLB_PIPE_MIN_BLOCKS 4
+#endif
+
+// Node group of pipelined task t (warp-uniform): row, segment and lane.
+template <int D, typename T, bool O32, int G>
+__device__ __forceinline__ void PipeSetup(const BlockDev& b,
+                                          const PipeGeom& g, long long t,
+                                          NodeGroup<D, T, G>& n) {
+    const long long row = t / g.tpr;
+    const int seg = (int)(t - row * g.tpr);
+    const int y = 1 + (int)(row % g.ny);
+    const int z = D == 3 ? 1 + (int)(row / g.ny) : 0;
+    const int x0 = g.xs + seg * 32 * G + (int)(threadIdx.x & 31);
+    n.first = 0;
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+        const int x = x0 + 32 * j;
+        n.valid[j] = x < g.xe;
+        // an invalid node reads the row's last pipelined node (in bounds)
+        n.node[j] = NodeIndexT<D, O32>(b, n.valid[j] ? x : g.xe - 1, y, z);
+    }
+}
+
+template <int D, typename T, bool O32>
+__global__ void __launch_bounds__(128, MPLB_PIPE_MIN_BLOCKS)
+    PipeStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
+                   T* __restrict__ dst, PipeGeom g) {
+    constexpr int G = SplitGroup<T>();
+    const int warps = (int)(blockDim.x >> 5);
+    const long long stride = (long long)gridDim.x * warps;
+    long long t = (long long)blockIdx.x * warps + (threadIdx.x >> 5);
+    if (t >= g.tasks) return;
+    NodeGroup<D, T, G> a, c;
+    PipeSetup<D, T, O32, G>(b, g, t, a);
+    GroupLoad<D, T, O32, G>(b, pc, src, a);
+    // two register sets in turn (no copies between them)
+    while (true) {
+        long long nt = t + stride;
+        if (nt < g.tasks) {
+            PipeSetup<D, T, O32, G>(b, g, nt, c);
+            GroupLoad<D, T, O32, G>(b, pc, src, c);
+        }
+        GroupFinish<D, T, O32, G>(b, pc, dst, a);
+        if (nt >= g.tasks) return;
+        t = nt;
+        nt = t + stride;
+        if (nt < g.tasks) {
+            PipeSetup<D, T, O32, G>(b, g, nt, a);
+            GroupLoad<D, T, O32, G>(b, pc, src, a);
+        }
+        GroupFinish<D, T, O32, G>(b, pc, dst, c);
+        if (nt >= g.tasks) return;
+        t = nt;
+    }
+}
+
+// Shell rows (as SplitStepKernel's first CTAs) and the 2 S edge nodes of
+// every interior row, one node per thread.
+template <int D, typename T, bool O32>
+__global__ void __launch_bounds__(128, std::is_same<T, double>::value
+                                           ? MPLB_F64_MIN_BLOCKS
+                                           : MPLB_LP_MIN_BLOCKS)
+    EdgeStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
+                   T* __restrict__ dst, PipeGeom g) {
+    const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int ny = b.n[1] - 2;
+    const int nz = D == 3 ? b.n[2] : 1;
+    const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
+    const unsigned blk = blockIdx.x;
+    if (blk < nsr) {
+        const int row = (int)(blk / nbx);
+        const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
+        if (x >= b.n[0]) return;
+        int y, z;
+        if (row < 2 * nz) {
+            y = (row & 1) ? b.n[1] - 1 : 0;
+            z = row >> 1;
+        } else {
+            const int r2 = row - 2 * nz;
+            z = (r2 & 1) ? b.n[2] - 1 : 0;
+            y = 1 + (r2 >> 1);
+        }
+        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
+                                       nullptr, nullptr, x, y, z);
+        return;
+    }
+    constexpr int S = SectorNodes<T>();
+    const long long e =
+        (long long)(blk - nsr) * blockDim.x + threadIdx.x;   // edge node
+    const long long row = e / (2 * S);
+    if (row >= g.rows) return;
+    const int k = (int)(e - row * 2 * S);
+    const int x = k < S ? k : g.xe + (k - S);
+    StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr, nullptr,
+                                   nullptr, x, 1 + (int)(row % g.ny),
+                                   D == 3 ? 1 + (int)(row / g.ny) : 0);
+}
+
 // Deferred nodes: thread t -> (region, node).
 __device__ __forceinline__ bool DeferredNode(const BlockDev& b, long long t,
                                              int& region, int& x, int& y,
@@ -1085,9 +1384,9 @@ __global__ void DeferredOpKernel(BlockDev b, PhysConst pc,
 #pragma unroll
     for (int i = 0; i < Q; i++) f[i] = (C)b.fdef[i * b.ndef + k];
     if (op.kind == kOpEqm) {
-        ApplyEqm<L, T>(f, op, pc);
+        ApplyEqm<L, T>(f, op, pc, x, y, z);
     } else if (op.kind == kOpHbb) {
-        ApplyHbb<L, T>(f, op, pc, src, b, NodeIndex<D>(b, x, y, z));
+        ApplyHbb<L, T>(f, op, pc, src, b, NodeIndex<D>(b, x, y, z), x, y, z);
     } else if (op.kind == kOpExtrapol) {
         int q[3] = {x, y, z};
         if (op.nb_axis >= 0) q[op.nb_axis] += op.nb_sign;

@@ -16,6 +16,10 @@ struct Launch {
                             const BlockDev& b, const PhysConst& pc,
                             const T* src, T* dst, double* o0, double* o1,
                             double* o2, double* o3);
+    // the two parts of a pipelined step (b.split && b.pipe): 1 = the
+    // interior tasks (read no halo layer), 2 = shell rows and row edges
+    static cudaError_t StepPart(int part, cudaStream_t s, const BlockDev& b,
+                                const PhysConst& pc, const T* src, T* dst);
     static cudaError_t DeferredStream(unsigned grid, cudaStream_t s,
                                       const BlockDev& b, const PhysConst& pc,
                                       const T* src);

@@ -2,6 +2,8 @@
 // translation units that instantiate them).
 #pragma once
 
+#include <algorithm>
+
 #include "launch.h"
 #include "swap.cuh"
 
@@ -23,11 +25,86 @@ long long SplitBlocks(const BlockDev& b) {
     return blocks > 0x7fffffffLL ? 0 : blocks;
 }
 
+// Task geometry of PipeStepKernel for block b.
+template <int D, typename T>
+PipeGeom PipeGeometry(const BlockDev& b) {
+    constexpr int S = SectorNodes<T>();
+    constexpr int G = SplitGroup<T>();
+    PipeGeom g;
+    g.xs = S;
+    g.xe = b.n[0] - S;
+    g.tpr = (g.xe - g.xs + 32 * G - 1) / (32 * G);
+    g.ny = b.n[1] - 2;
+    g.rows = (long long)g.ny * (D == 3 ? b.n[2] - 2 : 1);
+    g.tasks = (long long)g.tpr * g.rows;
+    return g;
+}
+
+// Persistent grid of PipeStepKernel: the CTAs that fit on the device at
+// once (looked up once per instantiation).
+template <int D, typename T, bool O32>
+unsigned PipeCtas() {
+    static const unsigned ctas = [] {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
+                                   dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per, PipeStepKernel<D, T, O32>, kStepThreads, 0) !=
+                cudaSuccess)
+            return 0u;
+        return (unsigned)(sms * (per > 0 ? per : 1));
+    }();
+    return ctas;
+}
+
+// parts: bit 0 the edge launch (shell rows and row edges), bit 1 the
+// pipelined interior; the edge launch goes first when both are asked for.
+template <int D, typename T, bool O32>
+cudaError_t LaunchPipe(cudaStream_t s, const BlockDev& b, const PhysConst& pc,
+                       const T* src, T* dst, int parts) {
+    constexpr int S = SectorNodes<T>();
+    const PipeGeom g = PipeGeometry<D, T>(b);
+    const long long nbx = (b.n[0] + kStepThreads - 1) / kStepThreads;
+    const long long nz = D == 3 ? b.n[2] : 1;
+    const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * (long long)g.ny : 0));
+    const long long edge =
+        nsr + (g.rows * 2 * S + kStepThreads - 1) / kStepThreads;
+    const unsigned ctas = PipeCtas<D, T, O32>();
+    if (edge > 0x7fffffffLL || ctas == 0) return cudaErrorInvalidConfiguration;
+    if (parts & 1) {
+        EdgeStepKernel<D, T, O32><<<(unsigned)edge, kStepThreads, 0, s>>>(
+            b, pc, src, dst, g);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if ((parts & 2) && g.tasks > 0) {
+        const unsigned grid = (unsigned)std::min<long long>(ctas, g.tasks);
+        PipeStepKernel<D, T, O32><<<grid, kStepThreads, 0, s>>>(b, pc, src,
+                                                                dst, g);
+    }
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::StepPart(int part, cudaStream_t s, const BlockDev& b,
+                                   const PhysConst& pc, const T* src, T* dst) {
+    if (!(b.split && b.pipe) || (part != 1 && part != 2))
+        return cudaErrorInvalidValue;
+    const int parts = part == 1 ? 2 : 1;
+    return b.off32 ? LaunchPipe<D, T, true>(s, b, pc, src, dst, parts)
+                   : LaunchPipe<D, T, false>(s, b, pc, src, dst, parts);
+}
+
 template <int D, typename T>
 cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const BlockDev& b, const PhysConst& pc,
                                const T* src, T* dst, double* o0, double* o1,
                                double* o2, double* o3) {
+    if (mode == kModeStep && b.split && b.pipe) {
+        return b.off32 ? LaunchPipe<D, T, true>(s, b, pc, src, dst, 3)
+                       : LaunchPipe<D, T, false>(s, b, pc, src, dst, 3);
+    }
     if (mode == kModeStep && b.split) {
         const long long blocks = SplitBlocks<D, T>(b);
         if (blocks == 0) return cudaErrorInvalidConfiguration;

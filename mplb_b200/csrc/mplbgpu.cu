@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -69,12 +70,15 @@ struct mplbgpu_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0;
+    bool timing_pending = false;  // ev0/ev1 of the last step call unread
+    bool begun = false;           // mplbgpu_step_begin without its finish
     long long launches = 0;
     unsigned long long step_count = 0;
     double* part = nullptr;     // reduction partials
     unsigned long long* bad = nullptr;
     double* scratch = nullptr;  // dense f staging
     size_t scratch_elems = 0;
+    std::vector<double*> bc_field;  // per boundary: per-node wall velocity
     std::string err;
 };
 
@@ -155,6 +159,7 @@ void FreeAll(mplbgpu_ctx* c) {
         for (auto& d : b.dops) cudaFree(d.segs);
     }
     for (DevHalo& h : c->halos) cudaFree(h.prev);
+    for (double* p : c->bc_field) cudaFree(p);
     cudaFree(c->part);
     cudaFree(c->bad);
     cudaFree(c->scratch);
@@ -224,6 +229,7 @@ int StepOnce(mplbgpu_ctx* ctx) {
         CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D), ctx->stream,
                                        b.dev, ctx->pc, s, d, nullptr, nullptr,
                                        nullptr, nullptr));
+        if (b.dev.split && b.dev.pipe) ctx->launches++;   // two kernels
         if (B.ndeferred > 0) {
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
             CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, ctx->stream, b.dev,
@@ -243,6 +249,69 @@ int StepOnce(mplbgpu_ctx* ctx) {
     ctx->cur = dst;
     ctx->initial = false;
     return RunHalosT<D, T>(ctx);
+}
+
+// First part of a step: the halo-independent interior of every block with
+// the pipelined layout (other blocks do all their work in the second part).
+template <int D, typename T>
+int StepBeginT(mplbgpu_ctx* ctx) {
+    const int src = ctx->cur, dst = 1 - ctx->cur;
+    ctx->pc.seed = (uint32_t)(++ctx->step_count);
+    for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+        DevBlock& b = ctx->blocks[bi];
+        if (!(b.dev.split && b.dev.pipe)) continue;
+        CK_LAUNCH_E(Launch<D, T>::StepPart(
+            1, ctx->stream, b.dev, ctx->pc, static_cast<const T*>(b.pop[src]),
+            static_cast<T*>(b.pop[dst])));
+    }
+    ctx->begun = true;
+    return MPLBGPU_OK;
+}
+
+// The rest of a begun step: shell rows and row edges of pipelined blocks,
+// whole other blocks, deferred nodes, then the block-to-block halos.
+template <int D, typename T>
+int StepFinishT(mplbgpu_ctx* ctx) {
+    const int src = ctx->cur, dst = 1 - ctx->cur;
+    for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+        DevBlock& b = ctx->blocks[bi];
+        const BlockPlan& B = ctx->plan.blocks[bi];
+        const T* s = static_cast<const T*>(b.pop[src]);
+        T* d = static_cast<T*>(b.pop[dst]);
+        if (b.dev.split && b.dev.pipe) {
+            CK_LAUNCH_E(Launch<D, T>::StepPart(2, ctx->stream, b.dev, ctx->pc,
+                                               s, d));
+        } else {
+            CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D),
+                                           ctx->stream, b.dev, ctx->pc, s, d,
+                                           nullptr, nullptr, nullptr,
+                                           nullptr));
+        }
+        if (B.ndeferred > 0) {
+            const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
+            CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, ctx->stream, b.dev,
+                                                     ctx->pc, s));
+            for (auto& dop : b.dops) {
+                const unsigned gd =
+                    (unsigned)((dop.total + kThreads - 1) / kThreads);
+                CK_LAUNCH_E(Launch<D, T>::DeferredOp(gd, ctx->stream, b.dev,
+                                                     ctx->pc, s, dop.segs,
+                                                     dop.nseg, dop.total));
+            }
+            CK_LAUNCH_E(Launch<D, T>::DeferredFinish(
+                kModeStep, g, ctx->stream, b.dev, ctx->pc, d, nullptr, nullptr,
+                nullptr, nullptr));
+        }
+    }
+    ctx->cur = dst;
+    ctx->initial = false;
+    ctx->begun = false;
+    return RunHalosT<D, T>(ctx);
+}
+
+int StepBegin(mplbgpu_ctx* ctx) { return MPLB_DISPATCH(ctx, StepBeginT, ctx); }
+int StepFinish(mplbgpu_ctx* ctx) {
+    return MPLB_DISPATCH(ctx, StepFinishT, ctx);
 }
 
 // Current f -> moments (kModeMacro) or point-major f (kModeF) of one block.
@@ -289,7 +358,10 @@ int UpdateMacro(mplbgpu_ctx* ctx) {
     return MPLBGPU_OK;
 }
 
-int CheckReady(mplbgpu_ctx* ctx) {
+int CheckReady(mplbgpu_ctx* ctx, bool allow_begun = false) {
+    if (ctx->begun && !allow_begun)
+        return SetErr(ctx, MPLBGPU_ERR_STATE,
+                      "a step begun by mplbgpu_step_begin is not finished");
     for (size_t i = 0; i < ctx->initialised.size(); i++)
         if (!ctx->initialised[i])
             return SetErr(ctx, MPLBGPU_ERR_STATE,
@@ -572,6 +644,16 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
                       ? 1
                       : 0;
         d.center_fluid = B.region[center].fluidlike ? 1 : 0;
+        // the split step as edge + pipelined interior launches where a row
+        // holds more than two 32-byte sectors of nodes;
+        // MPLB_B200_STEP_KERNEL=split keeps the one-launch split kernel
+        // (both give the same FP64/FP32 bits; tests compare them)
+        const char* sk = std::getenv("MPLB_B200_STEP_KERNEL");
+        const int sector = 32 / P.elem_bytes;
+        d.pipe = d.split && B.n[0] >= 2 * sector + 1 &&
+                         !(sk && std::strcmp(sk, "split") == 0)
+                     ? 1
+                     : 0;
     }
     for (const HaloCopy& h : P.halos) {
         DevHalo dh;
@@ -622,6 +704,9 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
     DevBlock* b = FindBlock(ctx, block);
     const BlockPlan* B = FindPlan(ctx, block);
     if (!b) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    if (ctx->begun)
+        return SetErr(ctx, MPLBGPU_ERR_STATE,
+                      "a step begun by mplbgpu_step_begin is not finished");
     if (!ctx->initial) {
         // a new initial state after steps: every block starts again
         std::fill(ctx->initialised.begin(), ctx->initialised.end(), false);
@@ -653,6 +738,7 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
     ctx->initial = true;
     ctx->halos_pending = true;
     ctx->initialised[bi] = true;
+    ctx->step_count = 0;   // a new initial state is step 0
     CK(cudaStreamSynchronize(ctx->stream));
     return MPLBGPU_OK;
 }
@@ -663,6 +749,9 @@ mplbgpu_status mplbgpu_upload_f(mplbgpu_ctx* ctx, int block, const double* f) {
     DevBlock* b = FindBlock(ctx, block);
     const BlockPlan* B = FindPlan(ctx, block);
     if (!b) return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown block id");
+    if (ctx->begun)
+        return SetErr(ctx, MPLBGPU_ERR_STATE,
+                      "a step begun by mplbgpu_step_begin is not finished");
     if (!ctx->initial)
         std::fill(ctx->initialised.begin(), ctx->initialised.end(), false);
     const size_t elems = (size_t)B->nodes() * ctx->plan.Q;
@@ -704,9 +793,43 @@ mplbgpu_status mplbgpu_step(mplbgpu_ctx* ctx, int nsteps) {
         rc = MPLB_DISPATCH(ctx, StepOnce, ctx);
         if (rc != MPLBGPU_OK) return rc;
     }
+    // no host wait: the caller's next reading call (download, residual,
+    // mass, synchronize, last_step_ms) waits for the stream
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    CK(cudaEventSynchronize(ctx->ev1));
-    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    ctx->timing_pending = true;
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_step_begin(mplbgpu_ctx* ctx) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    int rc = CheckReady(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    if (ctx->plan.swap)
+        return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
+                      "a step in two parts needs the two-array scheme");
+    if (ctx->halos_pending) {
+        rc = RunHalos(ctx);
+        if (rc != MPLBGPU_OK) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    return StepBegin(ctx);
+}
+
+mplbgpu_status mplbgpu_step_finish(mplbgpu_ctx* ctx) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    if (!ctx->begun)
+        return SetErr(ctx, MPLBGPU_ERR_STATE,
+                      "mplbgpu_step_finish without mplbgpu_step_begin");
+    int rc = StepFinish(ctx);
+    if (rc != MPLBGPU_OK) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->timing_pending = true;
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_get_stream(mplbgpu_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return MPLBGPU_ERR_INVALID;
+    *stream = static_cast<void*>(ctx->stream);
     return MPLBGPU_OK;
 }
 
@@ -820,7 +943,7 @@ mplbgpu_status mplbgpu_export_face(mplbgpu_ctx* ctx, int block, int surface,
                                    void* buf) {
     if (!ctx || !buf) return ctx ? SetErr(ctx, MPLBGPU_ERR_INVALID, "null buffer")
                                  : MPLBGPU_ERR_INVALID;
-    int rc = CheckReady(ctx);
+    int rc = CheckReady(ctx, true);
     if (rc != MPLBGPU_OK) return rc;
     size_t bi;
     FaceDev fd;
@@ -833,7 +956,7 @@ mplbgpu_status mplbgpu_import_face(mplbgpu_ctx* ctx, int block, int surface,
                                    const void* buf) {
     if (!ctx || !buf) return ctx ? SetErr(ctx, MPLBGPU_ERR_INVALID, "null buffer")
                                  : MPLBGPU_ERR_INVALID;
-    int rc = CheckReady(ctx);
+    int rc = CheckReady(ctx, true);
     if (rc != MPLBGPU_OK) return rc;
     size_t bi;
     FaceDev fd;
@@ -889,6 +1012,91 @@ mplbgpu_status mplbgpu_check_health(mplbgpu_ctx* ctx) {
     return MPLBGPU_OK;
 }
 
+mplbgpu_status mplbgpu_boundary_extent(mplbgpu_ctx* ctx, int boundary,
+                                       int ext[3]) {
+    if (!ctx || !ext) return MPLBGPU_ERR_INVALID;
+    if (boundary < 0 || boundary >= (int)ctx->plan.bc_block.size() ||
+        ctx->plan.bc_block[boundary] < 0)
+        return SetErr(ctx, MPLBGPU_ERR_INVALID, "unknown boundary index");
+    const int* r = &ctx->plan.bc_range[6 * (size_t)boundary];
+    for (int a = 0; a < 3; a++) ext[a] = r[2 * a + 1] - r[2 * a];
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_set_boundary_velocity(mplbgpu_ctx* ctx, int boundary,
+                                             const double* u, const double* v,
+                                             const double* w) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    int ext[3];
+    int rc = mplbgpu_boundary_extent(ctx, boundary, ext);
+    if (rc != MPLBGPU_OK) return rc;
+    if (ctx->plan.swap)
+        return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
+                      "per-node wall velocities are not available under the "
+                      "swap scheme");
+    // the scheme of this boundary: any op made from it tells
+    const int bi = ctx->plan.bc_block[boundary];
+    BlockPlan& B = ctx->plan.blocks[bi];
+    DevBlock& b = ctx->blocks[bi];
+    bool any = false;
+    for (const RegionOp& op : B.ops) {
+        if (op.bc != boundary) continue;
+        if (op.kind != kOpEqm && op.kind != kOpHbb)
+            return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
+                          "per-node velocities need an EQMDiffuseRefl or "
+                          "halfway bounce-back boundary");
+        any = true;
+    }
+    if (!any)
+        return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
+                      "the boundary has no boundary kernel (per-node "
+                      "velocities need EQMDiffuseRefl or halfway "
+                      "bounce-back)");
+    const int* r = &ctx->plan.bc_range[6 * (size_t)boundary];
+    const size_t cnt = (size_t)ext[0] * ext[1] * ext[2];
+    // no kernel of this context may read the op table while it changes
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->bc_field.size() < ctx->plan.bc_block.size())
+        ctx->bc_field.resize(ctx->plan.bc_block.size(), nullptr);
+    double*& dev = ctx->bc_field[boundary];
+    const bool clear = !u && !v && !w;
+    if (clear) {
+        CK(cudaFree(dev));
+        dev = nullptr;
+    } else {
+        std::vector<double> packed(3 * cnt, 0.0);
+        const double* src[3] = {u, v, ctx->plan.dim == 3 ? w : nullptr};
+        for (int c = 0; c < 3; c++)
+            if (src[c])
+                for (size_t k = 0; k < cnt; k++) packed[3 * k + c] = src[c][k];
+        for (double x : packed)
+            if (!std::isfinite(x))
+                return SetErr(ctx, MPLBGPU_ERR_INVALID,
+                              "non-finite wall velocity");
+        if (!dev) CK(cudaMalloc(&dev, packed.size() * sizeof(double)));
+        CK(cudaMemcpy(dev, packed.data(), packed.size() * sizeof(double),
+                      cudaMemcpyHostToDevice));
+    }
+    for (RegionOp& op : B.ops) {
+        if (op.bc != boundary) continue;
+        op.field = dev;
+        for (int a = 0; a < 3; a++) {
+            op.forg[a] = r[2 * a];
+            op.fext[a] = ext[a];
+        }
+    }
+    CK(cudaMemcpy(b.ops, B.ops.data(), B.ops.size() * sizeof(RegionOp),
+                  cudaMemcpyHostToDevice));
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_set_step(mplbgpu_ctx* ctx, long long step) {
+    if (!ctx) return MPLBGPU_ERR_INVALID;
+    if (step < 0) return SetErr(ctx, MPLBGPU_ERR_INVALID, "step < 0");
+    ctx->step_count = (unsigned long long)step;
+    return MPLBGPU_OK;
+}
+
 mplbgpu_status mplbgpu_synchronize(mplbgpu_ctx* ctx) {
     if (!ctx) return MPLBGPU_ERR_INVALID;
     CK(cudaStreamSynchronize(ctx->stream));
@@ -901,6 +1109,11 @@ long long mplbgpu_launch_count(const mplbgpu_ctx* ctx) {
 
 mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms) {
     if (!ctx || !ms) return MPLBGPU_ERR_INVALID;
+    if (ctx->timing_pending) {
+        CK(cudaEventSynchronize(ctx->ev1));
+        CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+        ctx->timing_pending = false;
+    }
     *ms = ctx->last_ms;
     return MPLBGPU_OK;
 }

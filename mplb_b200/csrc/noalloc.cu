@@ -15,6 +15,7 @@
 // variables of at most MPLBGPU_NOALLOC_MAX_NODES = 8192 x 2048 nodes.
 // Every call shares the array and it keeps the last call's partials; calls
 // that overlap on the GPU (different streams, or host threads) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -34,26 +35,87 @@ static_assert(kMaxCtas * kNodesPerCta == MPLBGPU_NOALLOC_MAX_NODES,
 // [variable][cta][0: sum (q - q_old)^2, 1: sum q^2]
 static __device__ __align__(256) double g_noalloc_partials[kVars][kMaxCtas][2];
 
-constexpr int kMaxDevices = 64;
+// Address cache, one entry per CUDA context.  Each context loads the
+// library's device code separately, so the array has one address per
+// context: a device's primary context after cudaDeviceReset, or a context
+// a caller made with the driver API, gets its own entry.  Contexts are told
+// apart by cuCtxGetId (unique for the life of the process, where a
+// CUcontext handle may be reused), reached through the runtime's driver
+// entry point so that the library does not link libcuda itself.
+constexpr int kMaxContexts = 64;
+struct ScratchEntry {
+    unsigned long long ctx_id;
+    double* addr;
+};
 std::mutex g_mu;
-double* g_scratch[kMaxDevices] = {};
+ScratchEntry g_scratch[kMaxContexts];
+int g_nscratch = 0;
 
-// Address of the scratch array on the current device, looked up once per
-// device.  In host code the symbol is only a stand-in for the device
-// variable, so kernels must be given this address, not the symbol.
+using CtxGetCurrentFn = CUresult(CUDAAPI*)(CUcontext*);
+using CtxGetIdFn = CUresult(CUDAAPI*)(CUcontext, unsigned long long*);
+
+// Id of the context current on this thread; false if there is none or the
+// driver does not offer the query.
+bool CurrentContextId(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000,
+                                             cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    static CtxGetIdFn get_id = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000,
+                                             cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetIdFn>(f);
+    }();
+    if (get_current == nullptr || get_id == nullptr) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Address of the scratch array in the current context, looked up once per
+// context (in practice once per device).  In host code the symbol is only
+// a stand-in for the device variable, so kernels must be given this
+// address, not the symbol.
 cudaError_t ScratchAddress(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (g_scratch[dev] == nullptr) {
+    unsigned long long id = 0;
+    if (!CurrentContextId(&id)) {
+        // no context bound to this thread yet: the lookup binds the
+        // device's primary context, after which the id can be read
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_partials);
         if (e != cudaSuccess) return e;
-        g_scratch[dev] = static_cast<double*>(p);
+        if (!CurrentContextId(&id)) {   // no id to key on: do not cache
+            *out = static_cast<double*>(p);
+            return cudaSuccess;
+        }
     }
-    *out = g_scratch[dev];
+    std::lock_guard<std::mutex> lock(g_mu);
+    for (int k = 0; k < g_nscratch; k++) {
+        if (g_scratch[k].ctx_id == id) {
+            *out = g_scratch[k].addr;
+            return cudaSuccess;
+        }
+    }
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess) return e;
+    if (g_nscratch < kMaxContexts)
+        g_scratch[g_nscratch++] = {id, static_cast<double*>(p)};
+    *out = static_cast<double*>(p);
     return cudaSuccess;
 }
 

@@ -698,6 +698,7 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                 else
                     prog.push_back(MakeHbb(L, P.cs, B.n, p, bc.surface,
                                            bc.given));
+                prog.back().bc = k;
             }
             bool extrapol = false;
             uint32_t written = 0, readfirst = 0;
@@ -903,6 +904,17 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
             }
         }
         if (!h.any_prev) h.prev.clear();
+    }
+    // surface range of every boundary, for per-node wall velocities
+    P.bc_block.assign(d.nboundaries, -1);
+    P.bc_range.assign(6 * (size_t)d.nboundaries, 0);
+    for (int k = 0; k < d.nboundaries; k++) {
+        for (const BlockPlan& B : P.blocks) {
+            if (B.id != d.boundaries[k].block) continue;
+            P.bc_block[k] = B.index;
+            SurfaceRange(P.dim, B.n, d.boundaries[k].surface,
+                         &P.bc_range[6 * (size_t)k]);
+        }
     }
     return MPLBGPU_OK;
 }

@@ -41,6 +41,7 @@ enum OpKind : int { kOpEqm = 1, kOpHbb = 2, kOpExtrapol = 3 };
 // here in the reference's operation order.
 struct RegionOp {
     int kind;
+    int bc;             // index of the boundary (definition order)
     uint32_t in_mask;   // EQM: incoming;  EXTRAPOL: copied populations
     uint32_t out_mask;  // EQM: outgoing;  HBB: bounced populations
     uint32_t par_mask;  // EQM: parallel
@@ -54,6 +55,12 @@ struct RegionOp {
     double rho_given;   // EXTRAPOL
     double a[kMaxQ];    // EQM: feq(1,u_w)/w per parallel population (res)
     double b[kMaxQ];    // EQM: c.u_w per outgoing; HBB: 2 w (c.u_w)
+    // EQM / HBB with a wall velocity per node (mplbgpu_set_boundary_velocity):
+    // (u, v, w) per node of the boundary's surface range, x fastest, from
+    // node forg; null: the uniform given values above
+    const double* field;
+    int forg[3];
+    int fext[3];
 };
 
 struct RegionInfo {
@@ -134,6 +141,10 @@ struct Plan {
     int swap = 0;       // Scheme_StreamCollision_Swap: one population array
     std::vector<BlockPlan> blocks;  // sorted by id
     std::vector<HaloCopy> halos;
+    // per boundary (definition order): its block's index and its surface
+    // range [r0, r1) x [r2, r3) x [r4, r5) (Block::BoundarySurfaceRange)
+    std::vector<int> bc_block;
+    std::vector<int> bc_range;
 };
 
 // Builds the plan; returns MPLBGPU_OK or an error code with a message.

@@ -68,7 +68,7 @@ __device__ __forceinline__ void SwapNode(const BlockDev& b,
     if (BC && !interior) {
         const RegionInfo& R = b.regions[r];
         for (int i = 0; i < R.nops; i++)
-            ApplyEqm<L, T>(v, b.ops[R.op[i]], pc);
+            ApplyEqm<L, T>(v, b.ops[R.op[i]], pc, x, y, z);
     }
     const bool fl = (b.rflags[r] & 4) != 0;
     if (MODE == kModeF) {

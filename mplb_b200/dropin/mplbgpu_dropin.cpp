@@ -2,6 +2,7 @@
 // (include/mplbgpu.h).  See mplbgpu_dropin.h.
 #include "mplbgpu_dropin.h"
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -153,6 +154,10 @@ void Create(Real time) {
                            reinterpret_cast<char*>(f.data()));
         Check(mplbgpu_upload_f(g_ctx, block.ID(), f.data()), "mplbgpu_upload_f");
     }
+    // a restart continues from its CurrentTimeStep (time = step * dt)
+    if (time != 0)
+        Check(mplbgpu_set_step(g_ctx, std::llround(time / TimeStep())),
+              "mplbgpu_set_step");
 }
 
 }  // namespace

@@ -93,18 +93,25 @@ def slab_case(case: CaseConfig, parts: int, index: int) -> CaseConfig:
 
 
 class LocalExchange:
-    """Face moves between slabs held by this process (device copies)."""
+    """Face moves between slabs held by this process (device copies).  A
+    step: every slab exports its faces, then begins its step (the interior,
+    which reads no halo), imports its neighbours' faces and finishes the
+    step."""
 
-    def exchange(self, solver: "SlabSolver"):
+    def step(self, solver: "SlabSolver"):
         parts = solver.parts
         for p in parts:
             p.export_faces()
         for p in parts:
-            p.synchronize()
+            p.synchronize()     # a neighbour's export is read by our import
+        for p in parts:
+            p.step_begin()
         for k in range(len(parts) - 1):
             lo, hi = parts[k], parts[k + 1]
             lo.import_face("high", hi.out["low"])
             hi.import_face("low", lo.out["high"])
+        for p in parts:
+            p.step_finish()
 
 
 class DistExchange:
@@ -130,13 +137,8 @@ class DistExchange:
             h = self.host[key] = buf.new_empty(buf.shape, device="cpu")
         return h
 
-    def exchange(self, solver: "SlabSolver"):
-        import torch
+    def _ops(self, p, rank):
         dist = self.dist
-        (p,) = solver.parts
-        rank, world = solver.index0, solver.nparts
-        p.export_faces()
-        p.synchronize()
         peers = {"low": rank - 1, "high": rank + 1}
         ops, recv = [], []
         for side in ("low", "high"):
@@ -149,16 +151,57 @@ class DistExchange:
             ops.append(dist.P2POp(dist.isend, send, peers[side], self.group))
             ops.append(dist.P2POp(dist.irecv, into, peers[side], self.group))
             recv.append((side, into))
+        return ops, recv
+
+    def step(self, solver: "SlabSolver"):
+        """One step: export the faces, begin the step (the interior), move
+        the faces while it runs, import them, finish the step."""
+        (p,) = solver.parts
+        if not self.staged:
+            return self._step_device(p, solver.index0)
+        # gloo: the faces go through host memory while the interior runs
+        p.export_faces()
+        p.synchronize()
+        p.step_begin()
+        ops, recv = self._ops(p, solver.index0)
         if ops:
-            for req in dist.batch_isend_irecv(ops):
+            for req in self.dist.batch_isend_irecv(ops):
                 req.wait()
         for side, into in recv:
             if into is not p.inb[side]:
                 p.inb[side].copy_(into)
         if any(b is not None and b.is_cuda for b in p.inb.values()):
+            import torch
             torch.cuda.current_stream().synchronize()
         for side, _ in recv:
             p.import_face(side, p.inb[side])
+        p.step_finish()
+
+    def _step_device(self, p, rank):
+        """NCCL: nothing waits on the host.  The context's stream exports
+        the faces and runs the interior; a side stream waits for the
+        export, sends and receives; the context's stream waits for the
+        transfer, imports and finishes the step."""
+        import torch
+        ctx = torch.cuda.ExternalStream(p.stream_ptr())
+        if getattr(self, "comm", None) is None:
+            self.comm = torch.cuda.Stream()
+        p.export_faces()
+        exported = torch.cuda.Event()
+        exported.record(ctx)
+        p.step_begin()
+        ops, recv = self._ops(p, rank)
+        moved = torch.cuda.Event()
+        with torch.cuda.stream(self.comm):
+            self.comm.wait_event(exported)
+            if ops:
+                for req in self.dist.batch_isend_irecv(ops):
+                    req.wait()
+            moved.record(self.comm)
+        ctx.wait_event(moved)
+        for side, _ in recv:
+            p.import_face(side, p.inb[side])
+        p.step_finish()
 
 
 class _Part:
@@ -211,6 +254,19 @@ class _Part:
     def synchronize(self):
         self.solver.synchronize()
 
+    def step_begin(self):
+        self._check(self.lib.mplbgpu_step_begin(self.solver.h))
+
+    def step_finish(self):
+        self._check(self.lib.mplbgpu_step_finish(self.solver.h))
+        self.solver.steps_done += 1
+
+    def stream_ptr(self):
+        st = ctypes.c_void_p()
+        self._check(self.lib.mplbgpu_get_stream(self.solver.h,
+                                                ctypes.byref(st)))
+        return st.value or 0
+
 
 class SlabSolver:
     """Slabs `indices` of a `parts`-way decomposition of `case`, held by
@@ -251,12 +307,16 @@ class SlabSolver:
             part = f[lo:hi] if self.join_axis == 0 else f[:, lo:hi]
             p.solver.upload_f(p.bid, np.ascontiguousarray(part))
 
+    def set_step(self, step):
+        """Positions every slab held here at `step` (a restart)."""
+        for p in self.parts:
+            p.solver.set_step(step)
+
     def stream_collision(self, n=1):
-        """n steps; the faces cross before each step."""
+        """n steps; the faces cross during each step (after its interior
+        has been queued, before its boundary layers)."""
         for _ in range(int(n)):
-            self.exchange_impl.exchange(self)
-            for p in self.parts:
-                p.solver.stream_collision(1)
+            self.exchange_impl.step(self)
 
     def update_macro_vars(self):
         for p in self.parts:

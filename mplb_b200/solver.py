@@ -87,6 +87,33 @@ class Solver:
             raise ValueError(f"f must have shape {self._shape(block)} + (Q,)")
         self._check(self.lib.mplbgpu_upload_f(self.h, block, f.ctypes.data))
 
+    def boundary_extent(self, boundary):
+        """(nx, ny, nz) of the node range of boundary `boundary` (index in
+        definition order)."""
+        ext = (ctypes.c_int * 3)()
+        self._check(self.lib.mplbgpu_boundary_extent(self.h, int(boundary),
+                                                     ext))
+        return tuple(ext)
+
+    def set_boundary_velocity(self, boundary, u=None, v=None, w=None):
+        """Per-node wall velocity (MPLB units) of an EQMDiffuseRefl or
+        halfway bounce-back boundary: arrays of shape (nz, ny, nx) over its
+        node range (boundary_extent); all None restores the uniform given
+        values.  No counterpart in the reference (uniform GivenVars)."""
+        nx, ny, nz = self.boundary_extent(boundary)
+        arrs = [None if a is None else np.ascontiguousarray(
+            np.broadcast_to(a, (nz, ny, nx)), np.float64) for a in (u, v, w)]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        self._check(self.lib.mplbgpu_set_boundary_velocity(
+            self.h, int(boundary), *ptrs))
+
+    def set_step(self, step):
+        """Positions the run at `step` (a restart's CurrentTimeStep): the
+        check periods of iterate() and the FP16 rounding draws continue
+        from there."""
+        self._check(self.lib.mplbgpu_set_step(self.h, int(step)))
+        self.steps_done = int(step)
+
     # -- time stepping ------------------------------------------------------
     def stream_collision(self, n=1):
         self._check(self.lib.mplbgpu_step(self.h, int(n)))

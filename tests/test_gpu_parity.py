@@ -158,3 +158,17 @@ def test_gpu_matches_reference_app_files(gpu_lib, name):
     s.update_macro_vars()
     assert golden_cases.fingerprint(case, s.f, s.macro) == want
     s.close()
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.bench_cases()))
+def test_gpu_matches_reference_bench_cases(gpu_lib, name):
+    """The benchmark cavity (D3Q19, Re 400, lid 0.05) at 64^3 for 300 steps
+    and the 3-block L-channel at 96/32/32 for 200 steps: f and moments bit
+    for bit the reference's run (SHA-256 digests), residual history within
+    summation order."""
+    case, steps, residual, want = golden_cases.bench_cases()[name]
+    s, hist = run_gpu(case, steps)
+    assert golden_cases.fingerprint(case, s.f, s.macro) == want
+    np.testing.assert_allclose([h[0] for h in hist],
+                               [r[1] for r in residual], rtol=1e-12, atol=0)
+    s.close()

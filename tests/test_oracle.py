@@ -233,3 +233,30 @@ def test_oracle_matches_reference_bench_cases(oracle_mod, name):
     o, hist = run_oracle(oracle_mod, case, steps)
     assert golden_cases.fingerprint(case, o.f, o.macro) == want
     assert [h[0] for h in hist] == [r[1] for r in residual]
+
+
+def test_reference_fdperiodic_breaks_the_run(oracle_mod):
+    """Why this path rejects FDPeriodic (MPLBGPU_ERR_UNSUPPORTED): the
+    reference's KerCutCellPeriodic3D copies f from the halo of f, which its
+    StreamCollision never transfers, so those nodes get zeros and the field
+    turns to NaN within a few steps (the reference run here, 10 steps of a
+    forced channel made x-periodic through FDPeriodic instead of
+    MDPeriodic)."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    c = config.poiseuille(3, 8, 7, 6, g_lattice=1e-4)
+    bcs = [dataclasses.replace(b, scheme="FDPeriodic", vertex_type="FDPeriodic")
+           if b.surface in ("Left", "Right") else b for b in c.boundaries]
+    conns = [dataclasses.replace(x, type="FDPeriodic")
+             if x.from_surface in ("Left", "Right") else x
+             for x in c.connections]
+    case = dataclasses.replace(c, boundaries=bcs, connections=conns)
+    case.check_period = 5
+    ref = oracle_mod.run_reference(case, 10)
+    f = ref["f"][0]
+    # FDPeriodic nodes of the Left face hold zeros, the interior is NaN
+    assert np.all(f[:-1, 1:-1, 0] == 0.0)
+    assert np.isnan(f[1:-1, 1:-1, 2:-2]).all()
+    # the residual of rho is 0/0 (every interior rho is NaN but the sums
+    # skip nothing): the reference reports NaN for u, v, w at least
+    assert np.isnan(ref["residual"][-1][2][1:]).all()

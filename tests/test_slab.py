@@ -65,6 +65,7 @@ class _FakePart:
     def __init__(self, rank, world, nbytes=64):
         self.rank = rank
         self.out, self.inb, self.got = {}, {}, {}
+        self.events = []
         for side, present in (("low", rank > 0), ("high", rank < world - 1)):
             self.out[side] = (torch.full((nbytes,), 10 * rank + (side == "high"),
                                          dtype=torch.uint8)
@@ -73,13 +74,20 @@ class _FakePart:
                               if present else None)
 
     def export_faces(self):
-        pass
+        self.events.append("export")
 
     def synchronize(self):
         pass
 
+    def step_begin(self):
+        self.events.append("begin")
+
+    def step_finish(self):
+        self.events.append("finish")
+
     def import_face(self, side, buf):
         self.got[side] = int(buf[0])
+        self.events.append("import")
 
 
 class _FakeSolver:
@@ -95,15 +103,16 @@ def _rank(rank, world, port, out):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     s = _FakeSolver(rank, world)
-    slab.DistExchange().exchange(s)
-    out.put((rank, dict(s.parts[0].got)))
+    slab.DistExchange().step(s)
+    out.put((rank, dict(s.parts[0].got), list(s.parts[0].events)))
     dist.barrier()
     dist.destroy_process_group()
 
 
 def test_faces_cross_between_three_gloo_ranks():
     """Rank k's low halo gets rank k-1's high export and its high halo
-    rank k+1's low export."""
+    rank k+1's low export, after its step's interior part was queued and
+    before the step is finished."""
     with socket.socket() as sk:
         sk.bind(("127.0.0.1", 0))
         port = sk.getsockname()[1]
@@ -114,10 +123,17 @@ def test_faces_cross_between_three_gloo_ranks():
              for r in range(world)]
     for p in procs:
         p.start()
-    got = dict(q.get(timeout=120) for _ in range(world))
+    res = [q.get(timeout=120) for _ in range(world)]
+    got = {r: g for r, g, _ in res}
+    events = {r: e for r, _, e in res}
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
+    # the faces move between the step's interior part and its finish
+    nimp = {0: 1, 1: 2, 2: 1}
+    for r in range(world):
+        assert events[r] == ["export", "begin"] + ["import"] * nimp[r] + \
+            ["finish"]
     assert got[0] == {"high": 10 * 1 + 0}
     assert got[1] == {"low": 10 * 0 + 1, "high": 10 * 2 + 0}
     assert got[2] == {"low": 10 * 1 + 1}

@@ -33,13 +33,17 @@ def _noalloc(lib, q, qold):
     return s[0::2] / s[1::2]
 
 
-def test_noalloc_residual_matches_residual(gpu_lib):
-    case = config.cavity(3, 40, 0.05, re=100)
+@pytest.mark.parametrize("dim,n", [(3, 40), (2, 300)])
+def test_noalloc_residual_matches_residual(gpu_lib, dim, n):
+    # 3D: four variables; 2D: three (rho, u, v) over 90,000 nodes, a
+    # partial last CTA
+    case = config.cavity(dim, n, 0.05, re=100)
     s = Solver(case)
     s.init_uniform()
-    shp = (40, 40, 40)
+    shp = s._shape(0)
     qold = [torch.ones(shp, dtype=torch.float64, device="cuda")] + [
-        torch.zeros(shp, dtype=torch.float64, device="cuda") for _ in range(3)]
+        torch.zeros(shp, dtype=torch.float64, device="cuda")
+        for _ in range(dim)]
     for _ in range(2):
         s.stream_collision(25)
         s.update_macro_vars()
