@@ -42,14 +42,16 @@ sys.path.insert(0, ROOT)
 BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
                   ("fp32", 2): 72, ("fp16", 3): 76, ("fp16", 2): 36}
 # DRAM bytes per node update of the step kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of SplitStepKernel<3,double>
-# on the 128^3 cavity, 2 launches: 615 MB / 2,097,152 nodes; FP32: 311 MB;
-# captured with `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
-# --clock-control none -k regex:SplitStepKernel -s 5 -c 2 python bench.py
-# --size 128 --steps 10 --warmup 3 --no-cpu-baseline --precision fp64`).
-# Traffic grows with the node count, so a 256^3 launch moves this x
-# 16,777,216 bytes.
-TRAFFIC_PER_NODE = {("fp64", 3): 293.0, ("fp32", 3): 148.0}
+# (dram__bytes_read.sum + dram__bytes_write.sum of SplitStepKernel on the
+# 192^3 cavity, whose population arrays (1.08 GB FP64, 0.54 GB FP32) are
+# well beyond the 126 MB L2; mean of 2 launches over 7,077,888 nodes:
+# FP64 2,152.4 MB = 304.1 B, FP32 1,088.2 MB = 153.7 B), captured with
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,
+# gpu__time_duration.sum --clock-control none -k regex:SplitStepKernel -s 3
+# -c 2 python bench.py --size 192 --steps 10 --warmup 3 --no-cpu-baseline
+# --no-forms --min-time 0 --precision fp64|fp32`.  Traffic grows with the
+# node count, so a 256^3 launch moves this x 16,777,216 bytes.
+TRAFFIC_PER_NODE = {("fp64", 3): 304.1, ("fp32", 3): 153.7}
 METRIC = "MLUPS (D3Q19 3D lid-driven cavity 256^3)"
 DTYPES = {"fp64": "f64", "fp32": "f32 (shifted f - w)",
           "fp16": "f16 storage of (f - w)/w, f32 arithmetic"}
@@ -87,11 +89,12 @@ def parse():
                    help="lchannel: steps (checks every 1,000)")
     p.add_argument("--quick", action="store_true",
                    help="precision: small channels instead of the full ones")
-    p.add_argument("--decomp", default="replicas",
-                   choices=["replicas", "slab"],
-                   help="N > 1 on the cavity: independent 256^3 replicas, or "
-                        "one 256 x 256 x 256N cavity cut into z slabs with "
-                        "a face exchange (NCCL) before every step")
+    p.add_argument("--decomp", default="auto",
+                   choices=["auto", "replicas", "slab"],
+                   help="N > 1 on the cavity: one 256 x 256 x 256N cavity "
+                        "cut into z slabs with a face exchange (NCCL) in "
+                        "every step (auto, the default for N > 1), or "
+                        "independent 256^3 replicas")
     p.add_argument("--scheme", default="stream", choices=["stream", "swap"],
                    help="swap: the reference's one-array swap step "
                         "(Scheme_StreamCollision_Swap), half the memory")
@@ -287,14 +290,21 @@ def run_reference_arm(args, rank, world):
         "warmup": args.warmup, "ms_per_step": secs / n * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": cavity_config(args, world, case.nodes()),
+        "config": (slab_config(args, world, case.nodes())
+                   if use_slab(args, world)
+                   else cavity_config(args, world, case.nodes())),
         "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": threads,
                          "kind": "reference", "cpu_model": cpu_model(),
                          "sample": f"{n} {step_name} steps of the "
                                    f"{args.size}^3 cavity after "
                                    f"{args.warmup} warm-up steps (reference "
                                    "sources + sequential OPS stand-in, "
-                                   "OpenMP)"},
+                                   "OpenMP)" +
+                                   (f"; one slab's share of the {args.size}"
+                                    f" x {args.size} x {args.size * world} "
+                                    "cavity, the reference's cost per node "
+                                    "being that of the whole block"
+                                    if use_slab(args, world) else "")},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -596,13 +606,33 @@ def run_precision(args):
 
 
 
+def slab_config(args, world, local_nodes):
+    """The `config` of the slab-decomposed cavity (both arms)."""
+    n = args.size
+    face = 5 * n * n * (8 if args.precision == "fp64" else
+                        4 if args.precision == "fp32" else 2)
+    return {"workload": f"3D lid-driven cavity D3Q19 {n} x {n} x "
+                        f"{n * world} {args.precision.upper()}, lid 0.05 "
+                        f"(lattice), Re 400, z slabs of {n}^3 per GPU",
+            "nodes_per_gpu": local_nodes, "parallelism": f"slab{world}",
+            "exchange_bytes_per_step_per_cut": 2 * face,
+            "l2": "population arrays larger than L2"}
+
+
+def use_slab(args, world):
+    return args.workload == "cavity3d" and (
+        args.decomp == "slab" or (args.decomp == "auto" and world > 1))
+
+
 def run_slab(args, rank, world, local):
     """One 256 x 256 x 256N cavity cut into N z slabs, one per GPU (weak
-    scaling: 256^3 nodes per GPU); before every step each rank exports the
-    populations leaving its slab through each cut face and swaps them with
-    its neighbour (NCCL send/recv), then imports the neighbour's into its
-    halo.  Timed on the device over the K steps including the exchanges,
-    max over ranks."""
+    scaling: 256^3 nodes per GPU).  Every step: each rank exports the
+    populations leaving its slab through its cut faces, queues the step's
+    interior (which reads no halo), sends and receives the faces (NCCL, on
+    a side stream, overlapping the interior), imports the neighbours' faces
+    into its halos and finishes the step - no host wait inside the loop.
+    Timed with CUDA events on the library's stream over K steps including
+    the exchanges, repeated for at least a second, max over ranks."""
     import datetime
 
     import numpy as np
@@ -626,26 +656,30 @@ def run_slab(args, rank, world, local):
     s.init_uniform()
     s.stream_collision(args.warmup)
     part.synchronize()
+    ctx = torch.cuda.ExternalStream(part.stream_ptr())
     launches0 = part.solver.launch_count()
+
+    def run_k():
+        barrier(world)
+        part.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(ctx)
+        s.stream_collision(args.steps)
+        ev1.record(ctx)
+        ev1.synchronize()
+        barrier(world)
+        return ev0.elapsed_time(ev1)
+
     clocks = ClockSampler(local)
     clocks.start()
-    barrier(world)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    s.stream_collision(args.steps)
-    part.synchronize()
-    ev1.record()
-    ev1.synchronize()
+    times = repeat_timed(run_k, world, args.min_time)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    launches = part.solver.launch_count() - launches0
-    ms_max = max_over_ranks(ms, world)
+    launches = (part.solver.launch_count() - launches0) // len(times)
+    ms_max = statistics.median(times)
     value = nodes * args.steps / (ms_max * 1e-3) / 1e6
-    step_kernel_ms = part.solver.last_step_ms()   # the last step's kernel
     bpn = BYTES_PER_NODE[(case.precision, 3)]
-    achieved = bpn * local_nodes / (step_kernel_ms * 1e-3) / 1e9
+    achieved = bpn * local_nodes / (ms_max / args.steps * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     # end to end: initial fields from pinned host memory, K steps, moments
     # back to pinned host memory
@@ -676,26 +710,22 @@ def run_slab(args, rank, world, local):
         raise RuntimeError("non-finite density after the slab run")
     if rank != 0:
         return
-    face = 5 * n * n * (8 if case.precision == "fp64" else
-                        4 if case.precision == "fp32" else 2)
     line = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": DTYPES[args.precision], "data": "synthetic",
-        "config": {"workload": f"3D lid-driven cavity D3Q19 {n} x {n} x "
-                               f"{n * world} {args.precision.upper()}, lid "
-                               "0.05 (lattice), Re 400, z slabs of "
-                               f"{n}^3 per GPU",
-                   "nodes_per_gpu": local_nodes,
-                   "parallelism": f"slab{world}",
-                   "exchange_bytes_per_step_per_cut": 2 * face,
-                   "l2": "population arrays larger than L2"},
+        "config": slab_config(args, world, local_nodes),
+        "timing": {"repetitions": len(times),
+                   "statistic": "median over repetitions of K timed steps "
+                                "(max over ranks)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "bytes_per_node": bpn,
-                     "traffic": None},
+                     "traffic": None,
+                     "note": "per-node bytes over the whole step, face "
+                             "exchange included"},
         "e2e": {"value": e2e, "unit": "MLUPS",
                 "h2d_bytes_per_step": 4 * 8 * nodes / args.steps,
                 "d2h_bytes_per_step": 4 * 8 * nodes / args.steps},
@@ -731,7 +761,7 @@ def main():
             torch.cuda.set_device(local)
             run_precision(args)
         return
-    if args.decomp == "slab" and args.workload == "cavity3d":
+    if use_slab(args, world):
         run_slab(args, rank, world, local)
         return
     if args.workload == "cavities":

@@ -193,13 +193,14 @@ mplbgpu_status mplbgpu_step(mplbgpu_ctx* ctx, int nsteps);
 
 /* One step in two calls, for decomposed blocks whose cut faces come from
  * another GPU: mplbgpu_step_begin queues the part of the step that reads
- * no halo layer (the interior of every block whose rows are longer than
- * two 32-byte sectors), mplbgpu_step_finish the rest (shell rows, row
- * edges, deferred boundary nodes, block-to-block halos).  Between the two
- * only mplbgpu_export_face / mplbgpu_import_face are accepted (other calls
- * return MPLBGPU_ERR_STATE), so a face transfer on another stream overlaps
- * the interior's computation when the import waits for it.  begin + finish
- * is one mplbgpu_step(ctx, 1), bit for bit.  Two-array scheme only. */
+ * no halo layer beyond a y or z face (the x faces and interior rows of
+ * every block), mplbgpu_step_finish the rest (the rows on a y or z face,
+ * deferred boundary nodes, block-to-block halos).  Between the two only
+ * mplbgpu_export_face and mplbgpu_import_face of y and z faces are
+ * accepted (other calls return MPLBGPU_ERR_STATE), so a face transfer on
+ * another stream overlaps the interior's computation when the import waits
+ * for it.  begin + finish is one mplbgpu_step(ctx, 1), bit for bit.
+ * Two-array scheme only. */
 mplbgpu_status mplbgpu_step_begin(mplbgpu_ctx* ctx);
 mplbgpu_status mplbgpu_step_finish(mplbgpu_ctx* ctx);
 
@@ -316,11 +317,7 @@ typedef struct {
                         FP32 */
     int persistent;  /* 1: one cooperative launch per chunk of steps with a
                         bounded grid barrier between steps; 0: one launch
-                        per step (one CTA per tile), a chunk replayed from
-                        a CUDA graph; 2: the same with a grid of the CTAs
-                        that fit on the device whose warps walk the tiles,
-                        each loading its next piece of work before
-                        computing the current one */
+                        per step, a chunk replayed from a CUDA graph */
     int chunk;       /* steps per chunk (even) */
     int ctas_per_sm; /* CTAs per SM of the persistent launches (at most
                         the co-resident count) */

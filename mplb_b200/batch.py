@@ -128,7 +128,9 @@ def shard(specs: Sequence[CavitySpec], rank: int, world: int,
 
 
 class BatchError(RuntimeError):
-    pass
+    def __init__(self, message, status=None):
+        self.status = status
+        super().__init__(message)
 
 
 class Batch:
@@ -146,7 +148,8 @@ class Batch:
                                            abi.PRECISIONS[precision],
                                            ctypes.byref(h))
         if rc != abi.OK:
-            raise BatchError(self.lib.mplbgpu_batch_last_error(None).decode())
+            raise BatchError(self.lib.mplbgpu_batch_last_error(None).decode(),
+                             rc)
         self.h = h
         self.precision = precision
         self.offsets = np.cumsum([0] + [s.n * s.n for s in self.specs])
@@ -165,7 +168,8 @@ class Batch:
     def _check(self, rc):
         if rc != abi.OK:
             raise BatchError(f"{abi.STATUS_NAMES.get(rc, rc)}: " +
-                             self.lib.mplbgpu_batch_last_error(self.h).decode())
+                             self.lib.mplbgpu_batch_last_error(self.h).decode(),
+                             rc)
 
     @property
     def total_nodes(self) -> int:
@@ -175,6 +179,11 @@ class Batch:
                    ctas_per_sm=8):
         t = abi.BatchTuning(tile_nodes, persistent, chunk, ctas_per_sm)
         self._check(self.lib.mplbgpu_batch_set_tuning(self.h, ctypes.byref(t)))
+
+    def set_wait_limit(self, polls):
+        """Polls before a grid barrier of the persistent launch gives up
+        (MPLBGPU_ERR_TIMEOUT, after which the batch needs init again)."""
+        self._check(self.lib.mplbgpu_batch_set_wait_limit(self.h, int(polls)))
 
     def tuning(self):
         t = abi.BatchTuning()
@@ -242,8 +251,8 @@ def _cache_key(batch: Batch) -> str:
 
 
 def default_candidates():
-    """Tile size x launch style (x CTAs per SM, which only the persistent
-    launch uses)."""
+    """Tile size x launch style: one CTA per tile (persistent 0) or
+    cooperative persistent steps (1, x CTAs per SM)."""
     graph = [dict(tile_nodes=t, persistent=0, chunk=50, ctas_per_sm=8)
              for t in (64, 128, 256)]
     persistent = [dict(tile_nodes=t, persistent=1, chunk=50, ctas_per_sm=k)

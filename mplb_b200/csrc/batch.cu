@@ -62,6 +62,7 @@ struct mplbgpu_batch {
     long long launches = 0;
     unsigned long long seed = 1;
     bool initialised = false;
+    long long wait_limit = (long long)1 << 26;  // grid barrier polls
     std::string err;
 };
 
@@ -186,7 +187,7 @@ int LaunchChunk(mplbgpu_batch* b, int nsteps, bool macro_last) {
     const int threads = b->tune.tile_nodes / BatchNodesPerThread<T>();
     if (b->tune.persistent) {
         const GridSync gs{b->sync_count, b->sync_gen, b->sync_err,
-                          (long long)1 << 26};
+                          b->wait_limit};
         T* a = b->cur == 0 ? P0 : P1;
         T* c = b->cur == 0 ? P1 : P0;
         cudaError_t e = BatchLaunch<T>::Persistent(Grid(b, true), threads,
@@ -273,8 +274,12 @@ int CheckSync(mplbgpu_batch* b) {
     if (err) {
         cudaMemsetAsync(b->sync_err, 0, sizeof(int), b->stream);
         cudaMemsetAsync(b->sync_count, 0, sizeof(unsigned), b->stream);
+        // the CTAs that gave up left their steps undone: the fields are a
+        // mix of steps, so the batch needs a new initial state
+        b->initialised = false;
         return BErr(b, MPLBGPU_ERR_TIMEOUT,
-                    "a grid barrier of the persistent kernel gave up waiting");
+                    "a grid barrier of the persistent kernel gave up waiting "
+                    "(the batch must be initialised again)");
     }
     return MPLBGPU_OK;
 }
@@ -466,6 +471,8 @@ mplbgpu_status mplbgpu_batch_set_tuning(mplbgpu_batch* b,
                     "tile_nodes too small for the FP32 form's nodes per thread");
     if (t->chunk < 2 || (t->chunk & 1))
         return BErr(b, MPLBGPU_ERR_INVALID, "chunk must be even and >= 2");
+    if (t->persistent < 0 || t->persistent > 1)
+        return BErr(b, MPLBGPU_ERR_INVALID, "persistent must be 0 or 1");
     if (t->ctas_per_sm < 1 || t->ctas_per_sm > 32)
         return BErr(b, MPLBGPU_ERR_INVALID, "ctas_per_sm must be 1..32");
     const bool retile = t->tile_nodes != b->tune.tile_nodes;
@@ -477,6 +484,17 @@ mplbgpu_status mplbgpu_batch_set_tuning(mplbgpu_batch* b,
         if (rc != MPLBGPU_OK) return rc;
         return UploadActive(b);
     }
+    return MPLBGPU_OK;
+}
+
+mplbgpu_status mplbgpu_batch_set_wait_limit(mplbgpu_batch* b,
+                                            long long polls) {
+    if (!b) return MPLBGPU_ERR_INVALID;
+    if (polls < 1)
+        return BErr(b, MPLBGPU_ERR_INVALID, "the wait limit must be >= 1");
+    b->wait_limit = polls;
+    DropGraphs(b);   // captured persistent launches carry the old limit
+    b->graph_ok = true;
     return MPLBGPU_OK;
 }
 

@@ -168,6 +168,7 @@ __host__ __device__ constexpr int BatchNodesPerThread() {
     return sizeof(T) < 8 ? MPLB_BATCH_GROUP : 1;
 }
 
+
 template <typename T, bool MACRO>
 __device__ __forceinline__ void BatchSweep(const BatchDev& bd,
                                            const PhysConst& pc, int nt,

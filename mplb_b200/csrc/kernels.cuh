@@ -84,9 +84,12 @@ struct BlockDev {
     // region PURE); center_fluid: the interior is fluid-like
     int split;
     int center_fluid;
-    // the split step runs as EdgeStepKernel + PipeStepKernel (rows longer
-    // than two 32-byte sectors)
-    int pipe;
+    // deferred nodes in one kernel (no deferred node reads another):
+    // per region, the first entry of its operation list in dops_flat (each
+    // list in definition order, ended by -1)
+    int deferred_fused;
+    int dops_first[kNumRegions];
+    const int* dops_flat;
     // per region: class (bits 0-1) and fluid-like flag (bit 2); the pulled
     // and the stale populations (copies of RegionInfo::pull / ::stale)
     uint8_t rflags[kNumRegions];
@@ -633,116 +636,17 @@ __device__ __forceinline__ void MomentsCollideT(typename Prec<T>::C* f,
     MomentsCollideT<L, T>(f, pc, fluidlike, pc.omc, pc.omcf, rho, u);
 }
 
-// Wall velocity of node (x, y, z) under an operation with a per-node field
-// (u, v, w per node of the boundary's surface range, x fastest).
-template <typename L>
-__device__ __forceinline__ void FieldVelocity(const RegionOp& op, int x, int y,
-                                              int z, double uw[3]) {
+// The operation that applies at node (x, y, z): the region's own, or with
+// a per-node wall velocity that node's entry of the boundary's per-node
+// operations (the same masks, its own constants).
+__device__ __forceinline__ const RegionOp& NodeOp(const RegionOp& op, int x,
+                                                  int y, int z) {
+    if (op.node_ops == nullptr) return op;
     const long long k =
         ((long long)(z - op.forg[2]) * op.fext[1] + (y - op.forg[1])) *
             op.fext[0] +
         (x - op.forg[0]);
-    const double* p = op.field + 3 * k;
-    uw[0] = p[0];
-    uw[1] = p[1];
-    uw[2] = L::D == 3 ? p[2] : 0.0;
-}
-
-// (CS c_l) . u_w, the reference's order (cx u + cy v) + cz w with
-// cx = CS * XI (Src/boundary_kernel.inc:1218-1231).
-template <typename L>
-__device__ __forceinline__ double WallCu(double CS, int l, const double uw[3]) {
-    const double cx = CS * (double)L::cx(l);
-    const double cy = CS * (double)L::cy(l);
-    if constexpr (L::D == 3) {
-        const double cz = CS * (double)L::cz(l);
-        return cx * uw[0] + cy * uw[1] + cz * uw[2];
-    } else {
-        return cx * uw[0] + cy * uw[1];
-    }
-}
-
-// CalcBGKFeq(l, rho, u, T = 1, order 2) / (w_l rho): the bracket of
-// Src/model_host_device.h:34-82 in its operation order.
-template <typename L>
-__device__ __forceinline__ double FeqBracket(double CS, int l,
-                                             const double u[3]) {
-    const double T = 1;
-    const double XI0 = L::cx(l), XI1 = L::cy(l);
-    double cu, c2, u2;
-    if constexpr (L::D == 2) {
-        cu = (CS * XI0 * u[0] + CS * XI1 * u[1]);
-        c2 = (CS * XI0 * CS * XI0 + CS * XI1 * CS * XI1);
-        u2 = u[0] * u[0] + u[1] * u[1];
-    } else {
-        const double XI2 = L::cz(l);
-        cu = (CS * XI0 * u[0] + CS * XI1 * u[1] + CS * XI2 * u[2]);
-        c2 = (CS * XI0 * CS * XI0 + CS * XI1 * CS * XI1 +
-              CS * XI2 * CS * XI2);
-        u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    }
-    const double cu2 = cu * cu;
-    return 1.0 + cu + 0.5 * (cu2 - u2 + (T - 1.0) * (c2 - L::D));
-}
-
-// EQMDiffuseRefl with the wall velocity of this node (a per-node field,
-// no counterpart in the reference, whose GivenVars are uniform): the
-// kernel's wall constants evaluated per node, FP64 in the reference's
-// operation order (the same values the uniform path takes from the plan).
-template <typename L, typename T>
-__device__ __noinline__ void ApplyEqmField(typename Prec<T>::C* f,
-                                           const RegionOp& op,
-                                           const PhysConst& pc, int x, int y,
-                                           int z) {
-    constexpr int Q = L::Q;
-    double uw[3];
-    FieldVelocity<L>(op, x, y, z, uw);
-    double deltaRho = 0.0, rhoParallel = 0.0;
-#pragma unroll
-    for (int l = 0; l < Q; l++) {
-        if (op.out_mask >> l & 1u)
-            deltaRho = deltaRho + (2.0 * pc.w[l]) * WallCu<L>(pc.cs, l, uw);
-        if (op.par_mask >> l & 1u)
-            rhoParallel =
-                rhoParallel + (pc.w[l] * 1.0) * FeqBracket<L>(pc.cs, l, uw);
-    }
-    const double denom = 1.0 - deltaRho - rhoParallel;
-    if constexpr (Prec<T>::kShifted) {
-        float sin = 0.0f;
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.in_mask >> i & 1u) sin += f[i];
-        const float inv = 1.0f / (float)denom;
-        const float drw = ((float)(2.0 * op.win - denom) + 2.0f * sin) * inv;
-        const float rhoWall = 1.0f + drw;
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            if (op.par_mask >> i & 1u) {
-                const double a = FeqBracket<L>(pc.cs, i, uw);
-                f[i] = pc.wf[i] * ((float)(a - 1.0) + drw * (float)a);
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.out_mask >> i & 1u)
-                f[i] = f[L::opp(i)] + 2.0f * rhoWall * pc.wf[i] *
-                                          (float)WallCu<L>(pc.cs, i, uw);
-    } else {
-        double rhoIn = 0.0;
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.in_mask >> i & 1u) rhoIn = rhoIn + f[i];
-        const double rhoWall = (2.0 * rhoIn) / denom;
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.par_mask >> i & 1u)
-                f[i] = (pc.w[i] * rhoWall) * FeqBracket<L>(pc.cs, i, uw);
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.out_mask >> i & 1u)
-                f[i] = f[L::opp(i)] +
-                       ((2.0 * rhoWall) * pc.w[i]) * WallCu<L>(pc.cs, i, uw);
-    }
+    return op.node_ops[k];
 }
 
 // EQMDiffuseRefl (KerCutCellEQMDiffuseRefl3D, Src/boundary_kernel.inc:
@@ -750,14 +654,11 @@ __device__ __noinline__ void ApplyEqmField(typename Prec<T>::C* f,
 // forms use sum_in f = sum_in h + sum_in w and w_opp(i) = w_i.
 template <typename L, typename T>
 __device__ __forceinline__ void ApplyEqm(typename Prec<T>::C* f,
-                                         const RegionOp& op,
+                                         const RegionOp& rop,
                                          const PhysConst& pc, int x, int y,
                                          int z) {
     constexpr int Q = L::Q;
-    if (op.field != nullptr) {
-        ApplyEqmField<L, T>(f, op, pc, x, y, z);
-        return;
-    }
+    const RegionOp& op = NodeOp(rop, x, y, z);
     if constexpr (Prec<T>::kShifted) {
         // rhoWall - 1 and w_i (rhoWall a_i - 1) without cancellation
         float sin = 0.0f;
@@ -796,26 +697,14 @@ __device__ __forceinline__ void ApplyEqm(typename Prec<T>::C* f,
 // for the deviation because w_opp(i) = w_i.
 template <typename L, typename T>
 __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
-                                         const RegionOp& op,
+                                         const RegionOp& rop,
                                          const PhysConst& pc,
                                          const T* __restrict__ src,
                                          const BlockDev& b, long long node,
                                          int x, int y, int z) {
     constexpr int Q = L::Q;
     using P = Prec<T>;
-    if (op.field != nullptr) {
-        // wall velocity of this node: 2 w_i (c_i . u_w) as the plan forms it
-        double uw[3];
-        FieldVelocity<L>(op, x, y, z, uw);
-#pragma unroll
-        for (int i = 0; i < Q; i++)
-            if (op.out_mask >> i & 1u)
-                f[i] = P::Load(src, L::opp(i) * b.popstride + node, L::opp(i),
-                               pc) +
-                       (typename P::C)((2.0 * pc.w[i]) *
-                                       WallCu<L>(pc.cs, i, uw));
-        return;
-    }
+    const RegionOp& op = NodeOp(rop, x, y, z);
 #pragma unroll
     for (int i = 0; i < Q; i++)
         if (op.out_mask >> i & 1u)
@@ -1017,7 +906,12 @@ __device__ __forceinline__ void GroupFinish(const BlockDev& b,
         // FP16 pairs: population i of the two converted together by the
         // hardware's stochastic rounding (cvt.rs.f16x2.f32 with 32 random
         // bits per pair)
-        const Rng rg = SeedRng(pc.seed, n.node[n.first]);
+        // the first valid node's index, without a dynamic array index
+        long long seed_node = n.node[0];
+#pragma unroll
+        for (int j = 1; j < G; j++)
+            if (j == n.first) seed_node = n.node[j];
+        const Rng rg = SeedRng(pc.seed, seed_node);
 #pragma unroll
         for (int i = 0; i < Q; i++) {
             const uint32_t pair = StochasticHalf2(n.f[0][i] * pc.winvf[i],
@@ -1114,7 +1008,9 @@ __host__ __device__ constexpr long long SplitChunkCtas(int n0) {
 // The step with no warp mixing interior and boundary nodes (a warp holding
 // one boundary node runs that node's boundary programme with the other 31
 // lanes idle: at 128^3 a third of the issue slots had no work).  One launch,
-// three kinds of CTA by blockIdx.x:
+// three kinds of CTA by blockIdx.x + blk0 (a step in two parts launches
+// kinds 2 and 3, which read no halo layer of a cut z face, apart from
+// kind 1):
 //   1. shell rows: every row with y or z on the block boundary (coalesced);
 //   2. per chunk of 64 interior rows, one CTA for their x = 0 and x = n0 - 1
 //      nodes, followed by
@@ -1129,14 +1025,15 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                            ? MPLB_F64_MIN_BLOCKS
                                            : MPLB_LP_MIN_BLOCKS)
     SplitStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
-                    T* __restrict__ dst) {
+                    T* __restrict__ dst, unsigned blk0) {
     // block and row counts fit in 32 bits (the launcher checks the grid),
     // so the index arithmetic stays 32-bit
     const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
     const int ny = b.n[1] - 2;
     const int nz = D == 3 ? b.n[2] : 1;
     const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
-    unsigned blk = blockIdx.x;
+    // blk0: a launch of the interior part alone starts after the shell rows
+    unsigned blk = blockIdx.x + blk0;
     if (blk < nsr) {
         const int row = (int)(blk / nbx);
         const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
@@ -1173,137 +1070,6 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     if (k.r < 0 || k.r >= rows) return;
     PureNodeGroup<D, T, O32, G>(b, pc, src, dst, k.x0, 1 + k.r % ny,
                                 D == 3 ? 1 + k.r / ny : 0);
-}
-
-// ---------------------------------------------------------------------------
-// Software-pipelined step, two launches (blocks whose interior region is
-// PURE and whose rows are longer than two sectors):
-//   EdgeStepKernel : the shell rows (y or z on the block boundary) and the
-//                    first and last S nodes of every interior row, S the
-//                    values of one 32-byte sector (4 FP64, 8 FP32, 16
-//                    FP16), one node per thread (StepNode: the x faces'
-//                    boundary programmes run here);
-//   PipeStepKernel : x in [S, n0 - S) of every interior row as warp tasks
-//                    of 32 G nodes in a persistent grid.  Each warp walks
-//                    its tasks holding two register sets: the next task's
-//                    populations are loaded before the current task is
-//                    collided and stored, so the warp's loads stay in
-//                    flight while it computes (a one-task warp waits for
-//                    its loads, then computes with none in flight).
-// The two launches share no 32-byte sector of any population row: a sector
-// written in part by one and in part by the other costs a read-modify-write
-// in HBM when the parts do not meet in L2.
-template <typename T>
-__host__ __device__ constexpr int SectorNodes() {
-    return 32 / (int)sizeof(T);
-}
-
-struct PipeGeom {
-    int xs, xe;       // x range of the pipelined tasks, [xs, xe)
-    int tpr;          // tasks per interior row
-    int ny;           // interior rows per z plane (n1 - 2)
-    long long rows;   // interior rows
-    long long tasks;  // tpr * rows
-};
-
-// Pipelined CTAs per SM: two register sets of a node group.
-#ifndef MPLB_PIPE_MIN_BLOCKS
-#define MPLB_PIPE_MIN_BLOCKS 4
-#endif
-
-// Node group of pipelined task t (warp-uniform): row, segment and lane.
-template <int D, typename T, bool O32, int G>
-__device__ __forceinline__ void PipeSetup(const BlockDev& b,
-                                          const PipeGeom& g, long long t,
-                                          NodeGroup<D, T, G>& n) {
-    const long long row = t / g.tpr;
-    const int seg = (int)(t - row * g.tpr);
-    const int y = 1 + (int)(row % g.ny);
-    const int z = D == 3 ? 1 + (int)(row / g.ny) : 0;
-    const int x0 = g.xs + seg * 32 * G + (int)(threadIdx.x & 31);
-    n.first = 0;
-#pragma unroll
-    for (int j = 0; j < G; j++) {
-        const int x = x0 + 32 * j;
-        n.valid[j] = x < g.xe;
-        // an invalid node reads the row's last pipelined node (in bounds)
-        n.node[j] = NodeIndexT<D, O32>(b, n.valid[j] ? x : g.xe - 1, y, z);
-    }
-}
-
-template <int D, typename T, bool O32>
-__global__ void __launch_bounds__(128, MPLB_PIPE_MIN_BLOCKS)
-    PipeStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
-                   T* __restrict__ dst, PipeGeom g) {
-    constexpr int G = SplitGroup<T>();
-    const int warps = (int)(blockDim.x >> 5);
-    const long long stride = (long long)gridDim.x * warps;
-    long long t = (long long)blockIdx.x * warps + (threadIdx.x >> 5);
-    if (t >= g.tasks) return;
-    NodeGroup<D, T, G> a, c;
-    PipeSetup<D, T, O32, G>(b, g, t, a);
-    GroupLoad<D, T, O32, G>(b, pc, src, a);
-    // two register sets in turn (no copies between them)
-    while (true) {
-        long long nt = t + stride;
-        if (nt < g.tasks) {
-            PipeSetup<D, T, O32, G>(b, g, nt, c);
-            GroupLoad<D, T, O32, G>(b, pc, src, c);
-        }
-        GroupFinish<D, T, O32, G>(b, pc, dst, a);
-        if (nt >= g.tasks) return;
-        t = nt;
-        nt = t + stride;
-        if (nt < g.tasks) {
-            PipeSetup<D, T, O32, G>(b, g, nt, a);
-            GroupLoad<D, T, O32, G>(b, pc, src, a);
-        }
-        GroupFinish<D, T, O32, G>(b, pc, dst, c);
-        if (nt >= g.tasks) return;
-        t = nt;
-    }
-}
-
-// Shell rows (as SplitStepKernel's first CTAs) and the 2 S edge nodes of
-// every interior row, one node per thread.
-template <int D, typename T, bool O32>
-__global__ void __launch_bounds__(128, std::is_same<T, double>::value
-                                           ? MPLB_F64_MIN_BLOCKS
-                                           : MPLB_LP_MIN_BLOCKS)
-    EdgeStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
-                   T* __restrict__ dst, PipeGeom g) {
-    const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
-    const int ny = b.n[1] - 2;
-    const int nz = D == 3 ? b.n[2] : 1;
-    const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
-    const unsigned blk = blockIdx.x;
-    if (blk < nsr) {
-        const int row = (int)(blk / nbx);
-        const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
-        if (x >= b.n[0]) return;
-        int y, z;
-        if (row < 2 * nz) {
-            y = (row & 1) ? b.n[1] - 1 : 0;
-            z = row >> 1;
-        } else {
-            const int r2 = row - 2 * nz;
-            z = (r2 & 1) ? b.n[2] - 1 : 0;
-            y = 1 + (r2 >> 1);
-        }
-        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
-                                       nullptr, nullptr, x, y, z);
-        return;
-    }
-    constexpr int S = SectorNodes<T>();
-    const long long e =
-        (long long)(blk - nsr) * blockDim.x + threadIdx.x;   // edge node
-    const long long row = e / (2 * S);
-    if (row >= g.rows) return;
-    const int k = (int)(e - row * 2 * S);
-    const int x = k < S ? k : g.xe + (k - S);
-    StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr, nullptr,
-                                   nullptr, x, 1 + (int)(row % g.ny),
-                                   D == 3 ? 1 + (int)(row / g.ny) : 0);
 }
 
 // Deferred nodes: thread t -> (region, node).
@@ -1359,6 +1125,99 @@ struct DeferredSeg {
 // (EQMDiffuseRefl, ExtrapolPressure1ST or halfway bounce-back).  The
 // extrapolation reads the inner neighbour's current f: from the store when
 // it is deferred, otherwise (a pure node) straight from its upstream g.
+// One boundary operation on a deferred node (x, y, z) holding f
+// (EQMDiffuseRefl, halfway bounce-back or ExtrapolPressure1ST).  The
+// extrapolation reads the inner neighbour's current f: from the store when
+// it is deferred, otherwise from its upstream g (pure), with its earlier
+// boundary operations applied (local).
+template <int D, typename T>
+__device__ __forceinline__ void DeferredApply(const BlockDev& b,
+                                              const PhysConst& pc,
+                                              const T* __restrict__ src,
+                                              const RegionOp& op, int x, int y,
+                                              int z,
+                                              typename Prec<T>::C* f) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int Q = L::Q;
+    if (op.kind == kOpEqm) {
+        ApplyEqm<L, T>(f, op, pc, x, y, z);
+    } else if (op.kind == kOpHbb) {
+        ApplyHbb<L, T>(f, op, pc, src, b, NodeIndex<D>(b, x, y, z), x, y, z);
+    } else if (op.kind == kOpExtrapol) {
+        int q[3] = {x, y, z};
+        if (op.nb_axis >= 0) q[op.nb_axis] += op.nb_sign;
+        const int nr = RegionOf(q[0], q[1], q[2], b.n, D);
+        const RegionInfo& N = b.regions[nr];
+        const bool nbdef = N.cls == kDeferred;
+        const long long nk =
+            nbdef ? N.side_base + LocalIndex(N, q[0], q[1], q[2]) : 0;
+        const long long nnode = NodeIndex<D>(b, q[0], q[1], q[2]);
+        // the neighbour's post-boundary f as the reference has it when this
+        // boundary runs: the store (deferred), its pulled values (pure), or
+        // its pulled and stale values after its boundary operations that
+        // come before this one (local)
+        C g[Q];
+        if (N.cls == kLocal) {
+#pragma unroll
+            for (int i = 0; i < Q; i++)
+                g[i] = (N.pull >> i & 1u)
+                           ? P::Load(src, i * b.popstride + nnode +
+                                              UpOffset<L>(b, i), i, pc)
+                           : (C)0;
+            if (N.stale) {
+                const double* st =
+                    b.stale + (N.side_base + LocalIndex(N, q[0], q[1], q[2])) * Q;
+#pragma unroll
+                for (int i = 0; i < Q; i++)
+                    if (N.stale >> i & 1u) g[i] = (C)st[i];
+            }
+            for (int j = 0; j < N.nops; j++) {
+                const RegionOp& nop = b.ops[N.op[j]];
+                if (nop.bc >= op.bc) break;
+                if (nop.kind == kOpEqm)
+                    ApplyEqm<L, T>(g, nop, pc, q[0], q[1], q[2]);
+                else if (nop.kind == kOpHbb)
+                    ApplyHbb<L, T>(g, nop, pc, src, b, nnode, q[0], q[1],
+                                   q[2]);
+            }
+        }
+        if constexpr (P::kShifted) {
+            // f_i = (h_i + w_i) rho_given / rho for all but the last
+            float drho = 0.0f;
+#pragma unroll
+            for (int i = 0; i < Q; i++) {
+                if (op.in_mask >> i & 1u)
+                    f[i] = nbdef ? (C)b.fdef[i * b.ndef + nk]
+                           : N.cls == kLocal
+                               ? g[i]
+                               : P::Load(src, i * b.popstride + nnode +
+                                                  UpOffset<L>(b, i), i, pc);
+                drho += f[i];
+            }
+            const float rm1 = ((float)(op.rho_given - 1.0) - drho) / (1.0f + drho);
+#pragma unroll
+            for (int i = 0; i < Q - 1; i++) f[i] += (f[i] + pc.wf[i]) * rm1;
+        } else {
+            double rho = 0.0;
+#pragma unroll
+            for (int i = 0; i < Q; i++) {
+                if (op.in_mask >> i & 1u)
+                    f[i] = nbdef ? b.fdef[i * b.ndef + nk]
+                           : N.cls == kLocal
+                               ? g[i]
+                               : P::Load(src, i * b.popstride + nnode +
+                                                  UpOffset<L>(b, i), i, pc);
+                rho = rho + f[i];
+            }
+            const double ratio = op.rho_given / rho;
+#pragma unroll
+            for (int i = 0; i < Q - 1; i++) f[i] = f[i] * ratio;
+        }
+    }
+}
+
 template <int D, typename T>
 __global__ void DeferredOpKernel(BlockDev b, PhysConst pc,
                                  const T* __restrict__ src,
@@ -1379,54 +1238,50 @@ __global__ void DeferredOpKernel(BlockDev b, PhysConst pc,
     const int y = R.org[1] + (int)((loc / R.ext[0]) % R.ext[1]);
     const int z = R.org[2] + (int)(loc / ((long long)R.ext[0] * R.ext[1]));
     const long long k = R.side_base + loc;
-    const RegionOp& op = b.ops[sg.op];
     C f[Q];
 #pragma unroll
     for (int i = 0; i < Q; i++) f[i] = (C)b.fdef[i * b.ndef + k];
-    if (op.kind == kOpEqm) {
-        ApplyEqm<L, T>(f, op, pc, x, y, z);
-    } else if (op.kind == kOpHbb) {
-        ApplyHbb<L, T>(f, op, pc, src, b, NodeIndex<D>(b, x, y, z), x, y, z);
-    } else if (op.kind == kOpExtrapol) {
-        int q[3] = {x, y, z};
-        if (op.nb_axis >= 0) q[op.nb_axis] += op.nb_sign;
-        const int nr = RegionOf(q[0], q[1], q[2], b.n, D);
-        const RegionInfo& N = b.regions[nr];
-        const bool nbdef = N.cls == kDeferred;
-        const long long nk =
-            nbdef ? N.side_base + LocalIndex(N, q[0], q[1], q[2]) : 0;
-        const long long nnode = NodeIndex<D>(b, q[0], q[1], q[2]);
-        if constexpr (P::kShifted) {
-            // f_i = (h_i + w_i) rho_given / rho for all but the last
-            float drho = 0.0f;
-#pragma unroll
-            for (int i = 0; i < Q; i++) {
-                if (op.in_mask >> i & 1u)
-                    f[i] = nbdef ? (C)b.fdef[i * b.ndef + nk]
-                                 : P::Load(src, i * b.popstride + nnode +
-                                                    UpOffset<L>(b, i), i, pc);
-                drho += f[i];
-            }
-            const float rm1 = ((float)(op.rho_given - 1.0) - drho) / (1.0f + drho);
-#pragma unroll
-            for (int i = 0; i < Q - 1; i++) f[i] += (f[i] + pc.wf[i]) * rm1;
-        } else {
-            double rho = 0.0;
-#pragma unroll
-            for (int i = 0; i < Q; i++) {
-                if (op.in_mask >> i & 1u)
-                    f[i] = nbdef ? b.fdef[i * b.ndef + nk]
-                                 : P::Load(src, i * b.popstride + nnode +
-                                                    UpOffset<L>(b, i), i, pc);
-                rho = rho + f[i];
-            }
-            const double ratio = op.rho_given / rho;
-#pragma unroll
-            for (int i = 0; i < Q - 1; i++) f[i] = f[i] * ratio;
-        }
-    }
+    DeferredApply<D, T>(b, pc, src, b.ops[sg.op], x, y, z, f);
 #pragma unroll
     for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = (double)f[i];
+}
+
+// The whole deferred programme of a node in one thread, where no deferred
+// node reads another's value (the usual case: an outlet reads the interior
+// next to it): streaming (non-pulled populations keep the stored value),
+// every boundary operation of its region in definition order, the store
+// for the next step and observations, moments, collision.
+template <int D, typename T>
+__global__ void DeferredFusedKernel(BlockDev b, PhysConst pc,
+                                    const T* __restrict__ src,
+                                    T* __restrict__ dst) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int Q = L::Q;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= b.ndef) return;
+    int r, x, y, z;
+    long long k;
+    if (!DeferredNode(b, t, r, x, y, z, k)) return;
+    const RegionInfo& R = b.regions[r];
+    const long long node = NodeIndex<D>(b, x, y, z);
+    C f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; i++)
+        f[i] = (R.pull >> i & 1u)
+                   ? P::Load(src, i * b.popstride + node + UpOffset<L>(b, i),
+                             i, pc)
+                   : (C)b.fdef[i * b.ndef + k];
+    for (const int* o = b.dops_flat + b.dops_first[r]; *o >= 0; o++)
+        DeferredApply<D, T>(b, pc, src, b.ops[*o], x, y, z, f);
+#pragma unroll
+    for (int i = 0; i < Q; i++) b.fdef[i * b.ndef + k] = (double)f[i];
+    MomentsCollideT<L, T>(f, pc, R.fluidlike != 0);
+    Rng rng = SeedRng(pc.seed, node);
+#pragma unroll
+    for (int i = 0; i < Q; i++)
+        P::Store(dst, i * b.popstride + node, i, f[i], pc, rng);
 }
 
 // Deferred nodes, part 3: moments and collision (or observation).
@@ -1560,6 +1415,27 @@ __global__ void __launch_bounds__(128)
         P::Store(g, i * b.popstride + node, i, f[i], pc, rng);
 }
 
+// Every element of a population array, halo layers and row padding
+// included, set to the storage form's encoding of f = 0.  The reference's
+// dats start at zero and a halo cell that no transfer writes keeps f = 0
+// (a stale value a boundary node can pull); the shifted forms store
+// h = f - w, so their zero is h = -w (FP16: -kHalfScale), not 0.
+template <typename T>
+__global__ void FillZeroFKernel(T* __restrict__ p, long long popstride,
+                                int Q, PhysConst pc) {
+    const long long total = popstride * Q;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e / popstride);
+        if constexpr (std::is_same<T, __half>::value)
+            p[e] = __float2half(-kHalfScale);
+        else if constexpr (std::is_same<T, float>::value)
+            p[e] = -pc.wf[i];
+        else
+            p[e] = 0.0;
+    }
+}
+
 // Observation straight from f^0 stored by InitKernel (before any step).
 template <int D, typename T, int MODE>
 __global__ void DirectObserveKernel(BlockDev b, PhysConst pc,
@@ -1602,39 +1478,117 @@ __global__ void DirectObserveKernel(BlockDev b, PhysConst pc,
     if (D == 3) out3[dn] = u[2];
 }
 
-struct HaloDev {
+// All halo copies of a step in one launch.  Copies run in definition order
+// in the reference; here the cells that cannot depend on that order (source
+// not written earlier in the step, destination written by this copy alone)
+// run in parallel, a fixed range of one copy per CTA, and the last CTA to
+// finish (an atomic ticket, no waiting) runs the other cells level by level
+// (each after the cells it reads from or overwrites), with a CTA barrier
+// between levels.
+struct HaloBlockDev {          // what a copy needs of a block
+    long long pitch, plane, popstride;
+    int xoff;
+    void* pop[2];
+};
+
+struct HaloCopyDev {
     int iter[3];
     int fbase[3];
     int tbase[3];
     uint32_t pops;
-    const uint8_t* prev;   // nullptr: every source cell is current
+    int from, to;              // block indices
+    long long cells;
+    const uint8_t* prev;       // per cell: read the previous array (or null)
+    const uint8_t* ordered;    // per cell: left to the ordered phase
 };
 
-// One connection's halo copy (Field::TransferHalos / ops_halo_transfer):
-// the face layer of the source block into the destination block's halo,
-// only the populations that point into the destination.
-template <int D, typename T>
-__global__ void HaloKernel(HaloDev h, BlockDev fb, BlockDev tb,
-                           const T* __restrict__ cur_from,
-                           const T* __restrict__ prev_from,
-                           T* __restrict__ cur_to) {
+constexpr int kHaloCellsPerCta = 1024;
+
+struct HaloFusedDev {
+    const HaloCopyDev* copies;
+    const HaloBlockDev* blocks;
+    const int2* ctas;          // per CTA: (copy, first cell)
+    const int2* olist;         // ordered cells (copy, cell) by level
+    const int* olevel;         // first entry of each level, nlevels + 1
+    int nlevels;
+    unsigned* ticket;          // CTAs done with the parallel phase
+};
+
+template <int D>
+__device__ __forceinline__ long long HaloNodeIndex(const HaloBlockDev& b,
+                                                  int x, int y, int z) {
+    return (long long)(D == 3 ? z + 1 : 0) * b.plane +
+           (long long)(y + 1) * b.pitch + (long long)(x + b.xoff);
+}
+
+// A load that bypasses L1: in the ordered phase a source cell may have
+// been written by another SM in this launch.
+template <typename T>
+__device__ __forceinline__ T LoadL2(const T* p) {
+    if constexpr (std::is_same<T, __half>::value)
+        return __ushort_as_half(
+            __ldcg(reinterpret_cast<const unsigned short*>(p)));
+    else
+        return __ldcg(p);
+}
+
+template <int D, typename T, bool ORDERED>
+__device__ __forceinline__ void HaloCell(const HaloFusedDev& h,
+                                         const HaloCopyDev& c, long long t,
+                                         int cur) {
     using L = Lattice<D>;
     constexpr int Q = L::Q;
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long cells = (long long)h.iter[0] * h.iter[1] * h.iter[2];
-    if (t >= cells) return;
-    const int i = (int)(t % h.iter[0]);
-    const int j = (int)((t / h.iter[0]) % h.iter[1]);
-    const int k = (int)(t / ((long long)h.iter[0] * h.iter[1]));
-    const long long s = NodeIndex<D>(fb, h.fbase[0] + i, h.fbase[1] + j,
-                                     h.fbase[2] + k);
-    const long long d = NodeIndex<D>(tb, h.tbase[0] + i, h.tbase[1] + j,
-                                     h.tbase[2] + k);
-    const T* from = (h.prev != nullptr && h.prev[t]) ? prev_from : cur_from;
+    const HaloBlockDev& fb = h.blocks[c.from];
+    const HaloBlockDev& tb = h.blocks[c.to];
+    const int i = (int)(t % c.iter[0]);
+    const int j = (int)((t / c.iter[0]) % c.iter[1]);
+    const int k = (int)(t / ((long long)c.iter[0] * c.iter[1]));
+    const long long s = HaloNodeIndex<D>(fb, c.fbase[0] + i, c.fbase[1] + j,
+                                         c.fbase[2] + k);
+    const long long d = HaloNodeIndex<D>(tb, c.tbase[0] + i, c.tbase[1] + j,
+                                         c.tbase[2] + k);
+    const int sa = (c.prev != nullptr && c.prev[t]) ? 1 - cur : cur;
+    const T* from = static_cast<const T*>(fb.pop[sa]);
+    T* to = static_cast<T*>(tb.pop[cur]);
 #pragma unroll
-    for (int q = 0; q < Q; q++)
-        if (h.pops >> q & 1u)
-            cur_to[q * tb.popstride + d] = from[q * fb.popstride + s];
+    for (int q = 0; q < Q; q++) {
+        if (!(c.pops >> q & 1u)) continue;
+        const T* src = from + q * fb.popstride + s;
+        to[q * tb.popstride + d] = ORDERED ? LoadL2(src) : *src;
+    }
+}
+
+template <int D, typename T>
+__global__ void __launch_bounds__(256)
+    HaloFusedKernel(HaloFusedDev h, int cur) {
+    // parallel phase: kHaloCellsPerCta cells of one copy
+    {
+        const int2 a = h.ctas[blockIdx.x];
+        const HaloCopyDev& c = h.copies[a.x];
+        const long long end =
+            min((long long)a.y + kHaloCellsPerCta, c.cells);
+        for (long long t = a.y + threadIdx.x; t < end; t += blockDim.x)
+            if (!c.ordered[t]) HaloCell<D, T, false>(h, c, t, cur);
+    }
+    // the last CTA to get here runs the ordered phase
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(h.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int lv = 0; lv < h.nlevels; lv++) {
+        for (int m = h.olevel[lv] + threadIdx.x; m < h.olevel[lv + 1];
+             m += blockDim.x) {
+            const int2 e = h.olist[m];
+            HaloCell<D, T, true>(h, h.copies[e.x], e.y, cur);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *h.ticket = 0u;   // for the next launch
 }
 
 // Residual sums of one macroscopic variable over one block, per CTA:

@@ -16,10 +16,14 @@ struct Launch {
                             const BlockDev& b, const PhysConst& pc,
                             const T* src, T* dst, double* o0, double* o1,
                             double* o2, double* o3);
-    // the two parts of a pipelined step (b.split && b.pipe): 1 = the
-    // interior tasks (read no halo layer), 2 = shell rows and row edges
+    // the two parts of a split step (b.split): 1 = the x faces and the
+    // interior rows (no node of theirs reads a halo layer beyond a y or z
+    // face), 2 = the shell rows
     static cudaError_t StepPart(int part, cudaStream_t s, const BlockDev& b,
                                 const PhysConst& pc, const T* src, T* dst);
+    static cudaError_t DeferredFused(unsigned grid, cudaStream_t s,
+                                     const BlockDev& b, const PhysConst& pc,
+                                     const T* src, T* dst);
     static cudaError_t DeferredStream(unsigned grid, cudaStream_t s,
                                       const BlockDev& b, const PhysConst& pc,
                                       const T* src);
@@ -31,6 +35,9 @@ struct Launch {
                                       const BlockDev& b, const PhysConst& pc,
                                       T* dst, double* o0, double* o1,
                                       double* o2, double* o3);
+    // a population array (Q x popstride elements) set to f = 0
+    static cudaError_t FillZero(cudaStream_t s, T* p, long long popstride,
+                                int Q, const PhysConst& pc);
     static cudaError_t Init(dim3 grid, cudaStream_t s, const BlockDev& b,
                             const PhysConst& pc, const double* rho,
                             const double* u, const double* v, const double* w,
@@ -39,9 +46,9 @@ struct Launch {
                                      const BlockDev& b, const PhysConst& pc,
                                      const T* fdirect, double* o0, double* o1,
                                      double* o2, double* o3);
-    static cudaError_t Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
-                            const BlockDev& fb, const BlockDev& tb,
-                            const T* cur_from, const T* prev_from, T* cur_to);
+    // every halo copy of a step in one launch (pop[cur] is current)
+    static cudaError_t HaloFused(cudaStream_t s, const HaloFusedDev& h,
+                                 int cur, unsigned ctas);
     // face exchange of a decomposed block: export (block -> buf) or import
     static cudaError_t Face(bool exp, unsigned grid, cudaStream_t s,
                             const BlockDev& b, const FaceDev& fd, T* f,

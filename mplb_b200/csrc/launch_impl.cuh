@@ -2,8 +2,6 @@
 // translation units that instantiate them).
 #pragma once
 
-#include <algorithm>
-
 #include "launch.h"
 #include "swap.cuh"
 
@@ -25,75 +23,34 @@ long long SplitBlocks(const BlockDev& b) {
     return blocks > 0x7fffffffLL ? 0 : blocks;
 }
 
-// Task geometry of PipeStepKernel for block b.
-template <int D, typename T>
-PipeGeom PipeGeometry(const BlockDev& b) {
-    constexpr int S = SectorNodes<T>();
-    constexpr int G = SplitGroup<T>();
-    PipeGeom g;
-    g.xs = S;
-    g.xe = b.n[0] - S;
-    g.tpr = (g.xe - g.xs + 32 * G - 1) / (32 * G);
-    g.ny = b.n[1] - 2;
-    g.rows = (long long)g.ny * (D == 3 ? b.n[2] - 2 : 1);
-    g.tasks = (long long)g.tpr * g.rows;
-    return g;
-}
-
-// Persistent grid of PipeStepKernel: the CTAs that fit on the device at
-// once (looked up once per instantiation).
-template <int D, typename T, bool O32>
-unsigned PipeCtas() {
-    static const unsigned ctas = [] {
-        int dev = 0, sms = 0, per = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
-                                   dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per, PipeStepKernel<D, T, O32>, kStepThreads, 0) !=
-                cudaSuccess)
-            return 0u;
-        return (unsigned)(sms * (per > 0 ? per : 1));
-    }();
-    return ctas;
-}
-
-// parts: bit 0 the edge launch (shell rows and row edges), bit 1 the
-// pipelined interior; the edge launch goes first when both are asked for.
-template <int D, typename T, bool O32>
-cudaError_t LaunchPipe(cudaStream_t s, const BlockDev& b, const PhysConst& pc,
-                       const T* src, T* dst, int parts) {
-    constexpr int S = SectorNodes<T>();
-    const PipeGeom g = PipeGeometry<D, T>(b);
+// Shell-row CTAs of SplitStepKernel for block b (its first CTAs).
+template <int D>
+long long SplitShellBlocks(const BlockDev& b) {
     const long long nbx = (b.n[0] + kStepThreads - 1) / kStepThreads;
+    const long long ny = b.n[1] - 2;
     const long long nz = D == 3 ? b.n[2] : 1;
-    const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * (long long)g.ny : 0));
-    const long long edge =
-        nsr + (g.rows * 2 * S + kStepThreads - 1) / kStepThreads;
-    const unsigned ctas = PipeCtas<D, T, O32>();
-    if (edge > 0x7fffffffLL || ctas == 0) return cudaErrorInvalidConfiguration;
-    if (parts & 1) {
-        EdgeStepKernel<D, T, O32><<<(unsigned)edge, kStepThreads, 0, s>>>(
-            b, pc, src, dst, g);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    if ((parts & 2) && g.tasks > 0) {
-        const unsigned grid = (unsigned)std::min<long long>(ctas, g.tasks);
-        PipeStepKernel<D, T, O32><<<grid, kStepThreads, 0, s>>>(b, pc, src,
-                                                                dst, g);
-    }
-    return cudaGetLastError();
+    return nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
 }
 
 template <int D, typename T>
 cudaError_t Launch<D, T>::StepPart(int part, cudaStream_t s, const BlockDev& b,
                                    const PhysConst& pc, const T* src, T* dst) {
-    if (!(b.split && b.pipe) || (part != 1 && part != 2))
-        return cudaErrorInvalidValue;
-    const int parts = part == 1 ? 2 : 1;
-    return b.off32 ? LaunchPipe<D, T, true>(s, b, pc, src, dst, parts)
-                   : LaunchPipe<D, T, false>(s, b, pc, src, dst, parts);
+    if (!b.split || (part != 1 && part != 2)) return cudaErrorInvalidValue;
+    const long long blocks = SplitBlocks<D, T>(b);
+    if (blocks == 0) return cudaErrorInvalidConfiguration;
+    const long long shell = SplitShellBlocks<D>(b);
+    // part 1: x faces and interior rows (CTAs shell .. blocks - 1);
+    // part 2: the shell rows (CTAs 0 .. shell - 1)
+    const unsigned grid = (unsigned)(part == 1 ? blocks - shell : shell);
+    const unsigned blk0 = part == 1 ? (unsigned)shell : 0u;
+    if (grid == 0) return cudaSuccess;
+    if (b.off32)
+        SplitStepKernel<D, T, true><<<grid, kStepThreads, 0, s>>>(b, pc, src,
+                                                                  dst, blk0);
+    else
+        SplitStepKernel<D, T, false><<<grid, kStepThreads, 0, s>>>(b, pc, src,
+                                                                   dst, blk0);
+    return cudaGetLastError();
 }
 
 template <int D, typename T>
@@ -101,19 +58,15 @@ cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const BlockDev& b, const PhysConst& pc,
                                const T* src, T* dst, double* o0, double* o1,
                                double* o2, double* o3) {
-    if (mode == kModeStep && b.split && b.pipe) {
-        return b.off32 ? LaunchPipe<D, T, true>(s, b, pc, src, dst, 3)
-                       : LaunchPipe<D, T, false>(s, b, pc, src, dst, 3);
-    }
     if (mode == kModeStep && b.split) {
         const long long blocks = SplitBlocks<D, T>(b);
         if (blocks == 0) return cudaErrorInvalidConfiguration;
         if (b.off32)
             SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(
-                b, pc, src, dst);
+                b, pc, src, dst, 0u);
         else
             SplitStepKernel<D, T, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(
-                b, pc, src, dst);
+                b, pc, src, dst, 0u);
     } else if (mode == kModeStep && b.off32)
         StepKernel<D, T, kModeStep, true><<<grid, kStepThreads, 0, s>>>(
             b, pc, src, dst, o0, o1, o2, o3);
@@ -126,6 +79,14 @@ cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
     else
         StepKernel<D, T, kModeF><<<grid, kStepThreads, 0, s>>>(
             b, pc, src, dst, o0, o1, o2, o3);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::DeferredFused(unsigned grid, cudaStream_t s,
+                                        const BlockDev& b, const PhysConst& pc,
+                                        const T* src, T* dst) {
+    DeferredFusedKernel<D, T><<<grid, kStepThreads, 0, s>>>(b, pc, src, dst);
     return cudaGetLastError();
 }
 
@@ -162,6 +123,13 @@ cudaError_t Launch<D, T>::DeferredFinish(int mode, unsigned grid,
     else
         DeferredFinishKernel<D, T, kModeF><<<grid, kStepThreads, 0, s>>>(
             b, pc, dst, o0, o1, o2, o3);
+    return cudaGetLastError();
+}
+
+template <int D, typename T>
+cudaError_t Launch<D, T>::FillZero(cudaStream_t s, T* p, long long popstride,
+                                   int Q, const PhysConst& pc) {
+    FillZeroFKernel<T><<<1024, 256, 0, s>>>(p, popstride, Q, pc);
     return cudaGetLastError();
 }
 
@@ -203,12 +171,9 @@ cudaError_t Launch<D, T>::Face(bool exp, unsigned grid, cudaStream_t s,
 }
 
 template <int D, typename T>
-cudaError_t Launch<D, T>::Halo(unsigned grid, cudaStream_t s, const HaloDev& h,
-                               const BlockDev& fb, const BlockDev& tb,
-                               const T* cur_from, const T* prev_from,
-                               T* cur_to) {
-    HaloKernel<D, T><<<grid, 256, 0, s>>>(h, fb, tb, cur_from, prev_from,
-                                          cur_to);
+cudaError_t Launch<D, T>::HaloFused(cudaStream_t s, const HaloFusedDev& h,
+                                    int cur, unsigned ctas) {
+    HaloFusedKernel<D, T><<<ctas, 256, 0, s>>>(h, cur);
     return cudaGetLastError();
 }
 

@@ -35,6 +35,7 @@ struct DevBlock {
     RegionOp* ops = nullptr;
     double* stale = nullptr;
     double* fdef = nullptr;
+    int* dops_flat = nullptr;
     int4* dregions = nullptr;
     double* macro[4] = {nullptr, nullptr, nullptr, nullptr};
     double* macro_old[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -46,10 +47,9 @@ struct DevBlock {
     std::vector<DOp> dops;
 };
 
-struct DevHalo {
-    HaloDev h{};
+struct DevHalo {          // device arrays of one copy of the halo plan
     uint8_t* prev = nullptr;
-    int from = 0, to = 0;
+    uint8_t* ordered = nullptr;
 };
 
 }  // namespace
@@ -59,6 +59,8 @@ struct mplbgpu_ctx {
     PhysConst pc{};
     std::vector<DevBlock> blocks;
     std::vector<DevHalo> halos;
+    HaloFusedDev hfd{};     // the fused transfer (copies, blocks, ticket)
+    unsigned halo_ctas = 0;
     int cur = 0;            // pop[cur] holds the latest g
     bool initial = true;    // pop[1 - cur] holds f^0 itself
     // swap scheme, contents of pop[0]: 0 f itself (initial or uploaded),
@@ -78,7 +80,7 @@ struct mplbgpu_ctx {
     unsigned long long* bad = nullptr;
     double* scratch = nullptr;  // dense f staging
     size_t scratch_elems = 0;
-    std::vector<double*> bc_field;  // per boundary: per-node wall velocity
+    std::vector<RegionOp*> bc_field;  // per boundary: per-node operations
     std::string err;
 };
 
@@ -151,6 +153,7 @@ void FreeAll(mplbgpu_ctx* c) {
         cudaFree(b.ops);
         cudaFree(b.stale);
         cudaFree(b.fdef);
+        cudaFree(b.dops_flat);
         cudaFree(b.dregions);
         for (int m = 0; m < 4; m++) {
             cudaFree(b.macro[m]);
@@ -158,14 +161,33 @@ void FreeAll(mplbgpu_ctx* c) {
         }
         for (auto& d : b.dops) cudaFree(d.segs);
     }
-    for (DevHalo& h : c->halos) cudaFree(h.prev);
-    for (double* p : c->bc_field) cudaFree(p);
+    for (DevHalo& h : c->halos) {
+        cudaFree(h.prev);
+        cudaFree(h.ordered);
+    }
+    cudaFree(const_cast<HaloCopyDev*>(c->hfd.copies));
+    cudaFree(const_cast<HaloBlockDev*>(c->hfd.blocks));
+    cudaFree(const_cast<int2*>(c->hfd.ctas));
+    cudaFree(const_cast<int2*>(c->hfd.olist));
+    cudaFree(const_cast<int*>(c->hfd.olevel));
+    cudaFree(c->hfd.ticket);
+    for (RegionOp* p : c->bc_field) cudaFree(p);
     cudaFree(c->part);
     cudaFree(c->bad);
     cudaFree(c->scratch);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+// A population array of the context's storage form set to f = 0.
+cudaError_t FillZeroF(mplbgpu_ctx* c, void* p, long long popstride) {
+    const int Q = c->plan.Q;
+    if (c->plan.precision == MPLBGPU_FP32_SHIFTED)
+        return Launch<3, float>::FillZero(c->stream, static_cast<float*>(p),
+                                          popstride, Q, c->pc);
+    return Launch<3, __half>::FillZero(c->stream, static_cast<__half*>(p),
+                                       popstride, Q, c->pc);
 }
 
 int EnsureScratch(mplbgpu_ctx* ctx, size_t elems) {
@@ -178,20 +200,13 @@ int EnsureScratch(mplbgpu_ctx* ctx, size_t elems) {
     return MPLBGPU_OK;
 }
 
+// Every halo copy of the step (Field::TransferHalos in CreateHalos order)
+// in one launch.
 template <int D, typename T>
 int RunHalosT(mplbgpu_ctx* ctx) {
-    for (DevHalo& h : ctx->halos) {
-        DevBlock& fb = ctx->blocks[h.from];
-        DevBlock& tb = ctx->blocks[h.to];
-        const long long cells =
-            (long long)h.h.iter[0] * h.h.iter[1] * h.h.iter[2];
-        const unsigned grid = (unsigned)((cells + 255) / 256);
-        CK_LAUNCH_E(Launch<D, T>::Halo(
-            grid, ctx->stream, h.h, fb.dev, tb.dev,
-            static_cast<const T*>(fb.pop[ctx->cur]),
-            static_cast<const T*>(fb.pop[1 - ctx->cur]),
-            static_cast<T*>(tb.pop[ctx->cur])));
-    }
+    if (!ctx->halos.empty())
+        CK_LAUNCH_E(Launch<D, T>::HaloFused(ctx->stream, ctx->hfd, ctx->cur,
+                                            ctx->halo_ctas));
     ctx->halos_pending = false;
     return MPLBGPU_OK;
 }
@@ -229,8 +244,11 @@ int StepOnce(mplbgpu_ctx* ctx) {
         CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D), ctx->stream,
                                        b.dev, ctx->pc, s, d, nullptr, nullptr,
                                        nullptr, nullptr));
-        if (b.dev.split && b.dev.pipe) ctx->launches++;   // two kernels
-        if (B.ndeferred > 0) {
+        if (B.ndeferred > 0 && b.dev.deferred_fused) {
+            const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
+            CK_LAUNCH_E(Launch<D, T>::DeferredFused(g, ctx->stream, b.dev,
+                                                    ctx->pc, s, d));
+        } else if (B.ndeferred > 0) {
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
             CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, ctx->stream, b.dev,
                                                      ctx->pc, s));
@@ -251,15 +269,16 @@ int StepOnce(mplbgpu_ctx* ctx) {
     return RunHalosT<D, T>(ctx);
 }
 
-// First part of a step: the halo-independent interior of every block with
-// the pipelined layout (other blocks do all their work in the second part).
+// First part of a step: the x faces and interior rows of every block with
+// the split layout, which read no halo layer beyond a y or z face (other
+// blocks do all their work in the second part).
 template <int D, typename T>
 int StepBeginT(mplbgpu_ctx* ctx) {
     const int src = ctx->cur, dst = 1 - ctx->cur;
     ctx->pc.seed = (uint32_t)(++ctx->step_count);
     for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
         DevBlock& b = ctx->blocks[bi];
-        if (!(b.dev.split && b.dev.pipe)) continue;
+        if (!b.dev.split) continue;
         CK_LAUNCH_E(Launch<D, T>::StepPart(
             1, ctx->stream, b.dev, ctx->pc, static_cast<const T*>(b.pop[src]),
             static_cast<T*>(b.pop[dst])));
@@ -268,8 +287,8 @@ int StepBeginT(mplbgpu_ctx* ctx) {
     return MPLBGPU_OK;
 }
 
-// The rest of a begun step: shell rows and row edges of pipelined blocks,
-// whole other blocks, deferred nodes, then the block-to-block halos.
+// The rest of a begun step: shell rows of split blocks, whole other
+// blocks, deferred nodes, then the block-to-block halos.
 template <int D, typename T>
 int StepFinishT(mplbgpu_ctx* ctx) {
     const int src = ctx->cur, dst = 1 - ctx->cur;
@@ -278,7 +297,7 @@ int StepFinishT(mplbgpu_ctx* ctx) {
         const BlockPlan& B = ctx->plan.blocks[bi];
         const T* s = static_cast<const T*>(b.pop[src]);
         T* d = static_cast<T*>(b.pop[dst]);
-        if (b.dev.split && b.dev.pipe) {
+        if (b.dev.split) {
             CK_LAUNCH_E(Launch<D, T>::StepPart(2, ctx->stream, b.dev, ctx->pc,
                                                s, d));
         } else {
@@ -287,7 +306,11 @@ int StepFinishT(mplbgpu_ctx* ctx) {
                                            nullptr, nullptr, nullptr,
                                            nullptr));
         }
-        if (B.ndeferred > 0) {
+        if (B.ndeferred > 0 && b.dev.deferred_fused) {
+            const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
+            CK_LAUNCH_E(Launch<D, T>::DeferredFused(g, ctx->stream, b.dev,
+                                                    ctx->pc, s, d));
+        } else if (B.ndeferred > 0) {
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
             CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, ctx->stream, b.dev,
                                                      ctx->pc, s));
@@ -511,9 +534,13 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
         for (int k = 0; k < (P.swap ? 1 : 2); k++) {
             if ((e = cudaMalloc(&b.pop[k], popbytes)) != cudaSuccess)
                 return fail_cuda(e, "cudaMalloc(populations)");
-            if ((e = cudaMemsetAsync(b.pop[k], 0, popbytes, c->stream)) !=
-                cudaSuccess)
-                return fail_cuda(e, "cudaMemset(populations)");
+            // f = 0 everywhere (the reference's zero-filled dats): zero
+            // bytes in FP64, h = -w in the shifted forms
+            if (P.precision == MPLBGPU_FP64)
+                e = cudaMemsetAsync(b.pop[k], 0, popbytes, c->stream);
+            else
+                e = FillZeroF(c.get(), b.pop[k], B.popstride);
+            if (e != cudaSuccess) return fail_cuda(e, "population fill");
         }
         if ((e = cudaMalloc(&b.regions, sizeof(B.region))) != cudaSuccess ||
             (e = cudaMemcpy(b.regions, B.region, sizeof(B.region),
@@ -594,6 +621,15 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
         d.ndef = B.ndeferred;
         d.dregions = b.dregions;
         d.ndregions = (int)dreg.size();
+        d.deferred_fused = B.deferred_fused ? 1 : 0;
+        for (int r = 0; r < kNumRegions; r++) d.dops_first[r] = B.dops_first[r];
+        if ((e = cudaMalloc(&b.dops_flat, B.dops_flat.size() * sizeof(int))) !=
+                cudaSuccess ||
+            (e = cudaMemcpy(b.dops_flat, B.dops_flat.data(),
+                            B.dops_flat.size() * sizeof(int),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return fail_cuda(e, "deferred programme");
+        d.dops_flat = b.dops_flat;
         for (int i = 0; i < kMaxQ; i++) {
             d.pop_off[i] = i < Q ? (long long)i * B.popstride : 0;
             d.pull_off[i] = 0;
@@ -644,36 +680,104 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
                       ? 1
                       : 0;
         d.center_fluid = B.region[center].fluidlike ? 1 : 0;
-        // the split step as edge + pipelined interior launches where a row
-        // holds more than two 32-byte sectors of nodes;
-        // MPLB_B200_STEP_KERNEL=split keeps the one-launch split kernel
-        // (both give the same FP64/FP32 bits; tests compare them)
-        const char* sk = std::getenv("MPLB_B200_STEP_KERNEL");
-        const int sector = 32 / P.elem_bytes;
-        d.pipe = d.split && B.n[0] >= 2 * sector + 1 &&
-                         !(sk && std::strcmp(sk, "split") == 0)
-                     ? 1
-                     : 0;
     }
-    for (const HaloCopy& h : P.halos) {
-        DevHalo dh;
-        dh.from = h.from;
-        dh.to = h.to;
-        for (int a = 0; a < 3; a++) {
-            dh.h.iter[a] = h.iter[a];
-            dh.h.fbase[a] = h.fbase[a];
-            dh.h.tbase[a] = h.tbase[a];
-        }
-        dh.h.pops = h.pops;
-        dh.h.prev = nullptr;
-        if (h.any_prev) {
-            if ((e = cudaMalloc(&dh.prev, h.prev.size())) != cudaSuccess ||
-                (e = cudaMemcpy(dh.prev, h.prev.data(), h.prev.size(),
+    if (!P.halos.empty()) {
+        std::vector<HaloCopyDev> copies;
+        std::vector<int2> ctas;
+        std::vector<std::pair<int, int2>> ordered;   // (level, (copy, cell))
+        int nlevels = 0;
+        for (size_t t = 0; t < P.halos.size(); t++) {
+            const HaloCopy& h = P.halos[t];
+            DevHalo dh;
+            HaloCopyDev cd{};
+            for (int a = 0; a < 3; a++) {
+                cd.iter[a] = h.iter[a];
+                cd.fbase[a] = h.fbase[a];
+                cd.tbase[a] = h.tbase[a];
+            }
+            cd.pops = h.pops;
+            cd.from = h.from;
+            cd.to = h.to;
+            cd.cells = (long long)h.iter[0] * h.iter[1] * h.iter[2];
+            for (long long t0 = 0; t0 < cd.cells; t0 += kHaloCellsPerCta)
+                ctas.push_back(make_int2((int)t, (int)t0));
+            for (size_t m = 0; m < h.ocell.size(); m++) {
+                ordered.push_back({h.olevel[m], make_int2((int)t, h.ocell[m])});
+                nlevels = std::max(nlevels, h.olevel[m]);
+            }
+            if (h.any_prev) {
+                if ((e = cudaMalloc(&dh.prev, h.prev.size())) != cudaSuccess ||
+                    (e = cudaMemcpy(dh.prev, h.prev.data(), h.prev.size(),
+                                    cudaMemcpyHostToDevice)) != cudaSuccess)
+                    return fail_cuda(e, "halo masks");
+            }
+            if ((e = cudaMalloc(&dh.ordered, h.ordered.size())) != cudaSuccess ||
+                (e = cudaMemcpy(dh.ordered, h.ordered.data(), h.ordered.size(),
                                 cudaMemcpyHostToDevice)) != cudaSuccess)
-                return fail_cuda(e, "halo masks");
-            dh.h.prev = dh.prev;
+                return fail_cuda(e, "halo phases");
+            cd.prev = dh.prev;
+            cd.ordered = dh.ordered;
+            copies.push_back(cd);
+            c->halos.push_back(dh);
         }
-        c->halos.push_back(dh);
+        // ordered cells by level (levels 1..nlevels); stable within a level
+        std::stable_sort(ordered.begin(), ordered.end(),
+                         [](const std::pair<int, int2>& a,
+                            const std::pair<int, int2>& b) {
+                             return a.first < b.first;
+                         });
+        std::vector<int2> olist;
+        std::vector<int> olevel(nlevels + 1, 0);
+        for (size_t m = 0; m < ordered.size(); m++) olist.push_back(ordered[m].second);
+        for (int lv = 1, m = 0; lv <= nlevels; lv++) {
+            olevel[lv - 1] = m;
+            while (m < (int)ordered.size() && ordered[m].first == lv) m++;
+            olevel[lv] = m;
+        }
+        std::vector<HaloBlockDev> hb(c->blocks.size());
+        for (size_t bi = 0; bi < c->blocks.size(); bi++) {
+            const BlockPlan& B = P.blocks[bi];
+            hb[bi].pitch = B.pitch;
+            hb[bi].plane = B.plane;
+            hb[bi].popstride = B.popstride;
+            hb[bi].xoff = B.xoff;
+            hb[bi].pop[0] = c->blocks[bi].pop[0];
+            hb[bi].pop[1] = c->blocks[bi].pop[1];
+        }
+        auto upload = [&](const void* src, size_t bytes,
+                          void** dst) -> cudaError_t {
+            *dst = nullptr;
+            if (bytes == 0) return cudaSuccess;
+            cudaError_t r = cudaMalloc(dst, bytes);
+            if (r != cudaSuccess) return r;
+            return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        };
+        void* p = nullptr;
+        if ((e = upload(copies.data(), copies.size() * sizeof(HaloCopyDev),
+                        &p)) != cudaSuccess)
+            return fail_cuda(e, "halo copies");
+        c->hfd.copies = static_cast<HaloCopyDev*>(p);
+        if ((e = upload(hb.data(), hb.size() * sizeof(HaloBlockDev), &p)) !=
+            cudaSuccess)
+            return fail_cuda(e, "halo blocks");
+        c->hfd.blocks = static_cast<HaloBlockDev*>(p);
+        if ((e = upload(ctas.data(), ctas.size() * sizeof(int2), &p)) !=
+            cudaSuccess)
+            return fail_cuda(e, "halo work");
+        c->hfd.ctas = static_cast<int2*>(p);
+        if ((e = upload(olist.data(), olist.size() * sizeof(int2), &p)) !=
+            cudaSuccess)
+            return fail_cuda(e, "halo order");
+        c->hfd.olist = static_cast<int2*>(p);
+        if ((e = upload(olevel.data(), olevel.size() * sizeof(int), &p)) !=
+            cudaSuccess)
+            return fail_cuda(e, "halo levels");
+        c->hfd.olevel = static_cast<int*>(p);
+        c->hfd.nlevels = nlevels;
+        if ((e = cudaMalloc(&c->hfd.ticket, sizeof(unsigned))) != cudaSuccess ||
+            (e = cudaMemset(c->hfd.ticket, 0, sizeof(unsigned))) != cudaSuccess)
+            return fail_cuda(e, "halo ticket");
+        c->halo_ctas = (unsigned)ctas.size();
     }
     if ((e = cudaMalloc(&c->part, 2 * kRedBlocks * sizeof(double))) !=
             cudaSuccess ||
@@ -962,6 +1066,10 @@ mplbgpu_status mplbgpu_import_face(mplbgpu_ctx* ctx, int block, int surface,
     FaceDev fd;
     rc = FaceSetup(ctx, block, surface, false, &bi, &fd);
     if (rc != MPLBGPU_OK) return rc;
+    if (ctx->begun && fd.axis == 0)
+        return SetErr(ctx, MPLBGPU_ERR_STATE,
+                      "an x face cannot be imported while a step is begun "
+                      "(its first part reads the x halo layers)");
     return MPLB_DISPATCH(ctx, FaceCopy, ctx, bi, fd, false,
                          const_cast<void*>(buf));
 }
@@ -1034,36 +1142,14 @@ mplbgpu_status mplbgpu_set_boundary_velocity(mplbgpu_ctx* ctx, int boundary,
         return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
                       "per-node wall velocities are not available under the "
                       "swap scheme");
-    // the scheme of this boundary: any op made from it tells
     const int bi = ctx->plan.bc_block[boundary];
     BlockPlan& B = ctx->plan.blocks[bi];
     DevBlock& b = ctx->blocks[bi];
-    bool any = false;
-    for (const RegionOp& op : B.ops) {
-        if (op.bc != boundary) continue;
-        if (op.kind != kOpEqm && op.kind != kOpHbb)
-            return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
-                          "per-node velocities need an EQMDiffuseRefl or "
-                          "halfway bounce-back boundary");
-        any = true;
-    }
-    if (!any)
-        return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
-                      "the boundary has no boundary kernel (per-node "
-                      "velocities need EQMDiffuseRefl or halfway "
-                      "bounce-back)");
     const int* r = &ctx->plan.bc_range[6 * (size_t)boundary];
     const size_t cnt = (size_t)ext[0] * ext[1] * ext[2];
-    // no kernel of this context may read the op table while it changes
-    CK(cudaStreamSynchronize(ctx->stream));
-    if (ctx->bc_field.size() < ctx->plan.bc_block.size())
-        ctx->bc_field.resize(ctx->plan.bc_block.size(), nullptr);
-    double*& dev = ctx->bc_field[boundary];
     const bool clear = !u && !v && !w;
-    if (clear) {
-        CK(cudaFree(dev));
-        dev = nullptr;
-    } else {
+    std::vector<RegionOp> node_ops;
+    if (!clear) {
         std::vector<double> packed(3 * cnt, 0.0);
         const double* src[3] = {u, v, ctx->plan.dim == 3 ? w : nullptr};
         for (int c = 0; c < 3; c++)
@@ -1073,13 +1159,32 @@ mplbgpu_status mplbgpu_set_boundary_velocity(mplbgpu_ctx* ctx, int boundary,
             if (!std::isfinite(x))
                 return SetErr(ctx, MPLBGPU_ERR_INVALID,
                               "non-finite wall velocity");
-        if (!dev) CK(cudaMalloc(&dev, packed.size() * sizeof(double)));
-        CK(cudaMemcpy(dev, packed.data(), packed.size() * sizeof(double),
-                      cudaMemcpyHostToDevice));
+        std::string err;
+        rc = BoundaryNodeOps(ctx->plan, boundary, packed.data(), &node_ops,
+                             &err);
+        if (rc != MPLBGPU_OK) return SetErr(ctx, rc, err);
+    } else if (ctx->plan.bc_scheme[boundary] != MPLBGPU_BC_EQM_DIFFUSE_REFL &&
+               ctx->plan.bc_scheme[boundary] !=
+                   MPLBGPU_BC_HALFWAY_BOUNCE_BACK) {
+        return SetErr(ctx, MPLBGPU_ERR_UNSUPPORTED,
+                      "per-node velocities need an EQMDiffuseRefl or halfway "
+                      "bounce-back boundary");
+    }
+    // no kernel of this context may read the op tables while they change
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->bc_field.size() < ctx->plan.bc_block.size())
+        ctx->bc_field.resize(ctx->plan.bc_block.size(), nullptr);
+    RegionOp*& dev = ctx->bc_field[boundary];
+    CK(cudaFree(dev));
+    dev = nullptr;
+    if (!clear) {
+        const size_t bytes = node_ops.size() * sizeof(RegionOp);
+        CK(cudaMalloc(&dev, bytes));
+        CK(cudaMemcpy(dev, node_ops.data(), bytes, cudaMemcpyHostToDevice));
     }
     for (RegionOp& op : B.ops) {
         if (op.bc != boundary) continue;
-        op.field = dev;
+        op.node_ops = dev;
         for (int a = 0; a < 3; a++) {
             op.forg[a] = r[2 * a];
             op.fext[a] = ext[a];

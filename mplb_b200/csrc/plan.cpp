@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 
 #include "lattice.h"
 
@@ -731,8 +732,16 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                 B.ops.push_back(op);
             }
         }
-        // nodes whose post-boundary value an ExtrapolPressure1ST reads must
-        // be materialised too
+        // An ExtrapolPressure1ST reads its inner neighbour's post-boundary
+        // f: the deferred kernel takes it from the store when the
+        // neighbour is deferred, re-pulls it when the neighbour is pure,
+        // and re-evaluates it (pull, stale store, the neighbour's boundary
+        // operations defined before this one) when the neighbour is local.
+        // A local neighbour is materialised all the same when a population
+        // the extrapolation copies is none of those - neither pulled nor
+        // stale nor written by an earlier operation: the reference has the
+        // neighbour's value of the previous step there, which only the
+        // deferred store keeps.
         for (int r = 0; r < kNumRegions; r++) {
             const RegionInfo& R = B.region[r];
             if (R.cls != kDeferred) continue;
@@ -744,8 +753,17 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                 int rc[3];
                 for (int a = 0; a < 3; a++)
                     rc[a] = a < P.dim ? RegionCoord(q[a], B.n[a]) : 1;
-                RegionInfo& N = B.region[rc[0] + 3 * rc[1] + 9 * rc[2]];
-                if (N.cls == kLocal) N.cls = kDeferred;
+                const int nr = rc[0] + 3 * rc[1] + 9 * rc[2];
+                RegionInfo& N = B.region[nr];
+                if (N.cls != kLocal) continue;
+                uint32_t avail = N.pull | N.stale;
+                for (int ni : B.allops[nr]) {
+                    const RegionOp& nop = B.ops[ni];
+                    if (nop.bc >= op.bc) break;
+                    avail |= nop.out_mask;
+                    if (nop.kind == kOpEqm) avail |= nop.par_mask;
+                }
+                if (op.in_mask & ~avail) N.cls = kDeferred;
             }
         }
         for (int r = 0; r < kNumRegions; r++) {
@@ -762,6 +780,29 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
         }
         B.nstale = stale_nodes;
         B.ndeferred = deferred_nodes;
+        // the deferred programme in one pass: independent unless an
+        // extrapolation reads a deferred neighbour
+        B.deferred_fused = B.ndeferred > 0;
+        B.dops_flat.clear();
+        for (int r = 0; r < kNumRegions; r++) {
+            const RegionInfo& R = B.region[r];
+            B.dops_first[r] = (int)B.dops_flat.size();
+            if (R.cls != kDeferred) continue;
+            for (int oi : B.allops[r]) {
+                const RegionOp& op = B.ops[oi];
+                B.dops_flat.push_back(oi);
+                if (op.kind != kOpExtrapol || op.nb_axis < 0) continue;
+                int q[3] = {R.org[0], R.org[1], R.org[2]};
+                q[op.nb_axis] += op.nb_sign;
+                int rc[3];
+                for (int a = 0; a < 3; a++)
+                    rc[a] = a < P.dim ? RegionCoord(q[a], B.n[a]) : 1;
+                if (B.region[rc[0] + 3 * rc[1] + 9 * rc[2]].cls == kDeferred)
+                    B.deferred_fused = false;
+            }
+            B.dops_flat.push_back(-1);
+        }
+        if (B.dops_flat.empty()) B.dops_flat.push_back(-1);
         // deferred programme: every boundary, in definition order, on the
         // deferred regions it covers
         if (B.ndeferred > 0) {
@@ -786,6 +827,7 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                     else
                         op = MakeHbb(L, P.cs, B.n, R.org, bc.surface,
                                      bc.given);
+                    op.bc = k;
                     dop.segments.push_back({r, (int)B.ops.size()});
                     B.ops.push_back(op);
                 }
@@ -905,10 +947,109 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
         }
         if (!h.any_prev) h.prev.clear();
     }
+    // Phases of the fused transfer.  A cell must run in definition order
+    // when its destination is written by more than one copy, or when its
+    // source (a halo cell) is written by an earlier copy of the step; every
+    // other cell reads a value no copy of this step changes (a block node, a
+    // halo cell no copy writes, or one only a later copy writes, which
+    // `prev` sends to the previous array) and writes a cell no other copy
+    // writes, so the cells can run in any order.
+    {
+        // first writer (copy index) and number of writers per halo cell
+        std::map<std::pair<int, long long>, std::pair<int, int>> writers;
+        auto cell = [&](int blk, int x, int y, int z) {
+            const BlockPlan& B = P.blocks[blk];
+            const long long a0 = B.n[0] + 2, a1 = B.n[1] + 2;
+            return std::make_pair(
+                blk, ((long long)(z + 1) * a1 + (y + 1)) * a0 + (x + 1));
+        };
+        for (size_t t = 0; t < P.halos.size(); t++) {
+            const HaloCopy& h = P.halos[t];
+            for (int k = 0; k < h.iter[2]; k++)
+                for (int j = 0; j < h.iter[1]; j++)
+                    for (int i = 0; i < h.iter[0]; i++) {
+                        auto& w = writers[cell(h.to, h.tbase[0] + i,
+                                               h.tbase[1] + j,
+                                               h.tbase[2] + k)];
+                        if (w.second++ == 0) w.first = (int)t;
+                    }
+        }
+        for (size_t t = 0; t < P.halos.size(); t++) {
+            HaloCopy& h = P.halos[t];
+            const long long cells =
+                (long long)h.iter[0] * h.iter[1] * h.iter[2];
+            h.ordered.assign(cells, 0);
+            h.nordered = 0;
+            long long cidx = 0;
+            for (int k = 0; k < h.iter[2]; k++)
+                for (int j = 0; j < h.iter[1]; j++)
+                    for (int i = 0; i < h.iter[0]; i++, cidx++) {
+                        const auto& dw = writers[cell(h.to, h.tbase[0] + i,
+                                                      h.tbase[1] + j,
+                                                      h.tbase[2] + k)];
+                        bool ord = dw.second > 1;
+                        const auto sw = writers.find(cell(
+                            h.from, h.fbase[0] + i, h.fbase[1] + j,
+                            h.fbase[2] + k));
+                        if (sw != writers.end() && sw->second.first < (int)t)
+                            ord = true;
+                        if (ord) {
+                            h.ordered[cidx] = 1;
+                            h.nordered++;
+                        }
+                    }
+        }
+        // Levels of the ordered cells, copy by copy in definition order:
+        // a cell comes after the writer of its source, after the earlier
+        // writer of its destination and after every earlier reader of its
+        // destination (parallel-phase writes are level 0).
+        std::map<std::pair<int, long long>, int> wlevel;   // last write
+        std::map<std::pair<int, long long>, int> rlevel;   // reads since
+        for (size_t t = 0; t < P.halos.size(); t++) {
+            HaloCopy& h = P.halos[t];
+            h.ocell.clear();
+            h.olevel.clear();
+            long long cidx = 0;
+            std::vector<std::pair<std::pair<int, long long>, int>> writes;
+            for (int k = 0; k < h.iter[2]; k++)
+                for (int j = 0; j < h.iter[1]; j++)
+                    for (int i = 0; i < h.iter[0]; i++, cidx++) {
+                        const auto dc = cell(h.to, h.tbase[0] + i,
+                                             h.tbase[1] + j, h.tbase[2] + k);
+                        const auto sc = cell(h.from, h.fbase[0] + i,
+                                             h.fbase[1] + j, h.fbase[2] + k);
+                        if (!h.ordered[cidx]) {
+                            writes.push_back({dc, 0});
+                            continue;
+                        }
+                        int lv = 1;
+                        auto sw = wlevel.find(sc);
+                        if (sw != wlevel.end()) lv = std::max(lv, sw->second + 1);
+                        auto dw = wlevel.find(dc);
+                        if (dw != wlevel.end()) lv = std::max(lv, dw->second + 1);
+                        auto dr = rlevel.find(dc);
+                        if (dr != rlevel.end()) lv = std::max(lv, dr->second + 1);
+                        auto& rl = rlevel[sc];
+                        rl = std::max(rl, lv);
+                        h.ocell.push_back((int)cidx);
+                        h.olevel.push_back(lv);
+                        writes.push_back({dc, lv});
+                    }
+            // this copy's writes take effect after its reads
+            for (const auto& w : writes) {
+                wlevel[w.first] = w.second;
+                rlevel.erase(w.first);
+            }
+        }
+    }
     // surface range of every boundary, for per-node wall velocities
     P.bc_block.assign(d.nboundaries, -1);
     P.bc_range.assign(6 * (size_t)d.nboundaries, 0);
+    P.bc_scheme.assign(d.nboundaries, 0);
+    P.bc_surface.assign(d.nboundaries, 0);
     for (int k = 0; k < d.nboundaries; k++) {
+        P.bc_scheme[k] = d.boundaries[k].scheme;
+        P.bc_surface[k] = d.boundaries[k].surface;
         for (const BlockPlan& B : P.blocks) {
             if (B.id != d.boundaries[k].block) continue;
             P.bc_block[k] = B.index;
@@ -916,6 +1057,42 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                          &P.bc_range[6 * (size_t)k]);
         }
     }
+    return MPLBGPU_OK;
+}
+
+int BoundaryNodeOps(const Plan& P, int k, const double* uvw,
+                    std::vector<RegionOp>* out, std::string* err) {
+    if (k < 0 || k >= (int)P.bc_block.size() || P.bc_block[k] < 0) {
+        *err = "unknown boundary index";
+        return MPLBGPU_ERR_INVALID;
+    }
+    const int scheme = P.bc_scheme[k];
+    if (scheme != MPLBGPU_BC_EQM_DIFFUSE_REFL &&
+        scheme != MPLBGPU_BC_HALFWAY_BOUNCE_BACK) {
+        *err = "per-node velocities need an EQMDiffuseRefl or halfway "
+               "bounce-back boundary";
+        return MPLBGPU_ERR_UNSUPPORTED;
+    }
+    const BlockPlan& B = P.blocks[P.bc_block[k]];
+    const int* r = &P.bc_range[6 * (size_t)k];
+    Lat L{};
+    if (P.dim == 2) FillLat<2>(&L); else FillLat<3>(&L);
+    out->clear();
+    size_t idx = 0;
+    for (int z = r[4]; z < r[5]; z++)
+        for (int y = r[2]; y < r[3]; y++)
+            for (int x = r[0]; x < r[1]; x++, idx++) {
+                const int p[3] = {x, y, z};
+                int axis[3], sign[3];
+                const int nf = NodeFaces(P.dim, B.n, p, axis, sign, B.cut);
+                const double* g = uvw + 3 * idx;
+                RegionOp op = scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL
+                                  ? MakeEqm(L, P.cs, nf, axis, sign, g)
+                                  : MakeHbb(L, P.cs, B.n, p, P.bc_surface[k],
+                                            g);
+                op.bc = k;
+                out->push_back(op);
+            }
     return MPLBGPU_OK;
 }
 

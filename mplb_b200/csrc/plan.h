@@ -56,9 +56,10 @@ struct RegionOp {
     double a[kMaxQ];    // EQM: feq(1,u_w)/w per parallel population (res)
     double b[kMaxQ];    // EQM: c.u_w per outgoing; HBB: 2 w (c.u_w)
     // EQM / HBB with a wall velocity per node (mplbgpu_set_boundary_velocity):
-    // (u, v, w) per node of the boundary's surface range, x fastest, from
-    // node forg; null: the uniform given values above
-    const double* field;
+    // this operation evaluated for every node of the boundary's surface
+    // range (x fastest, from node forg) with that node's velocity; null:
+    // the constants above (uniform given values) hold for every node
+    const RegionOp* node_ops;
     int forg[3];
     int fext[3];
 };
@@ -100,6 +101,12 @@ struct BlockPlan {
     long long nstale;   // nodes with a stale store
     long long ndeferred;
     std::vector<DeferredOp> dops;
+    // every deferred node's programme in one pass is possible when no
+    // ExtrapolPressure1ST of a deferred node reads a deferred neighbour:
+    // per deferred region its operations (definition order, -1 ended)
+    bool deferred_fused = false;
+    std::vector<int> dops_flat;
+    int dops_first[kNumRegions] = {};
     std::vector<int> allops[kNumRegions];  // every op of a region (host)
     // swap scheme: per region, slot k of a node holds population
     // swap_sigma[r][k] of the collided node after its local swap, and
@@ -121,6 +128,18 @@ struct HaloCopy {
     uint32_t pops;      // populations copied
     std::vector<uint8_t> prev;  // per box cell: read the previous array
     bool any_prev;
+    // Fused transfer (all copies in one launch): a cell whose source is a
+    // block node (never written by a copy) and whose destination no other
+    // copy writes runs in the parallel phase; the rest (sources in a halo
+    // layer, destinations written twice) run afterwards copy by copy in
+    // definition order, which keeps the sequential result.
+    std::vector<uint8_t> ordered;   // per box cell: 1 = ordered phase
+    long long nordered = 0;
+    // ordered cells with their level: a cell runs after every cell of a
+    // lower level (its source's writer, its destination's earlier writer
+    // and earlier readers); level 0 is the parallel phase
+    std::vector<int> ocell;
+    std::vector<int> olevel;
 };
 
 struct Plan {
@@ -145,10 +164,20 @@ struct Plan {
     // range [r0, r1) x [r2, r3) x [r4, r5) (Block::BoundarySurfaceRange)
     std::vector<int> bc_block;
     std::vector<int> bc_range;
+    std::vector<int> bc_scheme;
+    std::vector<int> bc_surface;
 };
 
 // Builds the plan; returns MPLBGPU_OK or an error code with a message.
 int BuildPlan(const mplbgpu_desc& desc, Plan* plan, std::string* err);
+
+// Boundary `boundary` (EQMDiffuseRefl or halfway bounce-back) evaluated
+// per node of its surface range with a per-node wall velocity `uvw`
+// (u, v, w per node, x fastest): each node's operation has the masks of its
+// region and the constants of its own velocity, computed as the uniform
+// operations are.
+int BoundaryNodeOps(const Plan& P, int boundary, const double* uvw,
+                    std::vector<RegionOp>* out, std::string* err);
 
 // Region of coordinate v on an axis of n nodes: 0 first, 2 last, 1 inside.
 inline int RegionCoord(int v, int n) {

@@ -211,6 +211,10 @@ void CalcResidualError() {
     }
 }
 
+void Synchronize() {
+    if (g_ctx) Check(mplbgpu_synchronize(g_ctx), "mplbgpu_synchronize");
+}
+
 void Release() {
     if (g_ctx) mplbgpu_destroy(g_ctx);
     g_ctx = nullptr;

@@ -12,7 +12,9 @@
 // creates an mplbgpu context and sets its state - from the initial
 // macroscopic fields when the first step is at time 0 (f = feq of them, and
 // they are the residual's previous values as in the reference), else by
-// uploading f (restart); from then on the distributions stay on the GPU.  UpdateMacroVars copies the moments (and, unless MPLB_B200_SYNC_F=0,
+// uploading f (restart); from then on the distributions stay on the GPU and
+// StreamCollision only queues the step's kernels (no host wait).
+// UpdateMacroVars copies the moments (and, unless MPLB_B200_SYNC_F=0,
 // the distributions) back into the reference's dats so that Iterate's HDF5
 // writers see current data.  MPLB_B200_PRECISION=fp32|fp16 selects a
 // shifted storage form (default fp64, bit-identical to the reference).
@@ -38,6 +40,10 @@ void UpdateMacroVars();
 
 // Replaces CalcResidualError (Src/flowfield_wrapper.cpp:31-89) when Active().
 void CalcResidualError();
+
+// Waits until the GPU has done every step queued so far (StreamCollision
+// returns as soon as its kernels are queued).
+void Synchronize();
 
 // Frees the GPU context.
 void Release();

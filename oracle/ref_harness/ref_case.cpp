@@ -242,6 +242,9 @@ int main(int argc, const char** argv) {
         for (long it = 0; it < timingSteps; it++) {
             Step((steps + it) * TimeStep());
         }
+#ifdef MPLB_DROPIN
+        mplbgpu_dropin::Synchronize();   // the GPU steps are queued only
+#endif
         const auto t1 = std::chrono::steady_clock::now();
         long cells{0};
         for (auto& idBlock : g_Block()) {

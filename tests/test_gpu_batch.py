@@ -1,6 +1,7 @@
 """Batched cavities: every cavity of an FP64 batch is bit-identical to the
 same cavity run alone through the single-block path (halfway bounce-back
-walls, lid on Top), in both launch styles; residuals match the
+walls, lid on Top), in both launch styles (one CTA per tile, cooperative
+persistent); residuals match the
 single-block residual; converged cavities drop out; FP32 tracks FP64."""
 import numpy as np
 import pytest
@@ -116,3 +117,58 @@ def test_batch_large_cavity_row_division(gpu_lib, tile):
         for a, w in zip(g, want):
             assert np.array_equal(a, w), spec
     b.close()
+
+
+def test_autotune_valid_cached_and_bitwise(gpu_lib, tmp_path):
+    """The autotuner times its candidates on the batch, keeps one of them,
+    caches it (a second call reads the cache), and the batch it tunes gives
+    the bits of the default tuning (FP64)."""
+    from mplb_b200.batch import autotune, default_candidates
+    cache = str(tmp_path / "tuning.json")
+    b = Batch(SPECS, "fp64")
+    best = autotune(b, steps=20, cache=cache)
+    assert best["tuning"] in default_candidates()
+    assert len(best["all"]) == len(default_candidates())
+    assert all(r["mlups"] > 0 for r in best["all"])
+    assert b.tuning() == best["tuning"]
+    again = autotune(b, steps=20, cache=cache)
+    assert again == best
+    b.init()
+    b.step(37)
+    tuned = b.macro()
+    b.close()
+    d = Batch(SPECS, "fp64")
+    d.init()
+    d.step(37)
+    for g, w in zip(tuned, d.macro()):
+        for x, y in zip(g, w):
+            assert np.array_equal(x, y)
+    d.close()
+
+
+def test_persistent_barrier_timeout_then_reinit(gpu_lib):
+    """A grid barrier that gives up (a one-poll limit) ends the persistent
+    launch with MPLBGPU_ERR_TIMEOUT instead of waiting on; the batch then
+    refuses to step (MPLBGPU_ERR_STATE) until it is initialised again, after
+    which it runs as a fresh batch, bit for bit."""
+    from mplb_b200 import abi
+    from mplb_b200.batch import BatchError
+    b = Batch(SPECS, "fp64")
+    b.set_tuning(tile_nodes=64, persistent=1, chunk=10, ctas_per_sm=2)
+    b.init()
+    b.set_wait_limit(1)
+    with pytest.raises(BatchError) as e:
+        b.step(10)
+    assert e.value.status == abi.ERR_TIMEOUT
+    with pytest.raises(BatchError) as e:
+        b.step(10)
+    assert e.value.status == abi.ERR_STATE
+    b.set_wait_limit(1 << 26)
+    b.init()
+    b.step(37)
+    got = b.macro()
+    b.close()
+    for spec, g in zip(SPECS, got):
+        want, _ = single(spec, 37)
+        for a, w in zip(g, want):
+            assert np.array_equal(a, w), spec

@@ -72,3 +72,34 @@ def test_fp32_forced_spin_up_vs_fp64(gpu_lib, wall):
     got = run(mk("fp32"), 30000)
     assert rel_l2(got[1], ref[1]) < 1e-5
     assert rel_l2(got[0], ref[0]) < 1e-5
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-5), ("fp16", 2e-3)])
+@pytest.mark.parametrize("perturbed", [False, True])
+def test_lchannel_shifted_vs_fp64(gpu_lib, prec, tol, perturbed):
+    """Three joined blocks with a velocity inlet (uniform or with its +-1 %
+    per-node perturbation), a pressure outlet and z-periodic halos, from
+    rest: the shifted forms against FP64 (relative L2 of u and of rho - 1
+    over all blocks).  Halo cells that no transfer writes hold f = 0 in
+    every form, as the reference's zero-filled dats do."""
+    def velocity(p):
+        case = config.lchannel(leg=40, side=16, depth=12, precision=p)
+        with Solver(case) as s:
+            if perturbed:
+                k, comps = config.inlet_perturbation(case)
+                s.set_boundary_velocity(k, *comps)
+            s.init_uniform()
+            s.stream_collision(300)
+            s.update_macro_vars()
+            return [[a.copy() for a in s.macro(b)] for b in case.block_ids]
+
+    ref = velocity("fp64")
+    got = velocity(prec)
+
+    def rel(q, shift=0.0):
+        num = sum(np.linalg.norm(g[q] - r[q]) for g, r in zip(got, ref))
+        den = sum(np.linalg.norm(r[q] - shift) for r in ref)
+        return num / den
+
+    assert rel(1) < tol
+    assert rel(0, 1.0) < tol
