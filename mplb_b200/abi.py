@@ -144,6 +144,8 @@ _SIGNATURES = {
     "mplbgpu_step_begin": (ctypes.c_int, [ctypes.c_void_p]),
     "mplbgpu_step_finish": (ctypes.c_int, [ctypes.c_void_p]),
     "mplbgpu_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mplbgpu_step_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int)]),
     "mplbgpu_set_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "mplbgpu_boundary_extent": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                ctypes.c_void_p]),

@@ -31,6 +31,7 @@
 
 #include "lattice.h"
 #include "plan.h"
+#include "tma.cuh"
 
 namespace mplb {
 
@@ -84,6 +85,8 @@ struct BlockDev {
     // region PURE); center_fluid: the interior is fluid-like
     int split;
     int center_fluid;
+    // set (bit 0) by a step kernel whose wait for its tile loads ran out
+    unsigned* err;
     // deferred nodes in one kernel (no deferred node reads another):
     // per region, the first entry of its operation list in dops_flat (each
     // list in definition order, ended by -1)
@@ -1072,6 +1075,158 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                 D == 3 ? 1 + k.r / ny : 0);
 }
 
+// ---------------------------------------------------------------------------
+// The step of the shifted forms with the interior loaded by TMA.
+//
+// An interior CTA takes a tile of kTileRows rows (one per warp) x 32 G nodes
+// of one plane.  One thread issues, per population, one tiled TMA copy of
+// the tile's upstream box - the rows y - c_y, the plane z - c_z and the
+// columns the x shift reaches, widened to a 16-byte boundary - into shared
+// memory; every lane then reads its nodes' populations from shared memory at
+// offsets known at compile time, so no per-population address arithmetic
+// remains in the loads.  The arithmetic and the stores are PureNodeGroup's
+// (the same node pairs, the same bits).  Rows are enumerated per plane
+// padded to a multiple of kTileRows so that no tile spans two planes; shell
+// rows and x faces are SplitStepKernel's.
+constexpr int kTileRows = kSplitWarps;
+
+template <typename T>
+__host__ __device__ constexpr int TmaPad() {   // 16 bytes of elements
+    return 16 / (int)sizeof(T);
+}
+template <typename T>
+__host__ __device__ constexpr int TmaBoxW() {
+    return 32 * SplitGroup<T>() + TmaPad<T>();
+}
+template <typename T>
+__host__ __device__ constexpr int TmaPopBytes() {   // 128-byte aligned
+    return (TmaBoxW<T>() * kTileRows * (int)sizeof(T) + 127) / 128 * 128;
+}
+template <int D, typename T>
+__host__ __device__ constexpr int TmaSmemBytes() {
+    // + the mbarrier + slack to align the base to 128 bytes
+    return Lattice<D>::Q * TmaPopBytes<T>() + 16 + 128;
+}
+
+// Rows of the TMA step: interior rows per plane padded to kTileRows.
+__host__ __device__ inline int TmaPlaneRows(int n1) {
+    return (n1 - 2 + kTileRows - 1) / kTileRows * kTileRows;
+}
+
+template <int D, typename T, bool O32>
+__global__ void __launch_bounds__(128, MPLB_LP_MIN_BLOCKS)
+    SplitTmaStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
+                       T* __restrict__ dst, unsigned blk0,
+                       const __grid_constant__ CUtensorMap tsrc) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    constexpr int Q = L::Q;
+    constexpr int G = SplitGroup<T>();
+    static_assert(G == 2 && P::kShifted, "TMA step: shifted forms, node pairs");
+    const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int ny = b.n[1] - 2;
+    const int nz = D == 3 ? b.n[2] : 1;
+    const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
+    unsigned blk = blockIdx.x + blk0;
+    if (blk < nsr) {
+        const int row = (int)(blk / nbx);
+        const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
+        if (x >= b.n[0]) return;
+        int y, z;
+        if (row < 2 * nz) {
+            y = (row & 1) ? b.n[1] - 1 : 0;
+            z = row >> 1;
+        } else {
+            const int r2 = row - 2 * nz;
+            z = (r2 & 1) ? b.n[2] - 1 : 0;
+            y = 1 + (r2 >> 1);
+        }
+        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
+                                       nullptr, nullptr, x, y, z);
+        return;
+    }
+    blk -= nsr;
+    const int ny4 = TmaPlaneRows(b.n[1]);
+    const int rows = ny4 * (D == 3 ? b.n[2] - 2 : 1);
+    const unsigned per_chunk = (unsigned)SplitChunkCtas<G>(b.n[0]);
+    const int chunk = (int)(blk / per_chunk);
+    const int w = (int)(blk % per_chunk);
+    if (w == 0) {
+        const int r = chunk * kSplitRows + (int)(threadIdx.x >> 1);
+        if (threadIdx.x >= 2 * kSplitRows || r >= rows || r % ny4 >= ny) return;
+        const int x = (threadIdx.x & 1) ? b.n[0] - 1 : 0;
+        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
+                                       nullptr, nullptr, x, 1 + r % ny4,
+                                       D == 3 ? 1 + r / ny4 : 0);
+        return;
+    }
+    const int tpr = (b.n[0] + 32 * G - 1) / (32 * G);
+    const int g = (w - 1) / tpr;              // row group in the chunk
+    const int r0 = chunk * kSplitRows + g * kTileRows;
+    if (g * kTileRows >= kSplitRows || r0 >= rows) return;   // whole CTA
+    const int xs = ((w - 1) % tpr) * 32 * G;  // first column of the tile
+    const int y0 = 1 + r0 % ny4;
+    const int z = D == 3 ? 1 + r0 / ny4 : 0;
+
+    extern __shared__ __align__(128) unsigned char tma_raw[];
+    // population boxes on 128-byte boundaries (the launch adds the slack)
+    unsigned char* tma_smem =
+        tma_raw + ((128 - (tma::SmemAddr(tma_raw) & 127)) & 127);
+    uint64_t* bar =
+        reinterpret_cast<uint64_t*>(tma_smem + Q * TmaPopBytes<T>());
+    if (threadIdx.x == 0) {
+        tma::BarInit(bar, 1);
+        tma::FenceBarrierInit();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        constexpr uint32_t kBox = TmaBoxW<T>() * kTileRows * sizeof(T);
+        tma::BarArriveExpectTx(bar, Q * kBox);
+        const uint64_t pol = tma::EvictFirstPolicy();
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const int xc = b.xoff + xs - (L::cx(i) > 0 ? TmaPad<T>() : 0);
+            tma::TmaLoad4DHint(tma_smem + i * TmaPopBytes<T>(), &tsrc, bar, xc,
+                               y0 + 1 - L::cy(i),
+                               D == 3 ? z + 1 - L::cz(i) : 0, i, pol);
+        }
+    }
+    if (!tma::BarWait(bar, 0, nullptr)) {
+        // the copies did not complete in time: record it, let them finish
+        // (bounded) and leave the tile unwritten
+        atomicOr(b.err, 1u);
+        tma::BarWaitDrain(bar, 0);
+        return;
+    }
+    const int k = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+    const int y = y0 + k;
+    if (r0 % ny4 + k >= ny) return;   // a padding row
+    NodeGroup<D, T, G> n;
+    n.first = -1;
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+        const int x = xs + lane + 32 * j;
+        n.valid[j] = x >= 1 && x <= b.n[0] - 2;
+        if (n.valid[j] && n.first < 0) n.first = j;
+    }
+    if (n.first < 0) return;
+    n.node[0] = NodeIndexT<D, O32>(b, xs + lane, y, z);
+#pragma unroll
+    for (int j = 1; j < G; j++) n.node[j] = n.node[0] + 32 * j;
+    const T* row = reinterpret_cast<const T*>(tma_smem) +
+                   k * TmaBoxW<T>() + lane;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        // column of x - c_x in the box of population i
+        constexpr int kPopElems = TmaPopBytes<T>() / (int)sizeof(T);
+        const int d = L::cx(i) > 0 ? TmaPad<T>() - 1 : (L::cx(i) < 0 ? 1 : 0);
+#pragma unroll
+        for (int j = 0; j < G; j++)
+            n.f[j][i] = P::Load(row + i * kPopElems + d + 32 * j, 0, i, pc);
+    }
+    GroupFinish<D, T, O32, G>(b, pc, dst, n);
+}
+
 // Deferred nodes: thread t -> (region, node).
 __device__ __forceinline__ bool DeferredNode(const BlockDev& b, long long t,
                                              int& region, int& x, int& y,
@@ -1502,13 +1657,27 @@ struct HaloCopyDev {
     const uint8_t* ordered;    // per cell: left to the ordered phase
 };
 
-constexpr int kHaloCellsPerCta = 1024;
+constexpr int kHaloThreads = 512;
+constexpr int kHaloCellsPerCta = 4 * kHaloThreads;
+constexpr int kHaloMaxBlocks = 64;   // blocks whose descriptors go to smem
+
+// An ordered cell with its addresses resolved on the host: element offsets
+// of the source and destination nodes, the source block and array (bit 0:
+// the previous array), the destination block and the populations copied.
+struct HaloOrderedCell {
+    long long s, d;
+    int from2;                 // 2 * source block + (previous array ? 1 : 0)
+    int to;
+    uint32_t pops;
+    int pad;
+};
 
 struct HaloFusedDev {
     const HaloCopyDev* copies;
     const HaloBlockDev* blocks;
+    int nblocks;
     const int2* ctas;          // per CTA: (copy, first cell)
-    const int2* olist;         // ordered cells (copy, cell) by level
+    const HaloOrderedCell* olist;   // ordered cells by level
     const int* olevel;         // first entry of each level, nlevels + 1
     int nlevels;
     unsigned* ticket;          // CTAs done with the parallel phase
@@ -1532,46 +1701,52 @@ __device__ __forceinline__ T LoadL2(const T* p) {
         return __ldcg(p);
 }
 
-template <int D, typename T, bool ORDERED>
-__device__ __forceinline__ void HaloCell(const HaloFusedDev& h,
-                                         const HaloCopyDev& c, long long t,
-                                         int cur) {
+template <int D, typename T>
+__global__ void __launch_bounds__(kHaloThreads)
+    HaloFusedKernel(HaloFusedDev h, int cur) {
     using L = Lattice<D>;
     constexpr int Q = L::Q;
-    const HaloBlockDev& fb = h.blocks[c.from];
-    const HaloBlockDev& tb = h.blocks[c.to];
-    const int i = (int)(t % c.iter[0]);
-    const int j = (int)((t / c.iter[0]) % c.iter[1]);
-    const int k = (int)(t / ((long long)c.iter[0] * c.iter[1]));
-    const long long s = HaloNodeIndex<D>(fb, c.fbase[0] + i, c.fbase[1] + j,
-                                         c.fbase[2] + k);
-    const long long d = HaloNodeIndex<D>(tb, c.tbase[0] + i, c.tbase[1] + j,
-                                         c.tbase[2] + k);
-    const int sa = (c.prev != nullptr && c.prev[t]) ? 1 - cur : cur;
-    const T* from = static_cast<const T*>(fb.pop[sa]);
-    T* to = static_cast<T*>(tb.pop[cur]);
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-        if (!(c.pops >> q & 1u)) continue;
-        const T* src = from + q * fb.popstride + s;
-        to[q * tb.popstride + d] = ORDERED ? LoadL2(src) : *src;
-    }
-}
-
-template <int D, typename T>
-__global__ void __launch_bounds__(256)
-    HaloFusedKernel(HaloFusedDev h, int cur) {
+    __shared__ HaloCopyDev sc;
+    __shared__ HaloBlockDev sb[2];
+    __shared__ bool last;
     // parallel phase: kHaloCellsPerCta cells of one copy
+    const int2 a = h.ctas[blockIdx.x];
+    if (threadIdx.x == 0) {
+        sc = h.copies[a.x];
+        sb[0] = h.blocks[sc.from];
+        sb[1] = h.blocks[sc.to];
+    }
+    __syncthreads();
     {
-        const int2 a = h.ctas[blockIdx.x];
-        const HaloCopyDev& c = h.copies[a.x];
-        const long long end =
-            min((long long)a.y + kHaloCellsPerCta, c.cells);
-        for (long long t = a.y + threadIdx.x; t < end; t += blockDim.x)
-            if (!c.ordered[t]) HaloCell<D, T, false>(h, c, t, cur);
+        const int cells = (int)sc.cells;
+        const int end = min(a.y + kHaloCellsPerCta, cells);
+        const T* cur_from = static_cast<const T*>(sb[0].pop[cur]);
+        const T* prev_from = static_cast<const T*>(sb[0].pop[1 - cur]);
+        T* to = static_cast<T*>(sb[1].pop[cur]);
+        for (int t = a.y + threadIdx.x; t < end; t += blockDim.x) {
+            if (sc.ordered[t]) continue;
+            const int i = t % sc.iter[0];
+            const int j = (t / sc.iter[0]) % sc.iter[1];
+            const int k = t / (sc.iter[0] * sc.iter[1]);
+            const long long s = HaloNodeIndex<D>(sb[0], sc.fbase[0] + i,
+                                                 sc.fbase[1] + j,
+                                                 sc.fbase[2] + k);
+            const long long d = HaloNodeIndex<D>(sb[1], sc.tbase[0] + i,
+                                                 sc.tbase[1] + j,
+                                                 sc.tbase[2] + k);
+            const T* from =
+                (sc.prev != nullptr && sc.prev[t]) ? prev_from : cur_from;
+            // every load of the cell before its stores: they overlap
+            T v[Q];
+#pragma unroll
+            for (int q = 0; q < Q; q++)
+                if (sc.pops >> q & 1u) v[q] = from[q * sb[0].popstride + s];
+#pragma unroll
+            for (int q = 0; q < Q; q++)
+                if (sc.pops >> q & 1u) to[q * sb[1].popstride + d] = v[q];
+        }
     }
     // the last CTA to get here runs the ordered phase
-    __shared__ bool last;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -1580,11 +1755,43 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // block descriptors in shared memory when they fit, else from global
+    __shared__ const void* pops[2 * kHaloMaxBlocks];
+    __shared__ long long pstride[kHaloMaxBlocks];
+    const bool in_smem = h.nblocks <= kHaloMaxBlocks;
+    if (in_smem)
+        for (int b = threadIdx.x; b < h.nblocks; b += blockDim.x) {
+            pops[2 * b] = h.blocks[b].pop[cur];
+            pops[2 * b + 1] = h.blocks[b].pop[1 - cur];
+            pstride[b] = h.blocks[b].popstride;
+        }
+    __syncthreads();
     for (int lv = 0; lv < h.nlevels; lv++) {
         for (int m = h.olevel[lv] + threadIdx.x; m < h.olevel[lv + 1];
              m += blockDim.x) {
-            const int2 e = h.olist[m];
-            HaloCell<D, T, true>(h, h.copies[e.x], e.y, cur);
+            const HaloOrderedCell e = h.olist[m];
+            const int fb = e.from2 >> 1, fa = (e.from2 & 1) ? 1 - cur : cur;
+            const T* from;
+            T* to;
+            long long fs, ts;
+            if (in_smem) {
+                from = static_cast<const T*>(pops[e.from2]);
+                to = static_cast<T*>(const_cast<void*>(pops[2 * e.to]));
+                fs = pstride[fb];
+                ts = pstride[e.to];
+            } else {
+                from = static_cast<const T*>(h.blocks[fb].pop[fa]);
+                to = static_cast<T*>(h.blocks[e.to].pop[cur]);
+                fs = h.blocks[fb].popstride;
+                ts = h.blocks[e.to].popstride;
+            }
+            T v[Q];
+#pragma unroll
+            for (int q = 0; q < Q; q++)
+                if (e.pops >> q & 1u) v[q] = LoadL2(from + q * fs + e.s);
+#pragma unroll
+            for (int q = 0; q < Q; q++)
+                if (e.pops >> q & 1u) to[q * ts + e.d] = v[q];
         }
         __syncthreads();
     }

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -23,6 +24,25 @@
 #include "plan.h"
 
 using namespace mplb;
+
+namespace mplb {
+namespace tma {
+EncodeTiledFn Encoder() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p,
+                                             12000, cudaEnableDefault,
+                                             &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+}  // namespace tma
+}  // namespace mplb
 
 namespace {
 
@@ -45,6 +65,10 @@ struct DevBlock {
         long long total = 0;
     };
     std::vector<DOp> dops;
+    // tiled TMA views of pop[0] / pop[1] (x, y, z, population), used by the
+    // shifted forms' interior loads when tma is set
+    CUtensorMap tmap[2];
+    bool tma = false;
 };
 
 struct DevHalo {          // device arrays of one copy of the halo plan
@@ -78,6 +102,9 @@ struct mplbgpu_ctx {
     unsigned long long step_count = 0;
     double* part = nullptr;     // reduction partials
     unsigned long long* bad = nullptr;
+    // step kernels' error word (mapped host memory, read after each wait)
+    unsigned* kerr_host = nullptr;
+    unsigned* kerr_dev = nullptr;
     double* scratch = nullptr;  // dense f staging
     size_t scratch_elems = 0;
     std::vector<RegionOp*> bc_field;  // per boundary: per-node operations
@@ -117,6 +144,16 @@ int SetErr(mplbgpu_ctx* c, int code, const std::string& m) {
                           std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// A wait on the context's stream, then the step kernels' error word: a step
+// kernel whose wait for its tile loads ran out left its tile unwritten, so
+// the state is lost (every block wants a new initial state).
+int CheckKernelErr(mplbgpu_ctx* ctx);
+#define CK_SYNC()                                                           \
+    do {                                                                    \
+        CK(cudaStreamSynchronize(ctx->stream));                             \
+        if (int rc_ = CheckKernelErr(ctx)) return rc_;                      \
+    } while (0)
+
 #define CK_LAUNCH_E(...)                                                    \
     do {                                                                    \
         ctx->launches++;                                                    \
@@ -127,6 +164,17 @@ int SetErr(mplbgpu_ctx* c, int code, const std::string& m) {
                               cudaGetErrorString(e_));                      \
     } while (0)
 #define CK_LAUNCH() CK_LAUNCH_E(cudaGetLastError())
+
+int CheckKernelErr(mplbgpu_ctx* ctx) {
+    if (ctx->kerr_host == nullptr ||
+        *static_cast<volatile unsigned*>(ctx->kerr_host) == 0)
+        return MPLBGPU_OK;
+    *static_cast<volatile unsigned*>(ctx->kerr_host) = 0;
+    ctx->initialised.assign(ctx->initialised.size(), false);
+    return SetErr(ctx, MPLBGPU_ERR_TIMEOUT,
+                  "a step kernel's wait for its tile loads ran out; the "
+                  "state is lost (initialise again)");
+}
 
 dim3 NodeGrid(const BlockPlan& B, int dim) {
     return dim3((B.n[0] + kThreads - 1) / kThreads, B.n[1],
@@ -143,6 +191,58 @@ const BlockPlan* FindPlan(mplbgpu_ctx* ctx, int id) {
     for (const BlockPlan& B : ctx->plan.blocks)
         if (B.id == id) return &B;
     return nullptr;
+}
+
+// The tiled TMA view of one population array of block B: dimensions (x
+// over the row pitch, y with its halo rows, z with its halo planes,
+// population), the box one interior tile of SplitTmaStepKernel loads per
+// population.  False if the driver has no encoder or rejects the view.
+template <int D, typename T>
+bool EncodePopView(CUtensorMap* m, void* pop, const BlockPlan& B) {
+    tma::EncodeTiledFn enc = tma::Encoder();
+    if (enc == nullptr) return false;
+    const size_t e = sizeof(T);
+    const cuuint64_t dims[4] = {(cuuint64_t)B.pitch, (cuuint64_t)B.n[1] + 2,
+                                (cuuint64_t)(D == 3 ? B.n[2] + 2 : 1),
+                                (cuuint64_t)Lattice<D>::Q};
+    const cuuint64_t strides[3] = {(cuuint64_t)B.pitch * e,
+                                   (cuuint64_t)B.plane * e,
+                                   (cuuint64_t)B.popstride * e};
+    const cuuint32_t box[4] = {(cuuint32_t)TmaBoxW<T>(),
+                               (cuuint32_t)kTileRows, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUtensorMapDataType dt = sizeof(T) == 4
+                                       ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                       : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    return enc(m, dt, 4, pop, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps for the TMA interior of the shifted forms' split step (not
+// when MPLBGPU_NO_TMA is set: the interior then loads per thread).
+void SetupTma(mplbgpu_ctx* c) {
+    const char* off = std::getenv("MPLBGPU_NO_TMA");
+    if (off != nullptr && off[0] != '\0' && off[0] != '0') return;
+    if (c->plan.precision == MPLBGPU_FP64 || c->plan.swap) return;
+    for (size_t bi = 0; bi < c->blocks.size(); bi++) {
+        DevBlock& b = c->blocks[bi];
+        const BlockPlan& B = c->plan.blocks[bi];
+        if (!b.dev.split) continue;
+        bool ok = true;
+        for (int k = 0; k < 2 && ok; k++) {
+            if (c->plan.dim == 3)
+                ok = c->plan.precision == MPLBGPU_FP32_SHIFTED
+                         ? EncodePopView<3, float>(&b.tmap[k], b.pop[k], B)
+                         : EncodePopView<3, __half>(&b.tmap[k], b.pop[k], B);
+            else
+                ok = c->plan.precision == MPLBGPU_FP32_SHIFTED
+                         ? EncodePopView<2, float>(&b.tmap[k], b.pop[k], B)
+                         : EncodePopView<2, __half>(&b.tmap[k], b.pop[k], B);
+        }
+        b.tma = ok;
+    }
 }
 
 void FreeAll(mplbgpu_ctx* c) {
@@ -168,12 +268,13 @@ void FreeAll(mplbgpu_ctx* c) {
     cudaFree(const_cast<HaloCopyDev*>(c->hfd.copies));
     cudaFree(const_cast<HaloBlockDev*>(c->hfd.blocks));
     cudaFree(const_cast<int2*>(c->hfd.ctas));
-    cudaFree(const_cast<int2*>(c->hfd.olist));
+    cudaFree(const_cast<HaloOrderedCell*>(c->hfd.olist));
     cudaFree(const_cast<int*>(c->hfd.olevel));
     cudaFree(c->hfd.ticket);
     for (RegionOp* p : c->bc_field) cudaFree(p);
     cudaFree(c->part);
     cudaFree(c->bad);
+    if (c->kerr_host) cudaFreeHost(c->kerr_host);
     cudaFree(c->scratch);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -243,7 +344,8 @@ int StepOnce(mplbgpu_ctx* ctx) {
         T* d = static_cast<T*>(b.pop[dst]);
         CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D), ctx->stream,
                                        b.dev, ctx->pc, s, d, nullptr, nullptr,
-                                       nullptr, nullptr));
+                                       nullptr, nullptr,
+                                       b.tma ? &b.tmap[src] : nullptr));
         if (B.ndeferred > 0 && b.dev.deferred_fused) {
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
             CK_LAUNCH_E(Launch<D, T>::DeferredFused(g, ctx->stream, b.dev,
@@ -281,7 +383,7 @@ int StepBeginT(mplbgpu_ctx* ctx) {
         if (!b.dev.split) continue;
         CK_LAUNCH_E(Launch<D, T>::StepPart(
             1, ctx->stream, b.dev, ctx->pc, static_cast<const T*>(b.pop[src]),
-            static_cast<T*>(b.pop[dst])));
+            static_cast<T*>(b.pop[dst]), b.tma ? &b.tmap[src] : nullptr));
     }
     ctx->begun = true;
     return MPLBGPU_OK;
@@ -299,11 +401,12 @@ int StepFinishT(mplbgpu_ctx* ctx) {
         T* d = static_cast<T*>(b.pop[dst]);
         if (b.dev.split) {
             CK_LAUNCH_E(Launch<D, T>::StepPart(2, ctx->stream, b.dev, ctx->pc,
-                                               s, d));
+                                               s, d,
+                                               b.tma ? &b.tmap[src] : nullptr));
         } else {
             CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D),
                                            ctx->stream, b.dev, ctx->pc, s, d,
-                                           nullptr, nullptr, nullptr,
+                                           nullptr, nullptr, nullptr, nullptr,
                                            nullptr));
         }
         if (B.ndeferred > 0 && b.dev.deferred_fused) {
@@ -360,7 +463,8 @@ int Observe(mplbgpu_ctx* ctx, int mode, size_t bi, double* o0, double* o1,
         return MPLBGPU_OK;
     }
     CK_LAUNCH_E(Launch<D, T>::Step(mode, NodeGrid(B, D), ctx->stream, b.dev,
-                                   ctx->pc, pv, nullptr, o0, o1, o2, o3));
+                                   ctx->pc, pv, nullptr, o0, o1, o2, o3,
+                                   nullptr));
     if (B.ndeferred > 0) {
         const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
         CK_LAUNCH_E(Launch<D, T>::DeferredFinish(mode, g, ctx->stream, b.dev,
@@ -684,7 +788,7 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     if (!P.halos.empty()) {
         std::vector<HaloCopyDev> copies;
         std::vector<int2> ctas;
-        std::vector<std::pair<int, int2>> ordered;   // (level, (copy, cell))
+        std::vector<std::pair<int, HaloOrderedCell>> ordered;   // by level
         int nlevels = 0;
         for (size_t t = 0; t < P.halos.size(); t++) {
             const HaloCopy& h = P.halos[t];
@@ -701,8 +805,24 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             cd.cells = (long long)h.iter[0] * h.iter[1] * h.iter[2];
             for (long long t0 = 0; t0 < cd.cells; t0 += kHaloCellsPerCta)
                 ctas.push_back(make_int2((int)t, (int)t0));
+            const BlockPlan& FB = P.blocks[h.from];
+            const BlockPlan& TB = P.blocks[h.to];
+            auto node = [&](const BlockPlan& B, long long x, long long y,
+                            long long z) {
+                return (P.dim == 3 ? z + 1 : 0) * B.plane + (y + 1) * B.pitch +
+                       x + B.xoff;
+            };
             for (size_t m = 0; m < h.ocell.size(); m++) {
-                ordered.push_back({h.olevel[m], make_int2((int)t, h.ocell[m])});
+                const long long u = h.ocell[m];
+                const long long i = u % h.iter[0], j = (u / h.iter[0]) % h.iter[1],
+                                k = u / ((long long)h.iter[0] * h.iter[1]);
+                HaloOrderedCell oc{};
+                oc.s = node(FB, h.fbase[0] + i, h.fbase[1] + j, h.fbase[2] + k);
+                oc.d = node(TB, h.tbase[0] + i, h.tbase[1] + j, h.tbase[2] + k);
+                oc.from2 = 2 * h.from + ((h.any_prev && h.prev[u]) ? 1 : 0);
+                oc.to = h.to;
+                oc.pops = h.pops;
+                ordered.push_back({h.olevel[m], oc});
                 nlevels = std::max(nlevels, h.olevel[m]);
             }
             if (h.any_prev) {
@@ -722,11 +842,11 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
         }
         // ordered cells by level (levels 1..nlevels); stable within a level
         std::stable_sort(ordered.begin(), ordered.end(),
-                         [](const std::pair<int, int2>& a,
-                            const std::pair<int, int2>& b) {
+                         [](const std::pair<int, HaloOrderedCell>& a,
+                            const std::pair<int, HaloOrderedCell>& b) {
                              return a.first < b.first;
                          });
-        std::vector<int2> olist;
+        std::vector<HaloOrderedCell> olist;
         std::vector<int> olevel(nlevels + 1, 0);
         for (size_t m = 0; m < ordered.size(); m++) olist.push_back(ordered[m].second);
         for (int lv = 1, m = 0; lv <= nlevels; lv++) {
@@ -761,14 +881,16 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             cudaSuccess)
             return fail_cuda(e, "halo blocks");
         c->hfd.blocks = static_cast<HaloBlockDev*>(p);
+        c->hfd.nblocks = (int)hb.size();
         if ((e = upload(ctas.data(), ctas.size() * sizeof(int2), &p)) !=
             cudaSuccess)
             return fail_cuda(e, "halo work");
         c->hfd.ctas = static_cast<int2*>(p);
-        if ((e = upload(olist.data(), olist.size() * sizeof(int2), &p)) !=
+        if ((e = upload(olist.data(),
+                        olist.size() * sizeof(HaloOrderedCell), &p)) !=
             cudaSuccess)
             return fail_cuda(e, "halo order");
-        c->hfd.olist = static_cast<int2*>(p);
+        c->hfd.olist = static_cast<HaloOrderedCell*>(p);
         if ((e = upload(olevel.data(), olevel.size() * sizeof(int), &p)) !=
             cudaSuccess)
             return fail_cuda(e, "halo levels");
@@ -783,6 +905,15 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             cudaSuccess ||
         (e = cudaMalloc(&c->bad, sizeof(unsigned long long))) != cudaSuccess)
         return fail_cuda(e, "reduction buffers");
+    if ((e = cudaHostAlloc(reinterpret_cast<void**>(&c->kerr_host),
+                           sizeof(unsigned), cudaHostAllocMapped)) !=
+            cudaSuccess ||
+        (e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->kerr_dev),
+                                      c->kerr_host, 0)) != cudaSuccess)
+        return fail_cuda(e, "error word");
+    *c->kerr_host = 0;
+    for (DevBlock& b : c->blocks) b.dev.err = c->kerr_dev;
+    SetupTma(c.get());
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
         return fail_cuda(e, "cudaStreamSynchronize");
     *out = c.release();
@@ -828,7 +959,7 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
             std::fill(fill.begin(), fill.end(), m == 0 ? 1.0 : 0.0);
             CK(cudaMemcpyAsync(b->macro[m], fill.data(), nodes * sizeof(double),
                                cudaMemcpyHostToDevice, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            CK_SYNC();
         }
         // CopyCurrentMacroVar after PreDefinedInitialCondition3D
         CK(cudaMemcpyAsync(b->macro_old[m], b->macro[m], nodes * sizeof(double),
@@ -843,7 +974,7 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
     ctx->halos_pending = true;
     ctx->initialised[bi] = true;
     ctx->step_count = 0;   // a new initial state is step 0
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     return MPLBGPU_OK;
 }
 
@@ -879,7 +1010,7 @@ mplbgpu_status mplbgpu_upload_f(mplbgpu_ctx* ctx, int block, const double* f) {
         CK(cudaMemcpyAsync(b->macro_old[m], b->macro[m],
                            (size_t)B->nodes() * sizeof(double),
                            cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     return MPLBGPU_OK;
 }
 
@@ -937,13 +1068,29 @@ mplbgpu_status mplbgpu_get_stream(mplbgpu_ctx* ctx, void** stream) {
     return MPLBGPU_OK;
 }
 
+mplbgpu_status mplbgpu_step_kernel(mplbgpu_ctx* ctx, int block_id,
+                                   int* kind) {
+    if (!ctx || !kind) return MPLBGPU_ERR_INVALID;
+    for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
+        if (ctx->plan.blocks[bi].id != block_id) continue;
+        const DevBlock& b = ctx->blocks[bi];
+        *kind = ctx->plan.swap ? MPLBGPU_KERNEL_SWAP
+                : b.tma        ? MPLBGPU_KERNEL_SPLIT_TMA
+                : b.dev.split  ? MPLBGPU_KERNEL_SPLIT
+                               : MPLBGPU_KERNEL_NODE;
+        return MPLBGPU_OK;
+    }
+    return SetErr(ctx, MPLBGPU_ERR_INVALID,
+                  "unknown block id " + std::to_string(block_id));
+}
+
 mplbgpu_status mplbgpu_update_macro(mplbgpu_ctx* ctx) {
     if (!ctx) return MPLBGPU_ERR_INVALID;
     int rc = CheckReady(ctx);
     if (rc != MPLBGPU_OK) return rc;
     rc = UpdateMacro(ctx);
     if (rc != MPLBGPU_OK) return rc;
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     return MPLBGPU_OK;
 }
 
@@ -963,7 +1110,7 @@ mplbgpu_status mplbgpu_residual_sums(mplbgpu_ctx* ctx, double* diff,
             CK(cudaMemcpyAsync(part.data(), ctx->part,
                                part.size() * sizeof(double),
                                cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            CK_SYNC();
             for (int k = 0; k < kRedBlocks; k++) {
                 diff[m] += part[2 * k];
                 sum[m] += part[2 * k + 1];
@@ -1006,7 +1153,7 @@ mplbgpu_status mplbgpu_download_macro(mplbgpu_ctx* ctx, int block, double* rho,
         if (dst[m])
             CK(cudaMemcpyAsync(dst[m], b->macro[m], bytes,
                                cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     return MPLBGPU_OK;
 }
 
@@ -1027,7 +1174,7 @@ mplbgpu_status mplbgpu_download_f(mplbgpu_ctx* ctx, int block, double* f) {
     if (rc != MPLBGPU_OK) return rc;
     CK(cudaMemcpyAsync(f, ctx->scratch, elems * sizeof(double),
                        cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     return MPLBGPU_OK;
 }
 
@@ -1087,12 +1234,12 @@ static int SumRho(mplbgpu_ctx* ctx, double* total, unsigned long long* nbad) {
         CK_LAUNCH();
         CK(cudaMemcpyAsync(part.data(), ctx->part, part.size() * sizeof(double),
                            cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        CK_SYNC();
         for (double v : part) s += v;
     }
     CK(cudaMemcpyAsync(nbad, ctx->bad, sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     *total = s;
     return MPLBGPU_OK;
 }
@@ -1171,7 +1318,7 @@ mplbgpu_status mplbgpu_set_boundary_velocity(mplbgpu_ctx* ctx, int boundary,
                       "bounce-back boundary");
     }
     // no kernel of this context may read the op tables while they change
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     if (ctx->bc_field.size() < ctx->plan.bc_block.size())
         ctx->bc_field.resize(ctx->plan.bc_block.size(), nullptr);
     RegionOp*& dev = ctx->bc_field[boundary];
@@ -1204,7 +1351,7 @@ mplbgpu_status mplbgpu_set_step(mplbgpu_ctx* ctx, long long step) {
 
 mplbgpu_status mplbgpu_synchronize(mplbgpu_ctx* ctx) {
     if (!ctx) return MPLBGPU_ERR_INVALID;
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC();
     return MPLBGPU_OK;
 }
 
@@ -1216,6 +1363,7 @@ mplbgpu_status mplbgpu_last_step_ms(mplbgpu_ctx* ctx, float* ms) {
     if (!ctx || !ms) return MPLBGPU_ERR_INVALID;
     if (ctx->timing_pending) {
         CK(cudaEventSynchronize(ctx->ev1));
+        if (int rc = CheckKernelErr(ctx)) return (mplbgpu_status)rc;
         CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
         ctx->timing_pending = false;
     }

@@ -114,6 +114,14 @@ class Solver:
         self._check(self.lib.mplbgpu_set_step(self.h, int(step)))
         self.steps_done = int(step)
 
+    def step_kernel(self, block_id):
+        """Which step kernel the block runs: "node", "split", "split_tma"
+        or "swap" (mplbgpu_step_kernel)."""
+        k = ctypes.c_int(-1)
+        self._check(self.lib.mplbgpu_step_kernel(self.h, int(block_id),
+                                                 ctypes.byref(k)))
+        return ("node", "split", "split_tma", "swap")[k.value]
+
     # -- time stepping ------------------------------------------------------
     def stream_collision(self, n=1):
         self._check(self.lib.mplbgpu_step(self.h, int(n)))
