@@ -210,16 +210,12 @@ mplbgpu_status mplbgpu_get_stream(mplbgpu_ctx* ctx, void** stream);
 
 /* Which step kernel a block runs (a diagnostic; no reference counterpart):
  * one thread per node (blocks with a non-pure interior or an extent below
- * 3), the split step (shell rows, x faces and interior node pairs in
- * separate CTAs), the same with the interior tiles of the shifted forms
- * loaded by TMA (the default where the driver encodes the tensor maps;
- * environment variable MPLBGPU_NO_TMA=1 at mplbgpu_create selects the
- * per-thread loads, same results bit for bit), or the swap scheme's. */
+ * 3), the split step (shell rows, x faces and interior nodes in separate
+ * CTAs) or the swap scheme's. */
 enum {
     MPLBGPU_KERNEL_NODE = 0,
     MPLBGPU_KERNEL_SPLIT = 1,
-    MPLBGPU_KERNEL_SPLIT_TMA = 2,
-    MPLBGPU_KERNEL_SWAP = 3
+    MPLBGPU_KERNEL_SWAP = 2
 };
 mplbgpu_status mplbgpu_step_kernel(mplbgpu_ctx* ctx, int block_id, int* kind);
 

@@ -31,7 +31,6 @@
 
 #include "lattice.h"
 #include "plan.h"
-#include "tma.cuh"
 
 namespace mplb {
 
@@ -85,8 +84,6 @@ struct BlockDev {
     // region PURE); center_fluid: the interior is fluid-like
     int split;
     int center_fluid;
-    // set (bit 0) by a step kernel whose wait for its tile loads ran out
-    unsigned* err;
     // deferred nodes in one kernel (no deferred node reads another):
     // per region, the first entry of its operation list in dops_flat (each
     // list in definition order, ended by -1)
@@ -868,8 +865,7 @@ struct NodeGroup {
     int first;   // first valid node (the one a node group's seed follows)
 };
 
-// Loads the pulled populations of every node of the group (an invalid node
-// loads a valid node's values and is not stored).
+// Loads the pulled populations of every node of the group.
 template <int D, typename T, bool O32, int G>
 __device__ __forceinline__ void GroupLoad(const BlockDev& b,
                                           const PhysConst& pc,
@@ -953,7 +949,10 @@ __device__ __forceinline__ void GroupFinish(const BlockDev& b,
 }
 
 // The G nodes x0 + 32 j (j < G) of one interior row; nodes outside
-// [1, n0 - 2] load from the first valid one and are not stored.
+// [1, n0 - 2] are computed on whatever their places hold (an x face, a halo
+// column, the row padding, the next row or the slack after the last
+// population, all inside the allocation) and not stored.  Their element
+// indices stay 32 j apart, so one address serves every node of the group.
 template <int D, typename T, bool O32, int G>
 __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
                                               const PhysConst& pc,
@@ -969,10 +968,9 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
         if (n.valid[j] && n.first < 0) n.first = j;
     }
     if (n.first < 0) return;
+    n.node[0] = NodeIndexT<D, O32>(b, x0, y, z);
 #pragma unroll
-    for (int j = 0; j < G; j++)
-        n.node[j] = NodeIndexT<D, O32>(
-            b, x0 + 32 * (n.valid[j] ? j : n.first), y, z);
+    for (int j = 1; j < G; j++) n.node[j] = n.node[0] + 32 * j;
     GroupLoad<D, T, O32, G>(b, pc, src, n);
     GroupFinish<D, T, O32, G>(b, pc, dst, n);
 }
@@ -1073,158 +1071,6 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     if (k.r < 0 || k.r >= rows) return;
     PureNodeGroup<D, T, O32, G>(b, pc, src, dst, k.x0, 1 + k.r % ny,
                                 D == 3 ? 1 + k.r / ny : 0);
-}
-
-// ---------------------------------------------------------------------------
-// The step of the shifted forms with the interior loaded by TMA.
-//
-// An interior CTA takes a tile of kTileRows rows (one per warp) x 32 G nodes
-// of one plane.  One thread issues, per population, one tiled TMA copy of
-// the tile's upstream box - the rows y - c_y, the plane z - c_z and the
-// columns the x shift reaches, widened to a 16-byte boundary - into shared
-// memory; every lane then reads its nodes' populations from shared memory at
-// offsets known at compile time, so no per-population address arithmetic
-// remains in the loads.  The arithmetic and the stores are PureNodeGroup's
-// (the same node pairs, the same bits).  Rows are enumerated per plane
-// padded to a multiple of kTileRows so that no tile spans two planes; shell
-// rows and x faces are SplitStepKernel's.
-constexpr int kTileRows = kSplitWarps;
-
-template <typename T>
-__host__ __device__ constexpr int TmaPad() {   // 16 bytes of elements
-    return 16 / (int)sizeof(T);
-}
-template <typename T>
-__host__ __device__ constexpr int TmaBoxW() {
-    return 32 * SplitGroup<T>() + TmaPad<T>();
-}
-template <typename T>
-__host__ __device__ constexpr int TmaPopBytes() {   // 128-byte aligned
-    return (TmaBoxW<T>() * kTileRows * (int)sizeof(T) + 127) / 128 * 128;
-}
-template <int D, typename T>
-__host__ __device__ constexpr int TmaSmemBytes() {
-    // + the mbarrier + slack to align the base to 128 bytes
-    return Lattice<D>::Q * TmaPopBytes<T>() + 16 + 128;
-}
-
-// Rows of the TMA step: interior rows per plane padded to kTileRows.
-__host__ __device__ inline int TmaPlaneRows(int n1) {
-    return (n1 - 2 + kTileRows - 1) / kTileRows * kTileRows;
-}
-
-template <int D, typename T, bool O32>
-__global__ void __launch_bounds__(128, MPLB_LP_MIN_BLOCKS)
-    SplitTmaStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
-                       T* __restrict__ dst, unsigned blk0,
-                       const __grid_constant__ CUtensorMap tsrc) {
-    using L = Lattice<D>;
-    using P = Prec<T>;
-    constexpr int Q = L::Q;
-    constexpr int G = SplitGroup<T>();
-    static_assert(G == 2 && P::kShifted, "TMA step: shifted forms, node pairs");
-    const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
-    const int ny = b.n[1] - 2;
-    const int nz = D == 3 ? b.n[2] : 1;
-    const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
-    unsigned blk = blockIdx.x + blk0;
-    if (blk < nsr) {
-        const int row = (int)(blk / nbx);
-        const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
-        if (x >= b.n[0]) return;
-        int y, z;
-        if (row < 2 * nz) {
-            y = (row & 1) ? b.n[1] - 1 : 0;
-            z = row >> 1;
-        } else {
-            const int r2 = row - 2 * nz;
-            z = (r2 & 1) ? b.n[2] - 1 : 0;
-            y = 1 + (r2 >> 1);
-        }
-        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
-                                       nullptr, nullptr, x, y, z);
-        return;
-    }
-    blk -= nsr;
-    const int ny4 = TmaPlaneRows(b.n[1]);
-    const int rows = ny4 * (D == 3 ? b.n[2] - 2 : 1);
-    const unsigned per_chunk = (unsigned)SplitChunkCtas<G>(b.n[0]);
-    const int chunk = (int)(blk / per_chunk);
-    const int w = (int)(blk % per_chunk);
-    if (w == 0) {
-        const int r = chunk * kSplitRows + (int)(threadIdx.x >> 1);
-        if (threadIdx.x >= 2 * kSplitRows || r >= rows || r % ny4 >= ny) return;
-        const int x = (threadIdx.x & 1) ? b.n[0] - 1 : 0;
-        StepNode<D, T, kModeStep, O32>(b, pc, src, dst, nullptr, nullptr,
-                                       nullptr, nullptr, x, 1 + r % ny4,
-                                       D == 3 ? 1 + r / ny4 : 0);
-        return;
-    }
-    const int tpr = (b.n[0] + 32 * G - 1) / (32 * G);
-    const int g = (w - 1) / tpr;              // row group in the chunk
-    const int r0 = chunk * kSplitRows + g * kTileRows;
-    if (g * kTileRows >= kSplitRows || r0 >= rows) return;   // whole CTA
-    const int xs = ((w - 1) % tpr) * 32 * G;  // first column of the tile
-    const int y0 = 1 + r0 % ny4;
-    const int z = D == 3 ? 1 + r0 / ny4 : 0;
-
-    extern __shared__ __align__(128) unsigned char tma_raw[];
-    // population boxes on 128-byte boundaries (the launch adds the slack)
-    unsigned char* tma_smem =
-        tma_raw + ((128 - (tma::SmemAddr(tma_raw) & 127)) & 127);
-    uint64_t* bar =
-        reinterpret_cast<uint64_t*>(tma_smem + Q * TmaPopBytes<T>());
-    if (threadIdx.x == 0) {
-        tma::BarInit(bar, 1);
-        tma::FenceBarrierInit();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        constexpr uint32_t kBox = TmaBoxW<T>() * kTileRows * sizeof(T);
-        tma::BarArriveExpectTx(bar, Q * kBox);
-        const uint64_t pol = tma::EvictFirstPolicy();
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const int xc = b.xoff + xs - (L::cx(i) > 0 ? TmaPad<T>() : 0);
-            tma::TmaLoad4DHint(tma_smem + i * TmaPopBytes<T>(), &tsrc, bar, xc,
-                               y0 + 1 - L::cy(i),
-                               D == 3 ? z + 1 - L::cz(i) : 0, i, pol);
-        }
-    }
-    if (!tma::BarWait(bar, 0, nullptr)) {
-        // the copies did not complete in time: record it, let them finish
-        // (bounded) and leave the tile unwritten
-        atomicOr(b.err, 1u);
-        tma::BarWaitDrain(bar, 0);
-        return;
-    }
-    const int k = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
-    const int y = y0 + k;
-    if (r0 % ny4 + k >= ny) return;   // a padding row
-    NodeGroup<D, T, G> n;
-    n.first = -1;
-#pragma unroll
-    for (int j = 0; j < G; j++) {
-        const int x = xs + lane + 32 * j;
-        n.valid[j] = x >= 1 && x <= b.n[0] - 2;
-        if (n.valid[j] && n.first < 0) n.first = j;
-    }
-    if (n.first < 0) return;
-    n.node[0] = NodeIndexT<D, O32>(b, xs + lane, y, z);
-#pragma unroll
-    for (int j = 1; j < G; j++) n.node[j] = n.node[0] + 32 * j;
-    const T* row = reinterpret_cast<const T*>(tma_smem) +
-                   k * TmaBoxW<T>() + lane;
-#pragma unroll
-    for (int i = 0; i < Q; i++) {
-        // column of x - c_x in the box of population i
-        constexpr int kPopElems = TmaPopBytes<T>() / (int)sizeof(T);
-        const int d = L::cx(i) > 0 ? TmaPad<T>() - 1 : (L::cx(i) < 0 ? 1 : 0);
-#pragma unroll
-        for (int j = 0; j < G; j++)
-            n.f[j][i] = P::Load(row + i * kPopElems + d + 32 * j, 0, i, pc);
-    }
-    GroupFinish<D, T, O32, G>(b, pc, dst, n);
 }
 
 // Deferred nodes: thread t -> (region, node).

@@ -12,18 +12,15 @@ namespace mplb {
 
 template <int D, typename T>
 struct Launch {
-    // tsrc: the TMA view of src for the shifted forms' split step (null:
-    // the interior loads per thread)
     static cudaError_t Step(int mode, dim3 grid, cudaStream_t s,
                             const BlockDev& b, const PhysConst& pc,
                             const T* src, T* dst, double* o0, double* o1,
-                            double* o2, double* o3, const CUtensorMap* tsrc);
+                            double* o2, double* o3);
     // the two parts of a split step (b.split): 1 = the x faces and the
     // interior rows (no node of theirs reads a halo layer beyond a y or z
     // face), 2 = the shell rows
     static cudaError_t StepPart(int part, cudaStream_t s, const BlockDev& b,
-                                const PhysConst& pc, const T* src, T* dst,
-                                const CUtensorMap* tsrc);
+                                const PhysConst& pc, const T* src, T* dst);
     static cudaError_t DeferredFused(unsigned grid, cudaStream_t s,
                                      const BlockDev& b, const PhysConst& pc,
                                      const T* src, T* dst);

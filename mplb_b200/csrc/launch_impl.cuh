@@ -32,53 +32,10 @@ long long SplitShellBlocks(const BlockDev& b) {
     return nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
 }
 
-// CTAs of SplitTmaStepKernel for block b (0: too many): chunks of the
-// per-plane padded rows.
-template <int D, typename T>
-long long SplitTmaBlocks(const BlockDev& b) {
-    const long long rows =
-        (long long)TmaPlaneRows(b.n[1]) * (D == 3 ? b.n[2] - 2 : 1);
-    const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
-    const long long blocks = SplitShellBlocks<D>(b) +
-                             chunks * SplitChunkCtas<SplitGroup<T>()>(b.n[0]);
-    return blocks > 0x7fffffffLL ? 0 : blocks;
-}
-
-// CTAs blk0 .. blk0 + grid - 1 of the shifted forms' TMA step.
-template <int D, typename T>
-cudaError_t LaunchTmaStep(cudaStream_t s, const BlockDev& b,
-                          const PhysConst& pc, const T* src, T* dst,
-                          unsigned grid, unsigned blk0,
-                          const CUtensorMap& tsrc) {
-    if constexpr (Prec<T>::kShifted) {
-        constexpr int smem = TmaSmemBytes<D, T>();
-        static_assert(smem <= 48 * 1024, "TMA step tile beyond 48 KB");
-        if (b.off32)
-            SplitTmaStepKernel<D, T, true><<<grid, kStepThreads, smem, s>>>(
-                b, pc, src, dst, blk0, tsrc);
-        else
-            SplitTmaStepKernel<D, T, false><<<grid, kStepThreads, smem, s>>>(
-                b, pc, src, dst, blk0, tsrc);
-        return cudaGetLastError();
-    } else {
-        return cudaErrorInvalidValue;
-    }
-}
-
 template <int D, typename T>
 cudaError_t Launch<D, T>::StepPart(int part, cudaStream_t s, const BlockDev& b,
-                                   const PhysConst& pc, const T* src, T* dst,
-                                   const CUtensorMap* tsrc) {
+                                   const PhysConst& pc, const T* src, T* dst) {
     if (!b.split || (part != 1 && part != 2)) return cudaErrorInvalidValue;
-    if (tsrc != nullptr) {
-        const long long blocks = SplitTmaBlocks<D, T>(b);
-        if (blocks == 0) return cudaErrorInvalidConfiguration;
-        const long long shell = SplitShellBlocks<D>(b);
-        const unsigned grid = (unsigned)(part == 1 ? blocks - shell : shell);
-        if (grid == 0) return cudaSuccess;
-        return LaunchTmaStep<D, T>(s, b, pc, src, dst, grid,
-                                   part == 1 ? (unsigned)shell : 0u, *tsrc);
-    }
     const long long blocks = SplitBlocks<D, T>(b);
     if (blocks == 0) return cudaErrorInvalidConfiguration;
     const long long shell = SplitShellBlocks<D>(b);
@@ -100,14 +57,7 @@ template <int D, typename T>
 cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const BlockDev& b, const PhysConst& pc,
                                const T* src, T* dst, double* o0, double* o1,
-                               double* o2, double* o3,
-                               const CUtensorMap* tsrc) {
-    if (mode == kModeStep && b.split && tsrc != nullptr) {
-        const long long blocks = SplitTmaBlocks<D, T>(b);
-        if (blocks == 0) return cudaErrorInvalidConfiguration;
-        return LaunchTmaStep<D, T>(s, b, pc, src, dst, (unsigned)blocks, 0u,
-                                   *tsrc);
-    }
+                               double* o2, double* o3) {
     if (mode == kModeStep && b.split) {
         const long long blocks = SplitBlocks<D, T>(b);
         if (blocks == 0) return cudaErrorInvalidConfiguration;

@@ -1,12 +1,15 @@
-// Inline-PTX wrappers for mbarriers and TMA tiled loads (sm_100a), shared
-// by the step kernels and the warm-start network.
+// Inline-PTX wrappers for mbarriers and TMA tiled loads (sm_100a) and the
+// driver's tensor-map encoder, for the warm-start network's kernels.
 //
 // Every wait here is bounded: a wait that runs out of polls returns false
 // and the caller records an error word and winds the kernel down.
 #pragma once
 
-#include <cstdint>
 #include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
 
 namespace mplb {
 namespace tma {
@@ -100,28 +103,6 @@ __device__ __forceinline__ void TmaLoad4D(void* dst, const CUtensorMap* m,
         : "memory");
 }
 
-// Tiled TMA load of a 4-D box with an L2 cache hint (an evict-first policy
-// for data read once).
-__device__ __forceinline__ void TmaLoad4DHint(void* dst, const CUtensorMap* m,
-                                              uint64_t* bar, int c0, int c1,
-                                              int c2, int c3,
-                                              uint64_t policy) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::"
-        "bytes.L2::cache_hint [%0], [%1, {%3, %4, %5, %6}], [%2], %7;" ::"r"(
-            SmemAddr(dst)),
-        "l"(reinterpret_cast<uint64_t>(m)), "r"(SmemAddr(bar)), "r"(c0),
-        "r"(c1), "r"(c2), "r"(c3), "l"(policy)
-        : "memory");
-}
-
-__device__ __forceinline__ uint64_t EvictFirstPolicy() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;"
-                 : "=l"(p));
-    return p;
-}
-
 // cuTensorMapEncodeTiled from the driver (no link against libcuda), or null.
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType,
                                   cuuint32_t, void*, const cuuint64_t*,
@@ -129,7 +110,20 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType,
                                   const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion,
                                   CUtensorMapFloatOOBfill);
-EncodeTiledFn Encoder();
+inline EncodeTiledFn Encoder() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p,
+                                             12000, cudaEnableDefault,
+                                             &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
 
 }  // namespace tma
 }  // namespace mplb

@@ -115,12 +115,12 @@ class Solver:
         self.steps_done = int(step)
 
     def step_kernel(self, block_id):
-        """Which step kernel the block runs: "node", "split", "split_tma"
-        or "swap" (mplbgpu_step_kernel)."""
+        """Which step kernel the block runs: "node", "split" or "swap"
+        (mplbgpu_step_kernel)."""
         k = ctypes.c_int(-1)
         self._check(self.lib.mplbgpu_step_kernel(self.h, int(block_id),
                                                  ctypes.byref(k)))
-        return ("node", "split", "split_tma", "swap")[k.value]
+        return ("node", "split", "swap")[k.value]
 
     # -- time stepping ------------------------------------------------------
     def stream_collision(self, n=1):
