@@ -25,7 +25,7 @@ SOURCES = [os.path.join(CSRC, u) for u, _ in UNITS]
 HEADERS = [os.path.join(CSRC, h) for h in ("kernels.cuh", "lattice.h",
                                             "plan.h", "launch.h",
                                             "launch_impl.cuh", "swap.cuh",
-                                            "batch_kernels.cuh",
+                                            "batch_kernels.cuh", "tma.cuh",
                                             "nn/umma.cuh", "nn/conv.cuh",
                                             "nn/conv_host.h")] + [
     os.path.join(HERE, "..", "include", h) for h in ("mplbgpu.h", "mplbnn.h")]
