@@ -665,18 +665,16 @@ __device__ __forceinline__ void ApplyEqm(typename Prec<T>::C* f,
 #pragma unroll
         for (int i = 0; i < Q; i++)
             if (op.in_mask >> i & 1u) sin += f[i];
-        const float inv = 1.0f / (float)op.denom;
-        const float drw = ((float)op.c0 + 2.0f * sin) * inv;
+        const float drw = (op.c0f + 2.0f * sin) * op.invf;
         const float rhoWall = 1.0f + drw;
 #pragma unroll
         for (int i = 0; i < Q; i++)
             if (op.par_mask >> i & 1u)
-                f[i] = pc.wf[i] * ((float)op.am1[i] + drw * (float)op.a[i]);
+                f[i] = pc.wf[i] * (op.am1f[i] + drw * op.af[i]);
 #pragma unroll
         for (int i = 0; i < Q; i++)
             if (op.out_mask >> i & 1u)
-                f[i] = f[L::opp(i)] +
-                       2.0f * rhoWall * pc.wf[i] * (float)op.b[i];
+                f[i] = f[L::opp(i)] + 2.0f * rhoWall * pc.wf[i] * op.bf[i];
     } else {
         double rhoIn = 0.0;
 #pragma unroll
@@ -709,7 +707,8 @@ __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
     for (int i = 0; i < Q; i++)
         if (op.out_mask >> i & 1u)
             f[i] = P::Load(src, L::opp(i) * b.popstride + node, L::opp(i), pc) +
-                   (typename P::C)op.b[i];
+                   (P::kShifted ? (typename P::C)op.bf[i]
+                                : (typename P::C)op.b[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -948,17 +947,89 @@ __device__ __forceinline__ void GroupFinish(const BlockDev& b,
     }
 }
 
-// The G nodes x0 + 32 j (j < G) of one interior row; nodes outside
-// [1, n0 - 2] are computed on whatever their places hold (an x face, a halo
-// column, the row padding, the next row or the slack after the last
-// population, all inside the allocation) and not stored.  Their element
-// indices stay 32 j apart, so one address serves every node of the group.
+// The shifted forms' node pair x0, x0 + 32 of one interior row, held
+// population by population in float2 registers from the loads through the
+// paired collision to the stores (no packing between the two).  A node
+// outside [1, n0 - 2] is computed on whatever its place holds (an x face, a
+// halo column, the row padding, the next row or the slack after the last
+// population, all inside the allocation) and not stored; the pair's element
+// indices stay 32 apart, so one address serves both.  Same bits as
+// MomentsCollidePair on the two nodes.
+template <int D, typename T, bool O32>
+__device__ __forceinline__ void PurePair(const BlockDev& b,
+                                         const PhysConst& pc,
+                                         const T* __restrict__ src,
+                                         T* __restrict__ dst, int x0, int y,
+                                         int z) {
+    using L = Lattice<D>;
+    using P = Prec<T>;
+    constexpr int Q = L::Q;
+    const bool v0 = x0 >= 1 && x0 <= b.n[0] - 2;
+    const bool v1 = x0 + 32 >= 1 && x0 + 32 <= b.n[0] - 2;
+    if (!v0 && !v1) return;
+    const long long node = NodeIndexT<D, O32>(b, x0, y, z);
+    float2 h[Q];
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        const long long k = O32 ? node + b.pull_off32[i]
+                                : PullIndex<L>(b, node, i);
+        if constexpr (std::is_same<T, __half>::value) {
+            // both scaled by one paired multiply (the same rounding as two)
+            h[i] = __fmul2_rn(make_float2(__half2float(src[k]),
+                                          __half2float(src[k + 32])),
+                              make_float2(pc.wlf[i], pc.wlf[i]));
+        } else {
+            h[i] = make_float2(P::Load(src, k, i, pc),
+                               P::Load(src, k + 32, i, pc));
+        }
+    }
+    const bool fl = b.center_fluid != 0;
+    float2 drho, u[3];
+    MomentsShiftedV<L, float2>(h, pc, fl, drho, u);
+    CollideShiftedV<L, float2>(h, pc, fl, drho, u, pc.omcf);
+    if constexpr (std::is_same<T, __half>::value) {
+        // population i of the two converted together by the hardware's
+        // stochastic rounding (cvt.rs.f16x2.f32, 32 random bits per pair
+        // from the first valid node's draw)
+        const Rng rg = SeedRng(pc.seed, v0 ? node : node + 32);
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const float2 sv =
+                __fmul2_rn(h[i], make_float2(pc.winvf[i], pc.winvf[i]));
+            const uint32_t pair = StochasticHalf2(sv.x, sv.y, SrDraw32(rg, i));
+            const long long k = O32 ? node + b.pop_off32[i]
+                                    : OwnIndex(b, node, i);
+            if (v0)
+                PopStore(dst + k,
+                         __ushort_as_half((unsigned short)(pair & 0xffffu)));
+            if (v1)
+                PopStore(dst + k + 32,
+                         __ushort_as_half((unsigned short)(pair >> 16)));
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const long long k = O32 ? node + b.pop_off32[i]
+                                    : OwnIndex(b, node, i);
+            if (v0) PopStore(dst + k, (T)h[i].x);
+            if (v1) PopStore(dst + k + 32, (T)h[i].y);
+        }
+    }
+}
+
+// The G nodes x0 + 32 j (j < G) of one interior row (the shifted forms'
+// pairs: PurePair); nodes outside [1, n0 - 2] are computed on whatever
+// their places hold and not stored.
 template <int D, typename T, bool O32, int G>
 __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
                                               const PhysConst& pc,
                                               const T* __restrict__ src,
                                               T* __restrict__ dst, int x0,
                                               int y, int z) {
+    if constexpr (Prec<T>::kShifted && G == 2) {
+        PurePair<D, T, O32>(b, pc, src, dst, x0, y, z);
+        return;
+    }
     NodeGroup<D, T, G> n;
     n.first = -1;
 #pragma unroll

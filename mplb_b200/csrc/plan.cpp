@@ -224,6 +224,18 @@ int DvType(const Lat& L, int nf, const int axis[3], const int sign[3], int l) {
 bool FluidLike(int vt) { return vt == kVtFluid || vt == kVtMD; }
 bool PullsAll(int vt) { return vt == kVtFluid || vt == kVtMD || vt == kVtVB; }
 
+// FP32 copies of an operation's constants for the shifted forms, rounded
+// as the device would round them (IEEE division and conversions).
+void SetFloatConsts(RegionOp& op) {
+    op.invf = op.denom != 0.0 ? 1.0f / (float)op.denom : 0.0f;
+    op.c0f = (float)op.c0;
+    for (int l = 0; l < kMaxQ; l++) {
+        op.am1f[l] = (float)op.am1[l];
+        op.af[l] = (float)op.a[l];
+        op.bf[l] = (float)op.b[l];
+    }
+}
+
 // EQMDiffuseRefl constants (KerCutCellEQMDiffuseRefl(3D),
 // Src/boundary_kernel.inc:534-613, 1184-1276).
 RegionOp MakeEqm(const Lat& L, double CS, int nf, const int axis[3],
@@ -263,6 +275,7 @@ RegionOp MakeEqm(const Lat& L, double CS, int nf, const int axis[3],
     op.c0 = 2 * op.win - op.denom;
     for (int l = 0; l < L.Q; l++)
         if (op.par_mask >> l & 1u) op.am1[l] = op.a[l] - 1.0;
+    SetFloatConsts(op);
     return op;
 }
 
@@ -330,6 +343,7 @@ RegionOp MakeHbb(const Lat& L, double CS, const int n[3], const int p[3],
         if (L.D == 3) cu = cu + CS * (double)L.c[l][2] * given[2];
         op.b[l] = 2.0 * L.w[l] * cu;
     }
+    SetFloatConsts(op);
     return op;
 }
 

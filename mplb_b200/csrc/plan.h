@@ -55,6 +55,10 @@ struct RegionOp {
     double rho_given;   // EXTRAPOL
     double a[kMaxQ];    // EQM: feq(1,u_w)/w per parallel population (res)
     double b[kMaxQ];    // EQM: c.u_w per outgoing; HBB: 2 w (c.u_w)
+    // the shifted forms' FP32 copies: 1 / (float)denom, (float)c0 and the
+    // arrays above rounded to float (SetFloatConsts)
+    float invf, c0f;
+    float am1f[kMaxQ], af[kMaxQ], bf[kMaxQ];
     // EQM / HBB with a wall velocity per node (mplbgpu_set_boundary_velocity):
     // this operation evaluated for every node of the boundary's surface
     // range (x fastest, from node forg) with that node's velocity; null:
