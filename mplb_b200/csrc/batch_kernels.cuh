@@ -50,6 +50,52 @@ struct GridSync {           // bounded grid-wide barrier state
     long long limit;        // polls before giving up
 };
 
+// Population i of node (x, y) = k of a cavity: pulled from x - c_i, or, when
+// that lies beyond a wall, the node's own opposite population plus the
+// lid's 2 w_i (c_i . u_lid) (the top wall).  Only the axes population i
+// moves along are checked (one unsigned compare each).
+template <typename T, int i>
+__device__ __forceinline__ typename Prec<T>::C BatchPull(
+    const BatchCav& cv, const T* __restrict__ s, int n, int nn, int x, int y,
+    int k, const PhysConst& pc) {
+    using L = Lattice<2>;
+    using P = Prec<T>;
+    using C = typename P::C;
+    constexpr int cx = L::cx(i), cy = L::cy(i);
+    const int sx = x - cx, sy = y - cy;
+    bool in = true;
+    if constexpr (cx != 0) in = in && (unsigned)sx < (unsigned)n;
+    if constexpr (cy != 0) in = in && (unsigned)sy < (unsigned)n;
+    if (in) return P::Load(s, (long long)i * nn + (long long)sy * n + sx, i, pc);
+    C b = (C)0;
+    if constexpr (cy < 0) {
+        if (sy > n - 1) {
+            if constexpr (P::kShifted) b = cv.lidbf[i];
+            else b = cv.lidb[i];
+        }
+    }
+    return P::Load(s, (long long)L::opp(i) * nn + k, L::opp(i), pc) + b;
+}
+
+template <typename T, int I>
+struct BatchPullAll {
+    __device__ static __forceinline__ void run(typename Prec<T>::C* f,
+                                               const BatchCav& cv,
+                                               const T* __restrict__ s, int n,
+                                               int nn, int x, int y, int k,
+                                               const PhysConst& pc) {
+        f[I] = BatchPull<T, I>(cv, s, n, nn, x, y, k, pc);
+        BatchPullAll<T, I + 1>::run(f, cv, s, n, nn, x, y, k, pc);
+    }
+};
+template <typename T>
+struct BatchPullAll<T, 9> {
+    __device__ static __forceinline__ void run(typename Prec<T>::C*,
+                                               const BatchCav&, const T*, int,
+                                               int, int, int, int,
+                                               const PhysConst&) {}
+};
+
 // One node of one cavity: pull with bounce-back, moments, collision.
 template <typename T, bool MACRO>
 __device__ __forceinline__ void BatchNode(const BatchDev& bd,
@@ -71,20 +117,7 @@ __device__ __forceinline__ void BatchNode(const BatchDev& bd,
     const T* s = src + base;
     T* d = dst + base;
     C f[Q];
-#pragma unroll
-    for (int i = 0; i < Q; i++) {
-        const int sx = x - L::cx(i), sy = y - L::cy(i);
-        if (sx >= 0 && sx < n && sy >= 0 && sy < n) {
-            f[i] = P::Load(s, i * nn + (long long)sy * n + sx, i, pc);
-        } else {
-            C b = (C)0;
-            if (sy > n - 1) {
-                if constexpr (P::kShifted) b = cv.lidbf[i];
-                else b = cv.lidb[i];
-            }
-            f[i] = P::Load(s, L::opp(i) * nn + k, L::opp(i), pc) + b;
-        }
-    }
+    BatchPullAll<T, 0>::run(f, cv, s, n, (int)nn, x, y, k, pc);
     double rho, u[3];
     MomentsCollideT<L, T>(f, pc, false, cv.omc, cv.omcf, rho, u);
     Rng rng = SeedRng(pc.seed, base + k);
@@ -125,20 +158,7 @@ __device__ __forceinline__ void BatchNodeGroup(const BatchDev& bd,
         const int k = kk[j];
         const int y = n <= 1024 ? (int)(((float)k + 0.5f) * ninv) : k / n;
         const int x = k - y * n;
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const int sx = x - L::cx(i), sy = y - L::cy(i);
-            if (sx >= 0 && sx < n && sy >= 0 && sy < n) {
-                f[j][i] = P::Load(s, i * nn + sy * n + sx, i, pc);
-            } else {
-                C b = (C)0;
-                if (sy > n - 1) {
-                    if constexpr (P::kShifted) b = cv.lidbf[i];
-                    else b = cv.lidb[i];
-                }
-                f[j][i] = P::Load(s, L::opp(i) * nn + k, L::opp(i), pc) + b;
-            }
-        }
+        BatchPullAll<T, 0>::run(f[j], cv, s, n, nn, x, y, k, pc);
     }
 #pragma unroll
     for (int j = 0; j < G; j++) {

@@ -1551,12 +1551,12 @@ __global__ void DirectObserveKernel(BlockDev b, PhysConst pc,
 }
 
 // All halo copies of a step in one launch.  Copies run in definition order
-// in the reference; here the cells that cannot depend on that order (source
-// not written earlier in the step, destination written by this copy alone)
-// run in parallel, a fixed range of one copy per CTA, and the last CTA to
-// finish (an atomic ticket, no waiting) runs the other cells level by level
-// (each after the cells it reads from or overwrites), with a CTA barrier
-// between levels.
+// in the reference; here every cell whose value one copy gives directly (its
+// source not written earlier in the step, its destination written by that
+// copy alone) is copied by its copy's box, a range of one copy per CTA, and
+// every other halo element is copied from its origin resolved on the host
+// (HaloElem), a range of those per CTA: no element is written twice and no
+// source is written in the launch, so the CTAs run in any order.
 struct HaloBlockDev {          // what a copy needs of a block
     long long pitch, plane, popstride;
     int xoff;
@@ -1571,33 +1571,28 @@ struct HaloCopyDev {
     int from, to;              // block indices
     long long cells;
     const uint8_t* prev;       // per cell: read the previous array (or null)
-    const uint8_t* ordered;    // per cell: left to the ordered phase
+    const uint8_t* ordered;    // per cell: copied as resolved elements
+};
+
+// A resolved element copy with its element offsets (population included).
+struct HaloElemDev {
+    long long s, d;
+    int from2;                 // 2 * origin block + (previous array ? 1 : 0)
+    int to;
 };
 
 constexpr int kHaloThreads = 512;
 constexpr int kHaloCellsPerCta = 4 * kHaloThreads;
 constexpr int kHaloMaxBlocks = 64;   // blocks whose descriptors go to smem
 
-// An ordered cell with its addresses resolved on the host: element offsets
-// of the source and destination nodes, the source block and array (bit 0:
-// the previous array), the destination block and the populations copied.
-struct HaloOrderedCell {
-    long long s, d;
-    int from2;                 // 2 * source block + (previous array ? 1 : 0)
-    int to;
-    uint32_t pops;
-    int pad;
-};
-
 struct HaloFusedDev {
     const HaloCopyDev* copies;
     const HaloBlockDev* blocks;
     int nblocks;
-    const int2* ctas;          // per CTA: (copy, first cell)
-    const HaloOrderedCell* olist;   // ordered cells by level
-    const int* olevel;         // first entry of each level, nlevels + 1
-    int nlevels;
-    unsigned* ticket;          // CTAs done with the parallel phase
+    const int2* ctas;          // per CTA: (copy, first cell) or (-1, first
+                               // resolved element)
+    const HaloElemDev* elems;
+    int nelems;
 };
 
 template <int D>
@@ -1607,121 +1602,70 @@ __device__ __forceinline__ long long HaloNodeIndex(const HaloBlockDev& b,
            (long long)(y + 1) * b.pitch + (long long)(x + b.xoff);
 }
 
-// A load that bypasses L1: in the ordered phase a source cell may have
-// been written by another SM in this launch.
-template <typename T>
-__device__ __forceinline__ T LoadL2(const T* p) {
-    if constexpr (std::is_same<T, __half>::value)
-        return __ushort_as_half(
-            __ldcg(reinterpret_cast<const unsigned short*>(p)));
-    else
-        return __ldcg(p);
-}
-
 template <int D, typename T>
 __global__ void __launch_bounds__(kHaloThreads)
     HaloFusedKernel(HaloFusedDev h, int cur) {
     using L = Lattice<D>;
     constexpr int Q = L::Q;
+    const int2 a = h.ctas[blockIdx.x];
+    if (a.x < 0) {
+        // resolved elements a.y .. a.y + kHaloCellsPerCta - 1
+        __shared__ const void* pops[2 * kHaloMaxBlocks];
+        const bool in_smem = h.nblocks <= kHaloMaxBlocks;
+        if (in_smem)
+            for (int b = threadIdx.x; b < h.nblocks; b += blockDim.x) {
+                pops[2 * b] = h.blocks[b].pop[cur];
+                pops[2 * b + 1] = h.blocks[b].pop[1 - cur];
+            }
+        __syncthreads();
+        const int end = min(a.y + kHaloCellsPerCta, h.nelems);
+        for (int m = a.y + threadIdx.x; m < end; m += blockDim.x) {
+            const HaloElemDev e = h.elems[m];
+            const int fb = e.from2 >> 1;
+            const T* from = static_cast<const T*>(
+                in_smem ? pops[e.from2]
+                        : h.blocks[fb].pop[(e.from2 & 1) ? 1 - cur : cur]);
+            T* to = static_cast<T*>(const_cast<void*>(
+                in_smem ? pops[2 * e.to] : h.blocks[e.to].pop[cur]));
+            to[e.d] = from[e.s];
+        }
+        return;
+    }
     __shared__ HaloCopyDev sc;
     __shared__ HaloBlockDev sb[2];
-    __shared__ bool last;
-    // parallel phase: kHaloCellsPerCta cells of one copy
-    const int2 a = h.ctas[blockIdx.x];
     if (threadIdx.x == 0) {
         sc = h.copies[a.x];
         sb[0] = h.blocks[sc.from];
         sb[1] = h.blocks[sc.to];
     }
     __syncthreads();
-    {
-        const int cells = (int)sc.cells;
-        const int end = min(a.y + kHaloCellsPerCta, cells);
-        const T* cur_from = static_cast<const T*>(sb[0].pop[cur]);
-        const T* prev_from = static_cast<const T*>(sb[0].pop[1 - cur]);
-        T* to = static_cast<T*>(sb[1].pop[cur]);
-        for (int t = a.y + threadIdx.x; t < end; t += blockDim.x) {
-            if (sc.ordered[t]) continue;
-            const int i = t % sc.iter[0];
-            const int j = (t / sc.iter[0]) % sc.iter[1];
-            const int k = t / (sc.iter[0] * sc.iter[1]);
-            const long long s = HaloNodeIndex<D>(sb[0], sc.fbase[0] + i,
-                                                 sc.fbase[1] + j,
-                                                 sc.fbase[2] + k);
-            const long long d = HaloNodeIndex<D>(sb[1], sc.tbase[0] + i,
-                                                 sc.tbase[1] + j,
-                                                 sc.tbase[2] + k);
-            const T* from =
-                (sc.prev != nullptr && sc.prev[t]) ? prev_from : cur_from;
-            // every load of the cell before its stores: they overlap
-            T v[Q];
+    const int cells = (int)sc.cells;
+    const int end = min(a.y + kHaloCellsPerCta, cells);
+    const T* cur_from = static_cast<const T*>(sb[0].pop[cur]);
+    const T* prev_from = static_cast<const T*>(sb[0].pop[1 - cur]);
+    T* to = static_cast<T*>(sb[1].pop[cur]);
+    for (int t = a.y + threadIdx.x; t < end; t += blockDim.x) {
+        if (sc.ordered[t]) continue;
+        const int i = t % sc.iter[0];
+        const int j = (t / sc.iter[0]) % sc.iter[1];
+        const int k = t / (sc.iter[0] * sc.iter[1]);
+        const long long s = HaloNodeIndex<D>(sb[0], sc.fbase[0] + i,
+                                             sc.fbase[1] + j, sc.fbase[2] + k);
+        const long long d = HaloNodeIndex<D>(sb[1], sc.tbase[0] + i,
+                                             sc.tbase[1] + j, sc.tbase[2] + k);
+        const T* from =
+            (sc.prev != nullptr && sc.prev[t]) ? prev_from : cur_from;
+        // every load of the cell before its stores: they overlap
+        T v[Q];
 #pragma unroll
-            for (int q = 0; q < Q; q++)
-                if (sc.pops >> q & 1u) v[q] = from[q * sb[0].popstride + s];
+        for (int q = 0; q < Q; q++)
+            if (sc.pops >> q & 1u) v[q] = from[q * sb[0].popstride + s];
 #pragma unroll
-            for (int q = 0; q < Q; q++)
-                if (sc.pops >> q & 1u) to[q * sb[1].popstride + d] = v[q];
-        }
+        for (int q = 0; q < Q; q++)
+            if (sc.pops >> q & 1u) to[q * sb[1].popstride + d] = v[q];
     }
-    // the last CTA to get here runs the ordered phase
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(h.ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // block descriptors in shared memory when they fit, else from global
-    __shared__ const void* pops[2 * kHaloMaxBlocks];
-    __shared__ long long pstride[kHaloMaxBlocks];
-    const bool in_smem = h.nblocks <= kHaloMaxBlocks;
-    if (in_smem)
-        for (int b = threadIdx.x; b < h.nblocks; b += blockDim.x) {
-            pops[2 * b] = h.blocks[b].pop[cur];
-            pops[2 * b + 1] = h.blocks[b].pop[1 - cur];
-            pstride[b] = h.blocks[b].popstride;
-        }
-    __syncthreads();
-    for (int lv = 0; lv < h.nlevels; lv++) {
-        for (int m = h.olevel[lv] + threadIdx.x; m < h.olevel[lv + 1];
-             m += blockDim.x) {
-            const HaloOrderedCell e = h.olist[m];
-            const int fb = e.from2 >> 1, fa = (e.from2 & 1) ? 1 - cur : cur;
-            const T* from;
-            T* to;
-            long long fs, ts;
-            if (in_smem) {
-                from = static_cast<const T*>(pops[e.from2]);
-                to = static_cast<T*>(const_cast<void*>(pops[2 * e.to]));
-                fs = pstride[fb];
-                ts = pstride[e.to];
-            } else {
-                from = static_cast<const T*>(h.blocks[fb].pop[fa]);
-                to = static_cast<T*>(h.blocks[e.to].pop[cur]);
-                fs = h.blocks[fb].popstride;
-                ts = h.blocks[e.to].popstride;
-            }
-            T v[Q];
-#pragma unroll
-            for (int q = 0; q < Q; q++)
-                if (e.pops >> q & 1u) v[q] = LoadL2(from + q * fs + e.s);
-#pragma unroll
-            for (int q = 0; q < Q; q++)
-                if (e.pops >> q & 1u) to[q * ts + e.d] = v[q];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *h.ticket = 0u;   // for the next launch
 }
 
-// Residual sums of one macroscopic variable over one block, per CTA:
-// sum (q - q_old)^2 and sum q^2 (KerCalcMacroVarSquareofDifference /
-// KerCalcMacroVarSquare, Src/flowfield_kernel.inc:131-153); q_old <- q.
-// Face exchange of a decomposed block (cut faces): element t of the face
-// buffer is population pop[t / (nu nv)] of the face node (u, v) =
-// (t % nu, (t / nu) % nv) on layer `layer` of the face's axis (the block's
-// own boundary layer for an export, the halo layer -1 or n for an import).
 struct FaceDev {
     int axis, layer;
     int ua, va;          // in-plane axes (va = -1 in 2D)

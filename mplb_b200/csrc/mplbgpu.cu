@@ -60,7 +60,7 @@ struct mplbgpu_ctx {
     PhysConst pc{};
     std::vector<DevBlock> blocks;
     std::vector<DevHalo> halos;
-    HaloFusedDev hfd{};     // the fused transfer (copies, blocks, ticket)
+    HaloFusedDev hfd{};     // the fused transfer (copies, blocks, elements)
     unsigned halo_ctas = 0;
     int cur = 0;            // pop[cur] holds the latest g
     bool initial = true;    // pop[1 - cur] holds f^0 itself
@@ -169,9 +169,7 @@ void FreeAll(mplbgpu_ctx* c) {
     cudaFree(const_cast<HaloCopyDev*>(c->hfd.copies));
     cudaFree(const_cast<HaloBlockDev*>(c->hfd.blocks));
     cudaFree(const_cast<int2*>(c->hfd.ctas));
-    cudaFree(const_cast<HaloOrderedCell*>(c->hfd.olist));
-    cudaFree(const_cast<int*>(c->hfd.olevel));
-    cudaFree(c->hfd.ticket);
+    cudaFree(const_cast<HaloElemDev*>(c->hfd.elems));
     for (RegionOp* p : c->bc_field) cudaFree(p);
     cudaFree(c->part);
     cudaFree(c->bad);
@@ -691,8 +689,6 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     if (!P.halos.empty()) {
         std::vector<HaloCopyDev> copies;
         std::vector<int2> ctas;
-        std::vector<std::pair<int, HaloOrderedCell>> ordered;   // by level
-        int nlevels = 0;
         for (size_t t = 0; t < P.halos.size(); t++) {
             const HaloCopy& h = P.halos[t];
             DevHalo dh;
@@ -708,26 +704,6 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             cd.cells = (long long)h.iter[0] * h.iter[1] * h.iter[2];
             for (long long t0 = 0; t0 < cd.cells; t0 += kHaloCellsPerCta)
                 ctas.push_back(make_int2((int)t, (int)t0));
-            const BlockPlan& FB = P.blocks[h.from];
-            const BlockPlan& TB = P.blocks[h.to];
-            auto node = [&](const BlockPlan& B, long long x, long long y,
-                            long long z) {
-                return (P.dim == 3 ? z + 1 : 0) * B.plane + (y + 1) * B.pitch +
-                       x + B.xoff;
-            };
-            for (size_t m = 0; m < h.ocell.size(); m++) {
-                const long long u = h.ocell[m];
-                const long long i = u % h.iter[0], j = (u / h.iter[0]) % h.iter[1],
-                                k = u / ((long long)h.iter[0] * h.iter[1]);
-                HaloOrderedCell oc{};
-                oc.s = node(FB, h.fbase[0] + i, h.fbase[1] + j, h.fbase[2] + k);
-                oc.d = node(TB, h.tbase[0] + i, h.tbase[1] + j, h.tbase[2] + k);
-                oc.from2 = 2 * h.from + ((h.any_prev && h.prev[u]) ? 1 : 0);
-                oc.to = h.to;
-                oc.pops = h.pops;
-                ordered.push_back({h.olevel[m], oc});
-                nlevels = std::max(nlevels, h.olevel[m]);
-            }
             if (h.any_prev) {
                 if ((e = cudaMalloc(&dh.prev, h.prev.size())) != cudaSuccess ||
                     (e = cudaMemcpy(dh.prev, h.prev.data(), h.prev.size(),
@@ -743,20 +719,24 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             copies.push_back(cd);
             c->halos.push_back(dh);
         }
-        // ordered cells by level (levels 1..nlevels); stable within a level
-        std::stable_sort(ordered.begin(), ordered.end(),
-                         [](const std::pair<int, HaloOrderedCell>& a,
-                            const std::pair<int, HaloOrderedCell>& b) {
-                             return a.first < b.first;
-                         });
-        std::vector<HaloOrderedCell> olist;
-        std::vector<int> olevel(nlevels + 1, 0);
-        for (size_t m = 0; m < ordered.size(); m++) olist.push_back(ordered[m].second);
-        for (int lv = 1, m = 0; lv <= nlevels; lv++) {
-            olevel[lv - 1] = m;
-            while (m < (int)ordered.size() && ordered[m].first == lv) m++;
-            olevel[lv] = m;
+        // the resolved element copies, with their element offsets
+        std::vector<HaloElemDev> elems;
+        for (const HaloElem& he : P.halo_elems) {
+            auto elem = [&](const BlockPlan& B, long long x, long long y,
+                            long long z) {
+                return (long long)he.pop * B.popstride +
+                       (P.dim == 3 ? z + 1 : 0) * B.plane + (y + 1) * B.pitch +
+                       x + B.xoff;
+            };
+            HaloElemDev ed{};
+            ed.s = elem(P.blocks[he.from], he.fx, he.fy, he.fz);
+            ed.d = elem(P.blocks[he.to], he.tx, he.ty, he.tz);
+            ed.from2 = 2 * he.from + he.prev;
+            ed.to = he.to;
+            elems.push_back(ed);
         }
+        for (size_t m0 = 0; m0 < elems.size(); m0 += kHaloCellsPerCta)
+            ctas.push_back(make_int2(-1, (int)m0));
         std::vector<HaloBlockDev> hb(c->blocks.size());
         for (size_t bi = 0; bi < c->blocks.size(); bi++) {
             const BlockPlan& B = P.blocks[bi];
@@ -789,19 +769,11 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
             cudaSuccess)
             return fail_cuda(e, "halo work");
         c->hfd.ctas = static_cast<int2*>(p);
-        if ((e = upload(olist.data(),
-                        olist.size() * sizeof(HaloOrderedCell), &p)) !=
-            cudaSuccess)
-            return fail_cuda(e, "halo order");
-        c->hfd.olist = static_cast<HaloOrderedCell*>(p);
-        if ((e = upload(olevel.data(), olevel.size() * sizeof(int), &p)) !=
-            cudaSuccess)
-            return fail_cuda(e, "halo levels");
-        c->hfd.olevel = static_cast<int*>(p);
-        c->hfd.nlevels = nlevels;
-        if ((e = cudaMalloc(&c->hfd.ticket, sizeof(unsigned))) != cudaSuccess ||
-            (e = cudaMemset(c->hfd.ticket, 0, sizeof(unsigned))) != cudaSuccess)
-            return fail_cuda(e, "halo ticket");
+        if ((e = upload(elems.data(), elems.size() * sizeof(HaloElemDev),
+                        &p)) != cudaSuccess)
+            return fail_cuda(e, "halo elements");
+        c->hfd.elems = static_cast<HaloElemDev*>(p);
+        c->hfd.nelems = (int)elems.size();
         c->halo_ctas = (unsigned)ctas.size();
     }
     if ((e = cudaMalloc(&c->part, 2 * kRedBlocks * sizeof(double))) !=

@@ -1013,48 +1013,51 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                         }
                     }
         }
-        // Levels of the ordered cells, copy by copy in definition order:
-        // a cell comes after the writer of its source, after the earlier
-        // writer of its destination and after every earlier reader of its
-        // destination (parallel-phase writes are level 0).
-        std::map<std::pair<int, long long>, int> wlevel;   // last write
-        std::map<std::pair<int, long long>, int> rlevel;   // reads since
+        // Resolved element copies: the copies run symbolically in
+        // definition order, each written element remembering where its
+        // value comes from (an element written earlier in the step passes
+        // on its own origin); the elements of the ordered cells' final
+        // writes are then copied from those origins directly.
+        struct Origin {
+            int blk, x, y, z, prev;
+        };
+        std::map<std::pair<std::pair<int, long long>, int>, Origin> origin;
+        std::map<std::pair<std::pair<int, long long>, int>, HaloElem> finals;
         for (size_t t = 0; t < P.halos.size(); t++) {
-            HaloCopy& h = P.halos[t];
-            h.ocell.clear();
-            h.olevel.clear();
+            const HaloCopy& h = P.halos[t];
             long long cidx = 0;
-            std::vector<std::pair<std::pair<int, long long>, int>> writes;
+            std::vector<std::pair<std::pair<std::pair<int, long long>, int>,
+                                  Origin>>
+                writes;
             for (int k = 0; k < h.iter[2]; k++)
                 for (int j = 0; j < h.iter[1]; j++)
                     for (int i = 0; i < h.iter[0]; i++, cidx++) {
-                        const auto dc = cell(h.to, h.tbase[0] + i,
-                                             h.tbase[1] + j, h.tbase[2] + k);
-                        const auto sc = cell(h.from, h.fbase[0] + i,
-                                             h.fbase[1] + j, h.fbase[2] + k);
-                        if (!h.ordered[cidx]) {
-                            writes.push_back({dc, 0});
-                            continue;
+                        const int fx = h.fbase[0] + i, fy = h.fbase[1] + j,
+                                  fz = h.fbase[2] + k;
+                        const int tx = h.tbase[0] + i, ty = h.tbase[1] + j,
+                                  tz = h.tbase[2] + k;
+                        const auto dc = cell(h.to, tx, ty, tz);
+                        const auto sc = cell(h.from, fx, fy, fz);
+                        const int pv = h.any_prev && h.prev[cidx] ? 1 : 0;
+                        for (int q = 0; q < P.Q; q++) {
+                            if (!(h.pops >> q & 1u)) continue;
+                            auto so = origin.find({sc, q});
+                            const Origin o =
+                                so != origin.end()
+                                    ? so->second
+                                    : Origin{h.from, fx, fy, fz, pv};
+                            writes.push_back({{dc, q}, o});
+                            if (h.ordered[cidx])
+                                finals[{dc, q}] = HaloElem{
+                                    h.to, tx, ty, tz, o.blk, o.x, o.y, o.z,
+                                    q, o.prev};
                         }
-                        int lv = 1;
-                        auto sw = wlevel.find(sc);
-                        if (sw != wlevel.end()) lv = std::max(lv, sw->second + 1);
-                        auto dw = wlevel.find(dc);
-                        if (dw != wlevel.end()) lv = std::max(lv, dw->second + 1);
-                        auto dr = rlevel.find(dc);
-                        if (dr != rlevel.end()) lv = std::max(lv, dr->second + 1);
-                        auto& rl = rlevel[sc];
-                        rl = std::max(rl, lv);
-                        h.ocell.push_back((int)cidx);
-                        h.olevel.push_back(lv);
-                        writes.push_back({dc, lv});
                     }
             // this copy's writes take effect after its reads
-            for (const auto& w : writes) {
-                wlevel[w.first] = w.second;
-                rlevel.erase(w.first);
-            }
+            for (const auto& w : writes) origin[w.first] = w.second;
         }
+        P.halo_elems.clear();
+        for (const auto& f : finals) P.halo_elems.push_back(f.second);
     }
     // surface range of every boundary, for per-node wall velocities
     P.bc_block.assign(d.nboundaries, -1);

@@ -132,21 +132,30 @@ struct HaloCopy {
     uint32_t pops;      // populations copied
     std::vector<uint8_t> prev;  // per box cell: read the previous array
     bool any_prev;
-    // Fused transfer (all copies in one launch): a cell whose source is a
-    // block node (never written by a copy) and whose destination no other
-    // copy writes runs in the parallel phase; the rest (sources in a halo
-    // layer, destinations written twice) run afterwards copy by copy in
-    // definition order, which keeps the sequential result.
-    std::vector<uint8_t> ordered;   // per box cell: 1 = ordered phase
+    // Fused transfer (all copies in one launch): a cell whose source no
+    // earlier copy writes and whose destination no other copy writes is
+    // copied by its box; the others (`ordered`) are left to the resolved
+    // element copies of Plan::halo_elems.
+    std::vector<uint8_t> ordered;   // per box cell: 1 = resolved elsewhere
     long long nordered = 0;
-    // ordered cells with their level: a cell runs after every cell of a
-    // lower level (its source's writer, its destination's earlier writer
-    // and earlier readers); level 0 is the parallel phase
-    std::vector<int> ocell;
-    std::vector<int> olevel;
+};
+
+// One population of one halo cell whose value the copies of a step produce
+// through more than one copy (a destination written twice, a source
+// written earlier): the final value's origin, resolved by following the
+// copies in definition order, so that it can be copied directly and in any
+// order (the origin is a place no copy of the step writes, read from the
+// current array, or from the previous one where the reference reads a
+// value that a later copy overwrites).
+struct HaloElem {
+    int to, tx, ty, tz;       // destination block and node (halo included)
+    int from, fx, fy, fz;     // origin block and node
+    int pop;
+    int prev;                 // 1: the origin is read from the previous array
 };
 
 struct Plan {
+    std::vector<HaloElem> halo_elems;   // resolved element copies
     int dim = 3;
     int Q = 19;
     int precision = MPLBGPU_FP64;
