@@ -72,6 +72,13 @@ struct mplbgpu_ctx {
     std::vector<bool> initialised;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // a step's independent launches (each block's step, deferred outlets)
+    // on side streams forked from `stream` and joined before the halos
+    static constexpr int kSides = 3;
+    cudaStream_t side[kSides] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kSides] = {nullptr, nullptr, nullptr};
+    int nlanes = 1;         // streams a step uses (1: no fork)
     float last_ms = 0;
     bool timing_pending = false;  // ev0/ev1 of the last step call unread
     bool begun = false;           // mplbgpu_step_begin without its finish
@@ -174,6 +181,11 @@ void FreeAll(mplbgpu_ctx* c) {
     cudaFree(c->part);
     cudaFree(c->bad);
     cudaFree(c->scratch);
+    for (int k = 0; k < mplbgpu_ctx::kSides; k++) {
+        if (c->side[k]) cudaStreamDestroy(c->side[k]);
+        if (c->join[k]) cudaEventDestroy(c->join[k]);
+    }
+    if (c->fork) cudaEventDestroy(c->fork);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -230,37 +242,63 @@ int SwapStepOnce(mplbgpu_ctx* ctx) {
     return MPLBGPU_OK;
 }
 
+// The launches of one step that depend on nothing else of the step - each
+// block's step kernel and each block's deferred-node kernels read only the
+// previous array and write disjoint nodes of the new one - go round-robin
+// over the context's stream and its side streams (forked after the previous
+// step's halos, joined before this step's), so that one launch's tail
+// overlaps the next one's start.
 template <int D, typename T>
 int StepOnce(mplbgpu_ctx* ctx) {
     if (ctx->plan.swap) return SwapStepOnce<D, T>(ctx);
     const int src = ctx->cur, dst = 1 - ctx->cur;
     ctx->pc.seed = (uint32_t)(++ctx->step_count);
+    const int lanes = ctx->nlanes;
+    if (lanes > 1) {
+        CK(cudaEventRecord(ctx->fork, ctx->stream));
+        for (int k = 0; k < lanes - 1; k++)
+            CK(cudaStreamWaitEvent(ctx->side[k], ctx->fork, 0));
+    }
+    int lane = 0;
+    auto next = [&]() {
+        cudaStream_t st = lane == 0 ? ctx->stream : ctx->side[lane - 1];
+        lane = (lane + 1) % lanes;
+        return st;
+    };
     for (size_t bi = 0; bi < ctx->blocks.size(); bi++) {
         DevBlock& b = ctx->blocks[bi];
         const BlockPlan& B = ctx->plan.blocks[bi];
         const T* s = static_cast<const T*>(b.pop[src]);
         T* d = static_cast<T*>(b.pop[dst]);
-        CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D), ctx->stream,
+        CK_LAUNCH_E(Launch<D, T>::Step(kModeStep, NodeGrid(B, D), next(),
                                        b.dev, ctx->pc, s, d, nullptr, nullptr,
                                        nullptr, nullptr));
         if (B.ndeferred > 0 && b.dev.deferred_fused) {
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
-            CK_LAUNCH_E(Launch<D, T>::DeferredFused(g, ctx->stream, b.dev,
-                                                    ctx->pc, s, d));
+            CK_LAUNCH_E(Launch<D, T>::DeferredFused(g, next(), b.dev, ctx->pc,
+                                                    s, d));
         } else if (B.ndeferred > 0) {
+            // the per-boundary programme: its kernels in order on one stream
+            cudaStream_t st = next();
             const unsigned g = (unsigned)((B.ndeferred + kThreads - 1) / kThreads);
-            CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, ctx->stream, b.dev,
-                                                     ctx->pc, s));
+            CK_LAUNCH_E(Launch<D, T>::DeferredStream(g, st, b.dev, ctx->pc, s));
             for (auto& dop : b.dops) {
                 const unsigned gd =
                     (unsigned)((dop.total + kThreads - 1) / kThreads);
-                CK_LAUNCH_E(Launch<D, T>::DeferredOp(gd, ctx->stream, b.dev,
-                                                     ctx->pc, s, dop.segs,
-                                                     dop.nseg, dop.total));
+                CK_LAUNCH_E(Launch<D, T>::DeferredOp(gd, st, b.dev, ctx->pc, s,
+                                                     dop.segs, dop.nseg,
+                                                     dop.total));
             }
-            CK_LAUNCH_E(Launch<D, T>::DeferredFinish(
-                kModeStep, g, ctx->stream, b.dev, ctx->pc, d, nullptr, nullptr,
-                nullptr, nullptr));
+            CK_LAUNCH_E(Launch<D, T>::DeferredFinish(kModeStep, g, st, b.dev,
+                                                     ctx->pc, d, nullptr,
+                                                     nullptr, nullptr,
+                                                     nullptr));
+        }
+    }
+    if (lanes > 1) {
+        for (int k = 0; k < lanes - 1; k++) {
+            CK(cudaEventRecord(ctx->join[k], ctx->side[k]));
+            CK(cudaStreamWaitEvent(ctx->stream, ctx->join[k], 0));
         }
     }
     ctx->cur = dst;
@@ -523,6 +561,25 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess ||
         (e = cudaEventCreate(&c->ev1)) != cudaSuccess)
         return fail_cuda(e, "cudaEventCreate");
+    {
+        // independent launches per step: every block's step kernel and
+        // every block's deferred kernels (two-array scheme)
+        int indep = 0;
+        for (const BlockPlan& B : P.blocks) indep += 1 + (B.ndeferred > 0);
+        c->nlanes = P.swap ? 1 : std::min(indep, mplbgpu_ctx::kSides + 1);
+        for (int k = 0; k < c->nlanes - 1; k++)
+            if ((e = cudaStreamCreateWithFlags(&c->side[k],
+                                               cudaStreamNonBlocking)) !=
+                    cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&c->join[k],
+                                              cudaEventDisableTiming)) !=
+                    cudaSuccess)
+                return fail_cuda(e, "side streams");
+        if (c->nlanes > 1 &&
+            (e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) !=
+                cudaSuccess)
+            return fail_cuda(e, "side streams");
+    }
     c->blocks.resize(P.blocks.size());
     c->initialised.assign(P.blocks.size(), false);
     const int Q = P.Q;
