@@ -43,15 +43,17 @@ BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
                   ("fp32", 2): 72, ("fp16", 3): 76, ("fp16", 2): 36}
 # DRAM bytes per node update of the step kernel measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum of SplitStepKernel on the
-# 192^3 cavity, whose population arrays (1.08 GB FP64, 0.54 GB FP32) are
-# well beyond the 126 MB L2; mean of 2 launches over 7,077,888 nodes:
-# FP64 2,152.4 MB = 304.1 B, FP32 1,088.2 MB = 153.7 B), captured with
+# 192^3 cavity, whose population arrays (1.08 GB FP64, 0.54 GB FP32,
+# 0.27 GB FP16) are well beyond the 126 MB L2; mean of 2 launches over
+# 7,077,888 nodes: FP64 2,152.4 MB = 304.1 B, FP32 1,087.0 MB = 153.6 B,
+# FP16 554.8 MB = 78.4 B), captured with
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,
 # gpu__time_duration.sum --clock-control none -k regex:SplitStepKernel -s 3
 # -c 2 python bench.py --size 192 --steps 10 --warmup 3 --no-cpu-baseline
-# --no-forms --min-time 0 --precision fp64|fp32`.  Traffic grows with the
-# node count, so a 256^3 launch moves this x 16,777,216 bytes.
-TRAFFIC_PER_NODE = {("fp64", 3): 304.1, ("fp32", 3): 153.7}
+# --no-forms --min-time 0 --precision fp64|fp32|fp16`.  Traffic grows with
+# the node count, so a 256^3 launch moves this x 16,777,216 bytes.
+TRAFFIC_PER_NODE = {("fp64", 3): 304.1, ("fp32", 3): 153.6,
+                    ("fp16", 3): 78.4}
 METRIC = "MLUPS (D3Q19 3D lid-driven cavity 256^3)"
 DTYPES = {"fp64": "f64", "fp32": "f32 (shifted f - w)",
           "fp16": "f16 storage of (f - w)/w, f32 arithmetic"}
