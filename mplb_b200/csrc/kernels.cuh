@@ -849,9 +849,12 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
 #ifndef MPLB_LP_GROUP
 #define MPLB_LP_GROUP 2
 #endif
+#ifndef MPLB_F64_GROUP
+#define MPLB_F64_GROUP 1
+#endif
 template <typename T>
 __host__ __device__ constexpr int SplitGroup() {
-    return sizeof(T) < 8 ? MPLB_LP_GROUP : 1;
+    return sizeof(T) < 8 ? MPLB_LP_GROUP : MPLB_F64_GROUP;
 }
 
 // G interior nodes of one row held by one thread: their populations, their
@@ -885,7 +888,8 @@ __device__ __forceinline__ void GroupLoad(const BlockDev& b,
     }
 }
 
-// Moments, collision and stores of the valid nodes of a loaded group.
+// Moments, collision and stores of the valid nodes of a loaded group, one
+// node at a time (the shifted forms' pairs are PurePair's).
 template <int D, typename T, bool O32, int G>
 __device__ __forceinline__ void GroupFinish(const BlockDev& b,
                                             const PhysConst& pc,
@@ -895,54 +899,20 @@ __device__ __forceinline__ void GroupFinish(const BlockDev& b,
     using P = Prec<T>;
     constexpr int Q = L::Q;
     const bool fl = b.center_fluid != 0;
-    // shifted forms: the two nodes collide together (paired FP32
-    // instructions); a node outside the row computes on its copy of the
-    // other's values and is not stored
-    constexpr bool kPair = P::kShifted && G == 2;
-    if constexpr (kPair) MomentsCollidePair<L>(n.f[0], n.f[1], pc, fl, pc.omcf);
-    if constexpr (std::is_same<T, __half>::value && G == 2) {
-        // FP16 pairs: population i of the two converted together by the
-        // hardware's stochastic rounding (cvt.rs.f16x2.f32 with 32 random
-        // bits per pair)
-        // the first valid node's index, without a dynamic array index
-        long long seed_node = n.node[0];
 #pragma unroll
-        for (int j = 1; j < G; j++)
-            if (j == n.first) seed_node = n.node[j];
-        const Rng rg = SeedRng(pc.seed, seed_node);
+    for (int j = 0; j < G; j++) {
+        if (!n.valid[j]) continue;
+        MomentsCollideT<L, T>(n.f[j], pc, fl);
+        Rng rg = SeedRng(pc.seed, n.node[j]);
+        if constexpr (O32) {
+            T* pd = dst + n.node[j];
 #pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const uint32_t pair = StochasticHalf2(n.f[0][i] * pc.winvf[i],
-                                                  n.f[1][i] * pc.winvf[i],
-                                                  SrDraw32(rg, i));
-            const long long k0 = O32 ? n.node[0] + b.pop_off32[i]
-                                     : OwnIndex(b, n.node[0], i);
-            const long long k1 = O32 ? n.node[1] + b.pop_off32[i]
-                                     : OwnIndex(b, n.node[1], i);
-            if (n.valid[0])
-                PopStore(dst + k0,
-                         __ushort_as_half((unsigned short)(pair & 0xffffu)));
-            if (n.valid[1])
-                PopStore(dst + k1,
-                         __ushort_as_half((unsigned short)(pair >> 16)));
-        }
-    } else {
+            for (int i = 0; i < Q; i++)
+                P::Store(pd, b.pop_off32[i], i, n.f[j][i], pc, rg);
+        } else {
 #pragma unroll
-        for (int j = 0; j < G; j++) {
-            if (!n.valid[j]) continue;
-            if constexpr (!kPair) MomentsCollideT<L, T>(n.f[j], pc, fl);
-            Rng rg = SeedRng(pc.seed, n.node[j]);
-            if constexpr (O32) {
-                T* pd = dst + n.node[j];
-#pragma unroll
-                for (int i = 0; i < Q; i++)
-                    P::Store(pd, b.pop_off32[i], i, n.f[j][i], pc, rg);
-            } else {
-#pragma unroll
-                for (int i = 0; i < Q; i++)
-                    P::Store(dst, OwnIndex(b, n.node[j], i), i, n.f[j][i], pc,
-                             rg);
-            }
+            for (int i = 0; i < Q; i++)
+                P::Store(dst, OwnIndex(b, n.node[j], i), i, n.f[j][i], pc, rg);
         }
     }
 }
@@ -953,8 +923,8 @@ __device__ __forceinline__ void GroupFinish(const BlockDev& b,
 // outside [1, n0 - 2] is computed on whatever its place holds (an x face, a
 // halo column, the row padding, the next row or the slack after the last
 // population, all inside the allocation) and not stored; the pair's element
-// indices stay 32 apart, so one address serves both.  Same bits as
-// MomentsCollidePair on the two nodes.
+// indices stay 32 apart, so one address serves both.  Same bits as the
+// single-node collision of each.
 template <int D, typename T, bool O32>
 __device__ __forceinline__ void PurePair(const BlockDev& b,
                                          const PhysConst& pc,
@@ -1028,22 +998,22 @@ __device__ __forceinline__ void PureNodeGroup(const BlockDev& b,
                                               int y, int z) {
     if constexpr (Prec<T>::kShifted && G == 2) {
         PurePair<D, T, O32>(b, pc, src, dst, x0, y, z);
-        return;
-    }
-    NodeGroup<D, T, G> n;
-    n.first = -1;
+    } else {
+        NodeGroup<D, T, G> n;
+        n.first = -1;
 #pragma unroll
-    for (int j = 0; j < G; j++) {
-        const int x = x0 + 32 * j;
-        n.valid[j] = x >= 1 && x <= b.n[0] - 2;
-        if (n.valid[j] && n.first < 0) n.first = j;
-    }
-    if (n.first < 0) return;
-    n.node[0] = NodeIndexT<D, O32>(b, x0, y, z);
+        for (int j = 0; j < G; j++) {
+            const int x = x0 + 32 * j;
+            n.valid[j] = x >= 1 && x <= b.n[0] - 2;
+            if (n.valid[j] && n.first < 0) n.first = j;
+        }
+        if (n.first < 0) return;
+        n.node[0] = NodeIndexT<D, O32>(b, x0, y, z);
 #pragma unroll
-    for (int j = 1; j < G; j++) n.node[j] = n.node[0] + 32 * j;
-    GroupLoad<D, T, O32, G>(b, pc, src, n);
-    GroupFinish<D, T, O32, G>(b, pc, dst, n);
+        for (int j = 1; j < G; j++) n.node[j] = n.node[0] + 32 * j;
+        GroupLoad<D, T, O32, G>(b, pc, src, n);
+        GroupFinish<D, T, O32, G>(b, pc, dst, n);
+    }
 }
 
 // Rows of interior nodes handled per x-face block of SplitStepKernel.
