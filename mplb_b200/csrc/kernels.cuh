@@ -53,6 +53,7 @@ struct PhysConst {
     float tw_omf;        // tau omega / omega: the force term relative to
                          // the relaxation rate
     float wf[kMaxQ];
+    float cf256f[kMaxQ]; // kHalfScale CS c_i . a (FP16 pairs' force term)
     float winvf[kMaxQ];  // FP16 store scale kHalfScale / w_i
     float wlf[kMaxQ];    // FP16 load scale w_i / kHalfScale
     uint32_t seed;       // per launch (FP16 stochastic rounding)
@@ -917,6 +918,119 @@ __device__ __forceinline__ void GroupFinish(const BlockDev& b,
     }
 }
 
+// Moments and collision of an FP16 node pair on the stored values
+// themselves, s_i = kHalfScale h_i / w_i (one node per half of each float2):
+// the same steps as MomentsShiftedV and CollideShiftedV (opposite pairs
+// summed first, heq whole per direction, the mass and momentum
+// projection), with each h_i = (w_i / kHalfScale) s_i and m_i taken into
+// the sums as multiply-adds by w_i / kHalfScale, and the equilibrium and
+// the update written for s directly - there the equilibrium carries no
+// weight (s_eq,i = kHalfScale [drho + rho (cu + (cu^2 - u^2) / 2)]), so
+// neither the loads nor the stores scale the populations.
+template <typename L>
+__device__ __forceinline__ void MomentsCollideScaledPair(float2* s,
+                                                         const PhysConst& pc,
+                                                         bool fluidlike) {
+    using O = VOps<float2>;
+    constexpr int Q = L::Q;
+    auto wl = [&](int i) { return O::splat(pc.wlf[i]); };
+    // moments
+    float2 drho = O::mul(s[0], wl(0));
+#pragma unroll
+    for (int i = 1; i < Q; i++)
+        if (i < L::opp(i))
+            drho = O::fma(O::add(s[i], s[L::opp(i)]), wl(i), drho);
+    const float2 rho = O::add(O::splat(1.0f), drho);
+    const float2 rinv = O::rcp(rho);
+    float2 u[3];
+#pragma unroll
+    for (int a = 0; a < L::D; a++) {
+        float2 j = O::splat(0.0f);
+        bool first = true;
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            if (comp<L>(i, a) > 0) {
+                const float2 d = O::sub(s[i], s[L::opp(i)]);
+                j = first ? O::mul(d, wl(i)) : O::fma(d, wl(i), j);
+                first = false;
+            }
+        }
+        j = O::mul(O::mul(O::splat(pc.csf), j), rinv);
+        if (pc.force_vel && fluidlike) j = O::add(j, O::splat(pc.hdtaf[a]));
+        u[a] = j;
+    }
+    if (L::D == 2) u[2] = O::splat(0.0f);
+    // collision: ms_i = s_i - s_eq,i, M0 = sum m_i, M = sum c_i m_i
+    const float2 hr = O::mul(O::splat(0.5f), rho);
+    const float2 csf = O::splat(pc.csf);
+    const float2 cu0 = O::mul(csf, u[0]), cu1 = O::mul(csf, u[1]),
+                 cu2 = O::mul(csf, u[2]);
+    const float2 u2 =
+        O::fma(u[0], u[0], O::fma(u[1], u[1], O::mul(u[2], u[2])));
+    const float2 half = O::splat(0.5f);
+    const float2 nscale = O::splat(-kHalfScale);
+    float2 m[Q];
+    m[0] = O::fma(nscale, O::fma(O::neg(hr), u2, drho), s[0]);
+    float2 m0 = O::mul(m[0], wl(0)), mv0 = O::splat(0.0f),
+           mv1 = O::splat(0.0f), mv2 = O::splat(0.0f);
+#pragma unroll
+    for (int i = 1; i < Q; i++) {
+        if (i > L::opp(i)) continue;
+        const int j = L::opp(i);
+        float2 cu = O::splat(0.0f);
+        bool first = true;
+        const float2 comps[3] = {cu0, cu1, cu2};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const int c = comp<L>(i, a);
+            if (c == 0 || a >= L::D) continue;
+            const float2 t = c > 0 ? comps[a] : O::neg(comps[a]);
+            cu = first ? t : O::add(cu, t);
+            first = false;
+        }
+        const float2 y = O::fma(cu, cu, O::neg(u2));
+        m[i] = O::fma(nscale, O::fma(rho, O::fma(half, y, cu), drho), s[i]);
+        m[j] = O::fma(nscale, O::fma(rho, O::fma(half, y, O::neg(cu)), drho),
+                      s[j]);
+        m0 = O::fma(O::add(m[i], m[j]), wl(i), m0);
+        const float2 d = O::mul(O::sub(m[i], m[j]), wl(i));
+        if (L::cx(i) > 0) mv0 = O::add(mv0, d);
+        if (L::cx(i) < 0) mv0 = O::sub(mv0, d);
+        if (L::cy(i) > 0) mv1 = O::add(mv1, d);
+        if (L::cy(i) < 0) mv1 = O::sub(mv1, d);
+        if (L::cz(i) > 0) mv2 = O::add(mv2, d);
+        if (L::cz(i) < 0) mv2 = O::sub(mv2, d);
+    }
+    if (pc.force_vel && fluidlike) {
+        mv0 = O::fma(rho, O::splat(pc.hdta_csf[0]), mv0);
+        mv1 = O::fma(rho, O::splat(pc.hdta_csf[1]), mv1);
+        mv2 = O::fma(rho, O::splat(pc.hdta_csf[2]), mv2);
+    }
+    const float2 three = O::splat(3.0f);
+    mv0 = O::mul(mv0, three);
+    mv1 = O::mul(mv1, three);
+    mv2 = O::mul(mv2, three);
+    // s'_i = s_i + omega (kHalfScale (M0 + 3 c_i . M) - ms_i
+    //                     + kHalfScale F_i / (omega w_i))
+    const float2 om = O::splat(1.0f - pc.omcf);
+    const bool force = pc.force && fluidlike;
+    const float2 fr = O::mul(O::splat(pc.tw_omf), rho);
+    const float2 scale = O::splat(kHalfScale);
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        float2 cm = m0;
+        if (L::cx(i) > 0) cm = O::add(cm, mv0);
+        if (L::cx(i) < 0) cm = O::sub(cm, mv0);
+        if (L::cy(i) > 0) cm = O::add(cm, mv1);
+        if (L::cy(i) < 0) cm = O::sub(cm, mv1);
+        if (L::cz(i) > 0) cm = O::add(cm, mv2);
+        if (L::cz(i) < 0) cm = O::sub(cm, mv2);
+        float2 t = O::fma(scale, cm, O::neg(m[i]));
+        if (force) t = O::fma(fr, O::splat(pc.cf256f[i]), t);
+        s[i] = O::fma(om, t, s[i]);
+    }
+}
+
 // The shifted forms' node pair x0, x0 + 32 of one interior row, held
 // population by population in float2 registers from the loads through the
 // paired collision to the stores (no packing between the two).  A node
@@ -944,19 +1058,21 @@ __device__ __forceinline__ void PurePair(const BlockDev& b,
         const long long k = O32 ? node + b.pull_off32[i]
                                 : PullIndex<L>(b, node, i);
         if constexpr (std::is_same<T, __half>::value) {
-            // both scaled by one paired multiply (the same rounding as two)
-            h[i] = __fmul2_rn(make_float2(__half2float(src[k]),
-                                          __half2float(src[k + 32])),
-                              make_float2(pc.wlf[i], pc.wlf[i]));
+            // the stored values themselves (MomentsCollideScaledPair)
+            h[i] = make_float2(__half2float(src[k]), __half2float(src[k + 32]));
         } else {
             h[i] = make_float2(P::Load(src, k, i, pc),
                                P::Load(src, k + 32, i, pc));
         }
     }
     const bool fl = b.center_fluid != 0;
-    float2 drho, u[3];
-    MomentsShiftedV<L, float2>(h, pc, fl, drho, u);
-    CollideShiftedV<L, float2>(h, pc, fl, drho, u, pc.omcf);
+    if constexpr (std::is_same<T, __half>::value) {
+        MomentsCollideScaledPair<L>(h, pc, fl);
+    } else {
+        float2 drho, u[3];
+        MomentsShiftedV<L, float2>(h, pc, fl, drho, u);
+        CollideShiftedV<L, float2>(h, pc, fl, drho, u, pc.omcf);
+    }
     if constexpr (std::is_same<T, __half>::value) {
         // population i of the two converted together by the hardware's
         // stochastic rounding (cvt.rs.f16x2.f32, 32 random bits per pair
@@ -964,9 +1080,8 @@ __device__ __forceinline__ void PurePair(const BlockDev& b,
         const Rng rg = SeedRng(pc.seed, v0 ? node : node + 32);
 #pragma unroll
         for (int i = 0; i < Q; i++) {
-            const float2 sv =
-                __fmul2_rn(h[i], make_float2(pc.winvf[i], pc.winvf[i]));
-            const uint32_t pair = StochasticHalf2(sv.x, sv.y, SrDraw32(rg, i));
+            const uint32_t pair =
+                StochasticHalf2(h[i].x, h[i].y, SrDraw32(rg, i));
             const long long k = O32 ? node + b.pop_off32[i]
                                     : OwnIndex(b, node, i);
             if (v0)

@@ -538,7 +538,10 @@ mplbgpu_status mplbgpu_create(const mplbgpu_desc* desc, mplbgpu_ctx** out) {
     pc.twf = (float)P.tw;
     for (int a = 0; a < 3; a++) pc.hdtaf[a] = (float)P.hdta[a];
     for (int a = 0; a < 3; a++) pc.hdta_csf[a] = (float)(P.hdta[a] / P.cs);
-    for (int i = 0; i < kMaxQ; i++) pc.wcff[i] = (float)(P.w[i] * P.cf[i]);
+    for (int i = 0; i < kMaxQ; i++) {
+        pc.wcff[i] = (float)(P.w[i] * P.cf[i]);
+        pc.cf256f[i] = (float)(kHalfScale * P.cf[i]);
+    }
     pc.tw_omf = (float)(P.tw / (1.0 - P.omc));
     if (P.swap) {
         // KerSwapCalcBodyForce1ST3D adds the first-order force term itself
