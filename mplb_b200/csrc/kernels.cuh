@@ -1031,6 +1031,49 @@ __device__ __forceinline__ void MomentsCollideScaledPair(float2* s,
     }
 }
 
+// Collision and stores of a shifted-form node pair whose populations are
+// loaded, population by population, in float2 registers (node, node + 32).
+template <int D, typename T, bool O32>
+__device__ __forceinline__ void PairFinish(const BlockDev& b,
+                                           const PhysConst& pc,
+                                           T* __restrict__ dst, long long node,
+                                           bool v0, bool v1, float2* h) {
+    using L = Lattice<D>;
+    constexpr int Q = L::Q;
+    const bool fl = b.center_fluid != 0;
+    if constexpr (std::is_same<T, __half>::value) {
+        MomentsCollideScaledPair<L>(h, pc, fl);
+        // population i of the two converted together by the hardware's
+        // stochastic rounding (cvt.rs.f16x2.f32, 32 random bits per pair
+        // from the first valid node's draw)
+        const Rng rg = SeedRng(pc.seed, v0 ? node : node + 32);
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const uint32_t pair =
+                StochasticHalf2(h[i].x, h[i].y, SrDraw32(rg, i));
+            const long long k = O32 ? node + b.pop_off32[i]
+                                    : OwnIndex(b, node, i);
+            if (v0)
+                PopStore(dst + k,
+                         __ushort_as_half((unsigned short)(pair & 0xffffu)));
+            if (v1)
+                PopStore(dst + k + 32,
+                         __ushort_as_half((unsigned short)(pair >> 16)));
+        }
+    } else {
+        float2 drho, u[3];
+        MomentsShiftedV<L, float2>(h, pc, fl, drho, u);
+        CollideShiftedV<L, float2>(h, pc, fl, drho, u, pc.omcf);
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            const long long k = O32 ? node + b.pop_off32[i]
+                                    : OwnIndex(b, node, i);
+            if (v0) PopStore(dst + k, (T)h[i].x);
+            if (v1) PopStore(dst + k + 32, (T)h[i].y);
+        }
+    }
+}
+
 // The shifted forms' node pair x0, x0 + 32 of one interior row, held
 // population by population in float2 registers from the loads through the
 // paired collision to the stores (no packing between the two).  A node
@@ -1038,7 +1081,8 @@ __device__ __forceinline__ void MomentsCollideScaledPair(float2* s,
 // halo column, the row padding, the next row or the slack after the last
 // population, all inside the allocation) and not stored; the pair's element
 // indices stay 32 apart, so one address serves both.  Same bits as the
-// single-node collision of each.
+// single-node collision of each (FP32; FP16 pairs collide on their stored
+// values, MomentsCollideScaledPair).
 template <int D, typename T, bool O32>
 __device__ __forceinline__ void PurePair(const BlockDev& b,
                                          const PhysConst& pc,
@@ -1065,41 +1109,7 @@ __device__ __forceinline__ void PurePair(const BlockDev& b,
                                P::Load(src, k + 32, i, pc));
         }
     }
-    const bool fl = b.center_fluid != 0;
-    if constexpr (std::is_same<T, __half>::value) {
-        MomentsCollideScaledPair<L>(h, pc, fl);
-    } else {
-        float2 drho, u[3];
-        MomentsShiftedV<L, float2>(h, pc, fl, drho, u);
-        CollideShiftedV<L, float2>(h, pc, fl, drho, u, pc.omcf);
-    }
-    if constexpr (std::is_same<T, __half>::value) {
-        // population i of the two converted together by the hardware's
-        // stochastic rounding (cvt.rs.f16x2.f32, 32 random bits per pair
-        // from the first valid node's draw)
-        const Rng rg = SeedRng(pc.seed, v0 ? node : node + 32);
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const uint32_t pair =
-                StochasticHalf2(h[i].x, h[i].y, SrDraw32(rg, i));
-            const long long k = O32 ? node + b.pop_off32[i]
-                                    : OwnIndex(b, node, i);
-            if (v0)
-                PopStore(dst + k,
-                         __ushort_as_half((unsigned short)(pair & 0xffffu)));
-            if (v1)
-                PopStore(dst + k + 32,
-                         __ushort_as_half((unsigned short)(pair >> 16)));
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            const long long k = O32 ? node + b.pop_off32[i]
-                                    : OwnIndex(b, node, i);
-            if (v0) PopStore(dst + k, (T)h[i].x);
-            if (v1) PopStore(dst + k + 32, (T)h[i].y);
-        }
-    }
+    PairFinish<D, T, O32>(b, pc, dst, node, v0, v1, h);
 }
 
 // The G nodes x0 + 32 j (j < G) of one interior row (the shifted forms'
@@ -1136,6 +1146,53 @@ constexpr int kSplitRows = 64;
 constexpr int kSplitCta = 128;   // threads per CTA of SplitStepKernel
 constexpr int kSplitWarps = kSplitCta / 32;
 
+// Staged interior of the shifted forms.  Each warp takes kStageTasks
+// consecutive 64-node row segments and runs them through a pipeline of
+// StageDepth<T>() shared-memory stages: while it computes one segment, the
+// copies of the next segments' 19 source windows are in flight (16-byte
+// cp.async copies into shared memory, which take no registers), so a warp
+// keeps several segments' bytes in flight where the per-thread loads keep
+// one.  A window is the row segment x - c_x needs, widened to 16-byte
+// boundaries: columns [xs - StageLead, xs + 64 + StageLead).
+#ifndef MPLB_LP_STAGED
+#define MPLB_LP_STAGED 1
+#endif
+#ifndef MPLB_STAGE_TASKS
+#define MPLB_STAGE_TASKS 8
+#endif
+constexpr int kStageTasks = MPLB_STAGE_TASKS;
+template <typename T>
+__host__ __device__ constexpr int StageLead() {   // 16 bytes of elements
+    return 16 / (int)sizeof(T);
+}
+template <typename T>
+__host__ __device__ constexpr int StageWinElems() {
+    return 64 + 2 * StageLead<T>();
+}
+#ifndef MPLB_STAGE_DEPTH
+#define MPLB_STAGE_DEPTH 2
+#endif
+template <typename T>
+__host__ __device__ constexpr int StageDepth() {
+    return MPLB_STAGE_DEPTH;
+}
+template <int D, typename T>
+__host__ __device__ constexpr int StageSmemBytes() {
+    return kSplitWarps * StageDepth<T>() * Lattice<D>::Q * StageWinElems<T>() *
+           (int)sizeof(T);
+}
+// The FP16 form only: its 2-byte loads keep half the FP32 form's bytes in
+// flight per warp, and the staged interior runs it 9-11 % faster at 256^3
+// (341-347 us against 382 us; 8 segments per warp in 2 stages, or 4 in 3,
+// or 2 in 3: within 2 % of each other); the FP32 form, which needs 2.6 KB
+// more per stage, ran 25 % slower staged.
+template <typename T>
+__host__ __device__ constexpr bool StagedStep() {
+    return MPLB_LP_STAGED != 0 && std::is_same<T, __half>::value &&
+           SplitGroup<T>() == 2;
+}
+
+
 // Interior "warp tasks": 32 G consecutive nodes of a row per warp; CTA c of
 // a chunk's interior takes tasks kSplitWarps c .. + kSplitWarps - 1.
 struct SplitTask {
@@ -1154,12 +1211,111 @@ __device__ __forceinline__ SplitTask InteriorTask(const BlockDev& b,
     return k;
 }
 
-// CTAs of one chunk: the x-face CTA and the interior CTAs.
-template <int G>
+// CTAs of one chunk: the x-face CTA and the interior CTAs (a warp takes
+// one task, or kStageTasks with the staged interior).
+template <int G, bool STAGED = false>
 __host__ __device__ constexpr long long SplitChunkCtas(int n0) {
     return 1 + ((long long)kSplitRows * ((n0 + 32 * G - 1) / (32 * G)) +
-                kSplitWarps - 1) /
-                   kSplitWarps;
+                kSplitWarps * (STAGED ? kStageTasks : 1) - 1) /
+                   (kSplitWarps * (STAGED ? kStageTasks : 1));
+}
+
+__device__ __forceinline__ void CpAsync16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void CpAsyncCommit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void CpAsyncWait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// The staged interior of one CTA of a chunk (see StagedStep): warp k takes
+// the chunk's tasks (w - 1) kSplitWarps kStageTasks + k kStageTasks + t,
+// t < kStageTasks (task -> row t / tasks per row, segment t % tasks per
+// row).  Lane l computes the pair l, l + 32 of the segment (PairFinish).
+template <int D, typename T, bool O32>
+__device__ __forceinline__ void StagedInterior(const BlockDev& b,
+                                               const PhysConst& pc,
+                                               const T* __restrict__ src,
+                                               T* __restrict__ dst, int chunk,
+                                               int w, int rows, int ny) {
+    using L = Lattice<D>;
+    constexpr int Q = L::Q;
+    constexpr int S = StageDepth<T>();
+    constexpr int kWin = StageWinElems<T>();
+    constexpr int kLead = StageLead<T>();
+    constexpr int kChunks = kWin * (int)sizeof(T) / 16;   // 16-byte copies
+    static_assert(kChunks <= 32, "one copy per lane and population");
+    extern __shared__ __align__(16) unsigned char stage_raw[];
+    const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+    T* stages = reinterpret_cast<T*>(stage_raw) + warp * S * Q * kWin;
+    const int tpr = (b.n[0] + 63) / 64;
+    const int t0 = ((w - 1) * kSplitWarps + warp) * kStageTasks;
+    // task t of this warp: its row (or -1) and first column
+    auto task = [&](int t, int& r, int& xs) {
+        const int g = t0 + t;
+        const int rl = g / tpr;
+        r = (t < kStageTasks && rl < kSplitRows &&
+             chunk * kSplitRows + rl < rows)
+                ? chunk * kSplitRows + rl
+                : -1;
+        xs = (g - rl * tpr) * 64;
+    };
+    // copies of task t's windows into stage st (one group, maybe empty)
+    auto issue = [&](int t, int st) {
+        int r, xs;
+        task(t, r, xs);
+        if (r >= 0 && lane < kChunks) {
+            const long long node = NodeIndexT<D, O32>(
+                b, xs, 1 + r % ny, D == 3 ? 1 + r / ny : 0);
+            T* win = stages + st * Q * kWin;
+#pragma unroll
+            for (int i = 0; i < Q; i++) {
+                const long long k0 =
+                    (O32 ? node + b.pull_off32[i] : PullIndex<L>(b, node, i)) +
+                    L::cx(i) - kLead;
+                CpAsync16(win + i * kWin + lane * (16 / (int)sizeof(T)),
+                          src + k0 + lane * (16 / (int)sizeof(T)));
+            }
+        }
+        CpAsyncCommit();
+    };
+#pragma unroll
+    for (int t = 0; t < S - 1; t++) issue(t, t);
+    for (int t = 0; t < kStageTasks; t++) {
+        issue(t + S - 1, (t + S - 1) % S);
+        CpAsyncWait<S - 1>();
+        __syncwarp();
+        int r, xs;
+        task(t, r, xs);
+        if (r >= 0) {
+            const int x0 = xs + lane;
+            const bool v0 = x0 >= 1 && x0 <= b.n[0] - 2;
+            const bool v1 = x0 + 32 >= 1 && x0 + 32 <= b.n[0] - 2;
+            if (v0 || v1) {
+                const T* win = stages + (t % S) * Q * kWin + lane + kLead;
+                float2 h[Q];
+#pragma unroll
+                for (int i = 0; i < Q; i++) {
+                    const T* p = win + i * kWin - L::cx(i);
+                    if constexpr (std::is_same<T, __half>::value)
+                        h[i] = make_float2(__half2float(p[0]),
+                                           __half2float(p[32]));
+                    else
+                        h[i] = make_float2((float)p[0], (float)p[32]);
+                }
+                const long long node = NodeIndexT<D, O32>(
+                    b, x0, 1 + r % ny, D == 3 ? 1 + r / ny : 0);
+                PairFinish<D, T, O32>(b, pc, dst, node, v0, v1, h);
+            }
+        }
+        __syncwarp();   // every lane is done with stage t % S
+    }
 }
 
 // The step with no warp mixing interior and boundary nodes (a warp holding
@@ -1211,7 +1367,8 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     blk -= nsr;
     const int rows = ny * (D == 3 ? b.n[2] - 2 : 1);
     constexpr int G = SplitGroup<T>();
-    const unsigned per_chunk = (unsigned)SplitChunkCtas<G>(b.n[0]);
+    constexpr bool kStaged = StagedStep<T>();
+    const unsigned per_chunk = (unsigned)SplitChunkCtas<G, kStaged>(b.n[0]);
     const int chunk = (int)(blk / per_chunk);
     const int w = (int)(blk % per_chunk);
     if (w == 0) {
@@ -1223,10 +1380,14 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                        D == 3 ? 1 + r / ny : 0);
         return;
     }
-    const SplitTask k = InteriorTask<G>(b, chunk, w);
-    if (k.r < 0 || k.r >= rows) return;
-    PureNodeGroup<D, T, O32, G>(b, pc, src, dst, k.x0, 1 + k.r % ny,
-                                D == 3 ? 1 + k.r / ny : 0);
+    if constexpr (kStaged) {
+        StagedInterior<D, T, O32>(b, pc, src, dst, chunk, w, rows, ny);
+    } else {
+        const SplitTask k = InteriorTask<G>(b, chunk, w);
+        if (k.r < 0 || k.r >= rows) return;
+        PureNodeGroup<D, T, O32, G>(b, pc, src, dst, k.x0, 1 + k.r % ny,
+                                    D == 3 ? 1 + k.r / ny : 0);
+    }
 }
 
 // Deferred nodes: thread t -> (region, node).

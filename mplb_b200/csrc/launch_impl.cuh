@@ -8,9 +8,13 @@
 namespace mplb {
 
 static_assert(kSplitCta == kStepThreads, "SplitStepKernel CTA size");
+static_assert(StageSmemBytes<3, __half>() <= 48 * 1024,
+              "staged interior within the default shared memory");
 
-// CTAs of SplitStepKernel / SplitSwapKernel for block b (0: too many).
-template <int D, typename T>
+// CTAs of SplitStepKernel (STAGED: with the staged interior of
+// StagedStep<T>()) or SplitSwapKernel (never staged) for block b (0: too
+// many).
+template <int D, typename T, bool STAGED = StagedStep<T>()>
 long long SplitBlocks(const BlockDev& b) {
     const long long nbx = (b.n[0] + kStepThreads - 1) / kStepThreads;
     const long long ny = b.n[1] - 2;
@@ -19,7 +23,7 @@ long long SplitBlocks(const BlockDev& b) {
     const long long nsr = nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
     const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
     const long long blocks =
-        nsr + chunks * SplitChunkCtas<SplitGroup<T>()>(b.n[0]);
+        nsr + chunks * SplitChunkCtas<SplitGroup<T>(), STAGED>(b.n[0]);
     return blocks > 0x7fffffffLL ? 0 : blocks;
 }
 
@@ -44,12 +48,13 @@ cudaError_t Launch<D, T>::StepPart(int part, cudaStream_t s, const BlockDev& b,
     const unsigned grid = (unsigned)(part == 1 ? blocks - shell : shell);
     const unsigned blk0 = part == 1 ? (unsigned)shell : 0u;
     if (grid == 0) return cudaSuccess;
+    const int smem = StagedStep<T>() ? StageSmemBytes<D, T>() : 0;
     if (b.off32)
-        SplitStepKernel<D, T, true><<<grid, kStepThreads, 0, s>>>(b, pc, src,
-                                                                  dst, blk0);
+        SplitStepKernel<D, T, true><<<grid, kStepThreads, smem, s>>>(
+            b, pc, src, dst, blk0);
     else
-        SplitStepKernel<D, T, false><<<grid, kStepThreads, 0, s>>>(b, pc, src,
-                                                                   dst, blk0);
+        SplitStepKernel<D, T, false><<<grid, kStepThreads, smem, s>>>(
+            b, pc, src, dst, blk0);
     return cudaGetLastError();
 }
 
@@ -61,12 +66,13 @@ cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
     if (mode == kModeStep && b.split) {
         const long long blocks = SplitBlocks<D, T>(b);
         if (blocks == 0) return cudaErrorInvalidConfiguration;
+        const int smem = StagedStep<T>() ? StageSmemBytes<D, T>() : 0;
         if (b.off32)
-            SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, 0, s>>>(
-                b, pc, src, dst, 0u);
+            SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, smem,
+                                          s>>>(b, pc, src, dst, 0u);
         else
-            SplitStepKernel<D, T, false><<<(unsigned)blocks, kStepThreads, 0, s>>>(
-                b, pc, src, dst, 0u);
+            SplitStepKernel<D, T, false><<<(unsigned)blocks, kStepThreads,
+                                           smem, s>>>(b, pc, src, dst, 0u);
     } else if (mode == kModeStep && b.off32)
         StepKernel<D, T, kModeStep, true><<<grid, kStepThreads, 0, s>>>(
             b, pc, src, dst, o0, o1, o2, o3);
@@ -180,7 +186,7 @@ cudaError_t Launch<D, T>::HaloFused(cudaStream_t s, const HaloFusedDev& h,
 template <typename T, bool GATHER, bool BC, bool O32>
 cudaError_t LaunchSplitSwap(cudaStream_t s, const BlockDev& b,
                             const PhysConst& pc, T* f) {
-    const long long blocks = SplitBlocks<3, T>(b);
+    const long long blocks = SplitBlocks<3, T, false>(b);
     if (blocks == 0) return cudaErrorInvalidConfiguration;
     SplitSwapKernel<T, GATHER, BC, O32><<<(unsigned)blocks, kStepThreads, 0,
                                           s>>>(b, pc, f);
