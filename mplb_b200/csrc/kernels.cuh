@@ -1338,15 +1338,34 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                            ? MPLB_F64_MIN_BLOCKS
                                            : MPLB_LP_MIN_BLOCKS)
     SplitStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
-                    T* __restrict__ dst, unsigned blk0) {
+                    T* __restrict__ dst, unsigned blk0, unsigned spc) {
     // block and row counts fit in 32 bits (the launcher checks the grid),
     // so the index arithmetic stays 32-bit
     const int nbx = (b.n[0] + (int)blockDim.x - 1) / (int)blockDim.x;
     const int ny = b.n[1] - 2;
     const int nz = D == 3 ? b.n[2] : 1;
     const unsigned nsr = (unsigned)nbx * (2 * nz + (D == 3 ? 2 * ny : 0));
-    // blk0: a launch of the interior part alone starts after the shell rows
-    unsigned blk = blockIdx.x + blk0;
+    constexpr int G = SplitGroup<T>();
+    constexpr bool kStaged = StagedStep<T>();
+    const unsigned per_chunk = (unsigned)SplitChunkCtas<G, kStaged>(b.n[0]);
+    // CTA order: spc = 0, the shell rows first, then the chunks (blk0: a
+    // launch of the chunks alone starts after the shell rows); spc > 0, each
+    // chunk's CTAs followed by spc shell-row CTAs, so the shell rows' long
+    // boundary programmes run beside interior CTAs instead of in waves of
+    // their own at the start
+    unsigned blk;
+    if (spc > 0) {
+        const unsigned slot = blockIdx.x / (per_chunk + spc);
+        const unsigned r = blockIdx.x - slot * (per_chunk + spc);
+        if (r >= per_chunk) {
+            blk = slot * spc + (r - per_chunk);
+            if (blk >= nsr) return;
+        } else {
+            blk = nsr + slot * per_chunk + r;
+        }
+    } else {
+        blk = blockIdx.x + blk0;
+    }
     if (blk < nsr) {
         const int row = (int)(blk / nbx);
         const int x = (int)(blk % nbx) * blockDim.x + threadIdx.x;
@@ -1366,9 +1385,6 @@ __global__ void __launch_bounds__(128, std::is_same<T, double>::value
     }
     blk -= nsr;
     const int rows = ny * (D == 3 ? b.n[2] - 2 : 1);
-    constexpr int G = SplitGroup<T>();
-    constexpr bool kStaged = StagedStep<T>();
-    const unsigned per_chunk = (unsigned)SplitChunkCtas<G, kStaged>(b.n[0]);
     const int chunk = (int)(blk / per_chunk);
     const int w = (int)(blk % per_chunk);
     if (w == 0) {

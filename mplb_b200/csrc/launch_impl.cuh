@@ -51,10 +51,10 @@ cudaError_t Launch<D, T>::StepPart(int part, cudaStream_t s, const BlockDev& b,
     const int smem = StagedStep<T>() ? StageSmemBytes<D, T>() : 0;
     if (b.off32)
         SplitStepKernel<D, T, true><<<grid, kStepThreads, smem, s>>>(
-            b, pc, src, dst, blk0);
+            b, pc, src, dst, blk0, 0u);
     else
         SplitStepKernel<D, T, false><<<grid, kStepThreads, smem, s>>>(
-            b, pc, src, dst, blk0);
+            b, pc, src, dst, blk0, 0u);
     return cudaGetLastError();
 }
 
@@ -64,15 +64,27 @@ cudaError_t Launch<D, T>::Step(int mode, dim3 grid, cudaStream_t s,
                                const T* src, T* dst, double* o0, double* o1,
                                double* o2, double* o3) {
     if (mode == kModeStep && b.split) {
-        const long long blocks = SplitBlocks<D, T>(b);
-        if (blocks == 0) return cudaErrorInvalidConfiguration;
+        if (SplitBlocks<D, T>(b) == 0) return cudaErrorInvalidConfiguration;
+        // the shell rows interleaved with the chunks: spc of them after
+        // each chunk's CTAs
+        const long long nsr = SplitShellBlocks<D>(b);
+        const long long rows =
+            (long long)(b.n[1] - 2) * (D == 3 ? b.n[2] - 2 : 1);
+        const long long chunks = (rows + kSplitRows - 1) / kSplitRows;
+        const long long per_chunk =
+            SplitChunkCtas<SplitGroup<T>(), StagedStep<T>()>(b.n[0]);
+        const long long spc = (nsr + chunks - 1) / chunks;
+        const long long blocks = chunks * (per_chunk + spc);
+        if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
         const int smem = StagedStep<T>() ? StageSmemBytes<D, T>() : 0;
         if (b.off32)
             SplitStepKernel<D, T, true><<<(unsigned)blocks, kStepThreads, smem,
-                                          s>>>(b, pc, src, dst, 0u);
+                                          s>>>(b, pc, src, dst, 0u,
+                                               (unsigned)spc);
         else
             SplitStepKernel<D, T, false><<<(unsigned)blocks, kStepThreads,
-                                           smem, s>>>(b, pc, src, dst, 0u);
+                                           smem, s>>>(b, pc, src, dst, 0u,
+                                                      (unsigned)spc);
     } else if (mode == kModeStep && b.off32)
         StepKernel<D, T, kModeStep, true><<<grid, kStepThreads, 0, s>>>(
             b, pc, src, dst, o0, o1, o2, o3);
