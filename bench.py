@@ -46,14 +46,15 @@ BYTES_PER_NODE = {("fp64", 3): 304, ("fp64", 2): 144, ("fp32", 3): 152,
 # 192^3 cavity, whose population arrays (1.08 GB FP64, 0.54 GB FP32,
 # 0.27 GB FP16) are well beyond the 126 MB L2; mean of 2 launches over
 # 7,077,888 nodes: FP64 2,152.4 MB = 304.1 B, FP32 1,087.0 MB = 153.6 B,
-# FP16 554.8 MB = 78.4 B), captured with
+# FP16 585.8 MB = 82.8 B: its staged interior copies 16-byte-aligned
+# windows, 6 % above the per-thread loads' 78.4 B), captured with
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,
 # gpu__time_duration.sum --clock-control none -k regex:SplitStepKernel -s 3
 # -c 2 python bench.py --size 192 --steps 10 --warmup 3 --no-cpu-baseline
 # --no-forms --min-time 0 --precision fp64|fp32|fp16`.  Traffic grows with
 # the node count, so a 256^3 launch moves this x 16,777,216 bytes.
 TRAFFIC_PER_NODE = {("fp64", 3): 304.1, ("fp32", 3): 153.6,
-                    ("fp16", 3): 78.4}
+                    ("fp16", 3): 82.8}
 METRIC = "MLUPS (D3Q19 3D lid-driven cavity 256^3)"
 DTYPES = {"fp64": "f64", "fp32": "f32 (shifted f - w)",
           "fp16": "f16 storage of (f - w)/w, f32 arithmetic"}
@@ -822,10 +823,13 @@ def main():
             fb = BYTES_PER_NODE[(prec, 3)]
             fach = fb * nodes / (fms / args.steps * 1e-3) / 1e9
             fv = world * nodes * args.steps / (fms * 1e-3) / 1e6
+            ftr = TRAFFIC_PER_NODE.get((prec, 3))
             forms[key] = {"value": fv, "unit": "MLUPS",
                           "ms_per_step": fms / args.steps,
                           "vs_fp64": fv / value, "bytes_per_node": fb,
                           "achieved_gbs": fach, "frac": fach / peak,
+                          "traffic": (ftr * nodes if ftr is not None and
+                                      not swap else None),
                           "dtype": DTYPES[prec], "sm_mhz": fclk["sm_mhz"]}
 
     # --- end to end through the C ABI with host buffers ------------------

@@ -1267,6 +1267,7 @@ __device__ __forceinline__ void StagedInterior(const BlockDev& b,
         xs = (g - rl * tpr) * 64;
     };
     // copies of task t's windows into stage st (one group, maybe empty)
+    constexpr int kE = 16 / (int)sizeof(T);   // elements per copy
     auto issue = [&](int t, int st) {
         int r, xs;
         task(t, r, xs);
@@ -1279,8 +1280,7 @@ __device__ __forceinline__ void StagedInterior(const BlockDev& b,
                 const long long k0 =
                     (O32 ? node + b.pull_off32[i] : PullIndex<L>(b, node, i)) +
                     L::cx(i) - kLead;
-                CpAsync16(win + i * kWin + lane * (16 / (int)sizeof(T)),
-                          src + k0 + lane * (16 / (int)sizeof(T)));
+                CpAsync16(win + i * kWin + lane * kE, src + k0 + lane * kE);
             }
         }
         CpAsyncCommit();
