@@ -692,6 +692,15 @@ __device__ __forceinline__ void ApplyEqm(typename Prec<T>::C* f,
     }
 }
 
+// FDPeriodic (KerCutCellPeriodic3D, Src/boundary_kernel.inc:1278-1666):
+// f = the halo cell's f, which no step writes: f = 0.
+template <typename L, typename T>
+__device__ __forceinline__ void ApplyZero(typename Prec<T>::C* f,
+                                          const PhysConst& pc) {
+#pragma unroll
+    for (int i = 0; i < L::Q; i++) f[i] = FromF<T>(0.0, i, pc);
+}
+
 // Halfway bounce-back: f_i = g_opp(i)(x) + 2 w_i (c_i . u_wall); the same
 // for the deviation because w_opp(i) = w_i.
 template <typename L, typename T>
@@ -790,6 +799,7 @@ __device__ __forceinline__ void StepNode(const BlockDev& b,
             if (op.kind == kOpEqm) ApplyEqm<L, T>(f, op, pc, x, y, z);
             else if (op.kind == kOpHbb)
                 ApplyHbb<L, T>(f, op, pc, src, b, node, x, y, z);
+            else if (op.kind == kOpZero) ApplyZero<L, T>(f, pc);
         }
     }
     const bool fl = (rf & 4) != 0;
@@ -1479,6 +1489,8 @@ __device__ __forceinline__ void DeferredApply(const BlockDev& b,
         ApplyEqm<L, T>(f, op, pc, x, y, z);
     } else if (op.kind == kOpHbb) {
         ApplyHbb<L, T>(f, op, pc, src, b, NodeIndex<D>(b, x, y, z), x, y, z);
+    } else if (op.kind == kOpZero) {
+        ApplyZero<L, T>(f, pc);
     } else if (op.kind == kOpExtrapol) {
         int q[3] = {x, y, z};
         if (op.nb_axis >= 0) q[op.nb_axis] += op.nb_sign;
@@ -1515,6 +1527,8 @@ __device__ __forceinline__ void DeferredApply(const BlockDev& b,
                 else if (nop.kind == kOpHbb)
                     ApplyHbb<L, T>(g, nop, pc, src, b, nnode, q[0], q[1],
                                    q[2]);
+                else if (nop.kind == kOpZero)
+                    ApplyZero<L, T>(g, pc);
             }
         }
         if constexpr (P::kShifted) {

@@ -477,7 +477,66 @@ int PlanSwap(const Lat& L, BlockPlan& B, std::string* err) {
 bool Dispatched(int scheme) {
     return scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL ||
            scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST ||
-           scheme == MPLBGPU_BC_HALFWAY_BOUNCE_BACK;
+           scheme == MPLBGPU_BC_HALFWAY_BOUNCE_BACK ||
+           scheme == MPLBGPU_BC_FDPERIODIC;
+}
+
+// KerCutCellPeriodic(3D) (Src/boundary_kernel.inc:615-719, 1278-1666): the
+// copies f(node) = f(node + off) it makes at a node of geometry vg for the
+// boundary surface being treated, in its order (the edge and corner cases
+// compare the surface with face values, a few of them with a face other
+// than the one the offset crosses).  Returns the number of copies.
+int FdPeriodicCopies(int vg, int surface, int off[3][3]) {
+    int n = 0;
+    auto add = [&](bool when, int x, int y, int z) {
+        if (!when) return;
+        off[n][0] = x;
+        off[n][1] = y;
+        off[n][2] = z;
+        n++;
+    };
+    const bool L = surface == MPLBGPU_LEFT, R = surface == MPLBGPU_RIGHT,
+               T = surface == MPLBGPU_TOP, B = surface == MPLBGPU_BOTTOM,
+               F = surface == MPLBGPU_FRONT, K = surface == MPLBGPU_BACK;
+    switch (vg) {
+        case 10: add(true, -1, 0, 0); break;                 // IP
+        case 11: add(true, 1, 0, 0); break;                  // IM
+        case 20: add(true, 0, -1, 0); break;                 // JP
+        case 21: add(true, 0, 1, 0); break;                  // JM
+        case 30: add(true, 0, 0, -1); break;                 // KP
+        case 31: add(true, 0, 0, 1); break;                  // KM
+        case 10200: add(L, -1, 0, 0); add(B, 0, -1, 0); break;   // IPJP
+        case 10210: add(L, -1, 0, 0); add(T, 0, 1, 0); break;    // IPJM
+        case 11200: add(R, 1, 0, 0); add(B, 0, -1, 0); break;    // IMJP
+        case 11210: add(R, 1, 0, 0); add(T, 0, 1, 0); break;     // IMJM
+        case 10300: add(L, -1, 0, 0); add(K, 0, 0, -1); break;   // IPKP
+        case 10310: add(R, -1, 0, 0); add(F, 0, 0, 1); break;    // IPKM
+        case 11300: add(R, 1, 0, 0); add(K, 0, 0, -1); break;    // IMKP
+        case 11310: add(R, 1, 0, 0); add(F, 0, 0, 1); break;     // IMKM
+        case 20300: add(B, 0, -1, 0); add(K, 0, 0, -1); break;   // JPKP
+        case 20310: add(B, 0, -1, 0); add(F, 0, 0, 1); break;    // JPKM
+        case 21300: add(T, 0, 1, 0); add(F, 0, 0, -1); break;    // JMKP
+        case 21310: add(T, 0, 1, 0); add(F, 0, 0, 1); break;     // JMKM
+        case 1020300:                                             // IPJPKP
+            add(L, -1, 0, 0); add(B, 0, -1, 0); add(K, 0, 0, -1); break;
+        case 1020310:                                             // IPJPKM
+            add(L, -1, 0, 0); add(B, 0, -1, 0); add(F, 0, 0, 1); break;
+        case 1021300:                                             // IPJMKP
+            add(L, -1, 0, 0); add(T, 0, 1, 0); add(K, 0, 0, -1); break;
+        case 1021310:                                             // IPJMKM
+            add(T, -1, 0, 0); add(T, 0, 1, 0); add(F, 0, 0, 1); break;
+        case 1120300:                                             // IMJPKP
+            add(R, 1, 0, 0); add(B, 0, -1, 0); add(K, 0, 0, -1); break;
+        case 1120310:                                             // IMJPKM
+            add(R, 1, 0, 0); add(B, 0, -1, 0); add(F, 0, 0, 1); break;
+        case 1121300:                                             // IMJMKP
+            add(R, 1, 0, 0); add(T, 0, 1, 0); add(K, 0, 0, -1); break;
+        case 1121310:                                             // IMJMKM
+            add(R, 1, 0, 0); add(T, 0, 1, 0); add(F, 0, 0, 1); break;
+        default:
+            break;
+    }
+    return n;
 }
 
 }  // namespace
@@ -596,10 +655,9 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
             return fail(MPLBGPU_ERR_INVALID, "boundary on an unknown block");
         if (!ValidSurface(P.dim, bc.surface))
             return fail(MPLBGPU_ERR_INVALID, "invalid boundary surface");
-        if (bc.scheme == MPLBGPU_BC_FDPERIODIC)
+        if (bc.scheme == MPLBGPU_BC_FDPERIODIC && swap)
             return fail(MPLBGPU_ERR_UNSUPPORTED,
-                        "FDPeriodic copies from a halo of f that the "
-                        "reference never transfers (use MDPeriodic)");
+                        "FDPeriodic with the swap scheme");
         if (bc.vertex_type == kVtSolid ||
             bc.vertex_type == MPLBGPU_VT_IMMERSED_BOUNDARY)
             return fail(MPLBGPU_ERR_UNSUPPORTED,
@@ -705,14 +763,37 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                 int rg[6];
                 SurfaceRange(P.dim, B.n, bc.surface, rg);
                 if (!InRange(p, rg)) continue;
-                if (bc.scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL)
+                if (bc.scheme == MPLBGPU_BC_FDPERIODIC) {
+                    // every copy reads a halo cell of f (the offsets point
+                    // out of the block at the nodes of the surface): one
+                    // that no step transfers or writes, zero from the
+                    // start, so a node with any copy ends with f = 0
+                    int off[3][3];
+                    const int nc = FdPeriodicCopies(R.vg, bc.surface, off);
+                    if (nc == 0) continue;
+                    for (int c = 0; c < nc; c++)
+                        for (int a = 0; a < P.dim; a++) {
+                            if (off[c][a] == 0) continue;
+                            const int q = p[a] + off[c][a];
+                            if (R.ext[a] != 1 || (q >= 0 && q < B.n[a]))
+                                return fail(MPLBGPU_ERR_UNSUPPORTED,
+                                            "FDPeriodic copying from inside "
+                                            "the block");
+                        }
+                    RegionOp op{};
+                    op.kind = kOpZero;
+                    op.nb_axis = -1;
+                    op.out_mask = (1u << P.Q) - 1u;
+                    prog.push_back(op);
+                } else if (bc.scheme == MPLBGPU_BC_EQM_DIFFUSE_REFL) {
                     prog.push_back(MakeEqm(L, P.cs, nf, axis, sign, bc.given));
-                else if (bc.scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST)
+                } else if (bc.scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST) {
                     prog.push_back(MakeExtrapol(L, nf, axis, sign, bc.surface,
                                                 bc.given[0]));
-                else
+                } else {
                     prog.push_back(MakeHbb(L, P.cs, B.n, p, bc.surface,
                                            bc.given));
+                }
                 prog.back().bc = k;
             }
             bool extrapol = false;
@@ -725,7 +806,7 @@ int BuildPlan(const mplbgpu_desc& d, Plan* plan, std::string* err) {
                         if (op.out_mask >> l & 1u) reads |= 1u << L.opp[l];
                     readfirst |= reads & ~written;
                     written |= op.out_mask | op.par_mask;
-                } else if (op.kind == kOpHbb) {
+                } else if (op.kind == kOpHbb || op.kind == kOpZero) {
                     written |= op.out_mask;
                 }
             }

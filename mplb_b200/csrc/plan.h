@@ -34,7 +34,9 @@ constexpr int kMaxOps = 4;
 constexpr int kNumRegions = 27;
 
 enum NodeClass : int { kPure = 0, kLocal = 1, kDeferred = 2 };
-enum OpKind : int { kOpEqm = 1, kOpHbb = 2, kOpExtrapol = 3 };
+// kOpZero: FDPeriodic, which sets every population of the node to the
+// value of a halo cell of f that no step writes (zero)
+enum OpKind : int { kOpEqm = 1, kOpHbb = 2, kOpExtrapol = 3, kOpZero = 4 };
 
 // One boundary operation specialised to one region's geometry.  All FP64
 // constants that depend only on the boundary's given values are computed

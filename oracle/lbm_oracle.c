@@ -423,10 +423,9 @@ int lbmo_create(const mplbgpu_desc* d, lbm_oracle** out) {
             lbmo_destroy(o);
             return fail("bad surface");
         }
-        if (o->bc[i].scheme == MPLBGPU_BC_FDPERIODIC) {
+        if (o->bc[i].scheme == MPLBGPU_BC_FDPERIODIC && o->swap) {
             lbmo_destroy(o);
-            return fail("FDPeriodic reads a halo of f that is never "
-                        "transferred");
+            return fail("FDPeriodic with the swap scheme");
         }
         if (o->swap && (o->bc[i].scheme == MPLBGPU_BC_EXTRAPOL_PRESSURE_1ST ||
                         o->bc[i].scheme == MPLBGPU_BC_HALFWAY_BOUNCE_BACK)) {
@@ -709,6 +708,93 @@ int lbmo_set_f(lbm_oracle* o, int block, const double* f) {
                        sizeof(double) * o->Q);
             }
     return 0;
+}
+
+/* KerCutCellPeriodic(3D), Src/boundary_kernel.inc:615-719, 1278-1666:
+ * f(node) = f(node + off) for every population, for the offsets the
+ * kernel's switch takes at a node of geometry vg when it treats `surface`
+ * (edge and corner cases compare the surface with face values).  The
+ * sources are halo cells of f, which the step never writes. */
+static int fd_copies(int vg, int surface, int off[3][3]) {
+    int n = 0;
+#define FD_ADD(cond, x, y, z)                                               \
+    do {                                                                    \
+        if (cond) {                                                         \
+            off[n][0] = (x);                                                \
+            off[n][1] = (y);                                                \
+            off[n][2] = (z);                                                \
+            n++;                                                            \
+        }                                                                   \
+    } while (0)
+    const int L = surface == MPLBGPU_LEFT, R = surface == MPLBGPU_RIGHT,
+              T = surface == MPLBGPU_TOP, B = surface == MPLBGPU_BOTTOM,
+              F = surface == MPLBGPU_FRONT, K = surface == MPLBGPU_BACK;
+    switch (vg) {
+        case 10: FD_ADD(1, -1, 0, 0); break;
+        case 11: FD_ADD(1, 1, 0, 0); break;
+        case 20: FD_ADD(1, 0, -1, 0); break;
+        case 21: FD_ADD(1, 0, 1, 0); break;
+        case 30: FD_ADD(1, 0, 0, -1); break;
+        case 31: FD_ADD(1, 0, 0, 1); break;
+        case 10200: FD_ADD(L, -1, 0, 0); FD_ADD(B, 0, -1, 0); break;
+        case 10210: FD_ADD(L, -1, 0, 0); FD_ADD(T, 0, 1, 0); break;
+        case 11200: FD_ADD(R, 1, 0, 0); FD_ADD(B, 0, -1, 0); break;
+        case 11210: FD_ADD(R, 1, 0, 0); FD_ADD(T, 0, 1, 0); break;
+        case 10300: FD_ADD(L, -1, 0, 0); FD_ADD(K, 0, 0, -1); break;
+        case 10310: FD_ADD(R, -1, 0, 0); FD_ADD(F, 0, 0, 1); break;
+        case 11300: FD_ADD(R, 1, 0, 0); FD_ADD(K, 0, 0, -1); break;
+        case 11310: FD_ADD(R, 1, 0, 0); FD_ADD(F, 0, 0, 1); break;
+        case 20300: FD_ADD(B, 0, -1, 0); FD_ADD(K, 0, 0, -1); break;
+        case 20310: FD_ADD(B, 0, -1, 0); FD_ADD(F, 0, 0, 1); break;
+        case 21300: FD_ADD(T, 0, 1, 0); FD_ADD(F, 0, 0, -1); break;
+        case 21310: FD_ADD(T, 0, 1, 0); FD_ADD(F, 0, 0, 1); break;
+        case 1020300:
+            FD_ADD(L, -1, 0, 0); FD_ADD(B, 0, -1, 0); FD_ADD(K, 0, 0, -1);
+            break;
+        case 1020310:
+            FD_ADD(L, -1, 0, 0); FD_ADD(B, 0, -1, 0); FD_ADD(F, 0, 0, 1);
+            break;
+        case 1021300:
+            FD_ADD(L, -1, 0, 0); FD_ADD(T, 0, 1, 0); FD_ADD(K, 0, 0, -1);
+            break;
+        case 1021310:
+            FD_ADD(T, -1, 0, 0); FD_ADD(T, 0, 1, 0); FD_ADD(F, 0, 0, 1);
+            break;
+        case 1120300:
+            FD_ADD(R, 1, 0, 0); FD_ADD(B, 0, -1, 0); FD_ADD(K, 0, 0, -1);
+            break;
+        case 1120310:
+            FD_ADD(R, 1, 0, 0); FD_ADD(B, 0, -1, 0); FD_ADD(F, 0, 0, 1);
+            break;
+        case 1121300:
+            FD_ADD(R, 1, 0, 0); FD_ADD(T, 0, 1, 0); FD_ADD(K, 0, 0, -1);
+            break;
+        case 1121310:
+            FD_ADD(R, 1, 0, 0); FD_ADD(T, 0, 1, 0); FD_ADD(F, 0, 0, 1);
+            break;
+        default:
+            break;
+    }
+#undef FD_ADD
+    return n;
+}
+
+static void bc_fdperiodic(lbm_oracle* o, oblock* b, const int r[6],
+                          int surface) {
+    const int Q = o->Q;
+    for (int k = r[4]; k < r[5]; k++)
+        for (int j = r[2]; j < r[3]; j++)
+            for (int i = r[0]; i < r[1]; i++) {
+                const size_t p = pidx(b, i, j, k);
+                int off[3][3];
+                const int nc = fd_copies(b->vg[p], surface, off);
+                for (int c = 0; c < nc; c++) {
+                    const size_t q = pidx(b, i + off[c][0], j + off[c][1],
+                                          k + off[c][2]);
+                    for (int l = 0; l < Q; l++)
+                        b->f[p * Q + l] = b->f[q * Q + l];
+                }
+            }
 }
 
 /* KerCutCellEQMDiffuseRefl(3D), Src/boundary_kernel.inc:534-613,1184-1276 */
@@ -1031,6 +1117,9 @@ static void one_step(lbm_oracle* o) {
             case MPLBGPU_BC_HALFWAY_BOUNCE_BACK:
                 bc_halfway_bb(o, b, r, bc->surface, bc->given,
                               o->bc_field[i]);
+                break;
+            case MPLBGPU_BC_FDPERIODIC:
+                bc_fdperiodic(o, b, r, bc->surface);
                 break;
             default:
                 break; /* TreatBlockBoundary3D: no kernel dispatched */

@@ -9,6 +9,7 @@ import pytest
 
 import golden_cases
 import random_cases
+import special_cases
 from mplb_b200 import config
 
 
@@ -236,21 +237,16 @@ def test_oracle_matches_reference_bench_cases(oracle_mod, name):
 
 
 def test_reference_fdperiodic_breaks_the_run(oracle_mod):
-    """Why this path rejects FDPeriodic (MPLBGPU_ERR_UNSUPPORTED): the
-    reference's KerCutCellPeriodic3D copies f from the halo of f, which its
-    StreamCollision never transfers, so those nodes get zeros and the field
-    turns to NaN within a few steps (the reference run here, 10 steps of a
-    forced channel made x-periodic through FDPeriodic instead of
-    MDPeriodic)."""
+    """FDPeriodic as the reference runs it: KerCutCellPeriodic3D copies f
+    from the halo of f, which its StreamCollision never transfers, so those
+    nodes get zeros and the field turns to NaN within a few steps (10 steps
+    of a forced channel made x-periodic through FDPeriodic instead of
+    MDPeriodic).  The restatement copies from its own untouched halo of f the
+    same way and gives the same field: zeros and NaNs at the same places,
+    every other value bit for bit."""
     if not oracle_mod.reference_available():
         pytest.skip("reference build (oracle/_ref) not present")
-    c = config.poiseuille(3, 8, 7, 6, g_lattice=1e-4)
-    bcs = [dataclasses.replace(b, scheme="FDPeriodic", vertex_type="FDPeriodic")
-           if b.surface in ("Left", "Right") else b for b in c.boundaries]
-    conns = [dataclasses.replace(x, type="FDPeriodic")
-             if x.from_surface in ("Left", "Right") else x
-             for x in c.connections]
-    case = dataclasses.replace(c, boundaries=bcs, connections=conns)
+    case = special_cases.fdperiodic_channel()
     case.check_period = 5
     ref = oracle_mod.run_reference(case, 10)
     f = ref["f"][0]
@@ -260,3 +256,30 @@ def test_reference_fdperiodic_breaks_the_run(oracle_mod):
     # the residual of rho is 0/0 (every interior rho is NaN but the sums
     # skip nothing): the reference reports NaN for u, v, w at least
     assert np.isnan(ref["residual"][-1][2][1:]).all()
+    o = oracle_mod.Oracle(case)
+    o.init_uniform()
+    o.step(10)
+    got = o.f(0)
+    assert np.array_equal(np.isnan(got), np.isnan(f))
+    assert np.array_equal(got[~np.isnan(got)], f[~np.isnan(f)])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_oracle_fdperiodic_edges_match_reference(oracle_mod, dim):
+    """FDPeriodic and EQMDiffuseRefl mixed over a cavity's faces: the
+    restatement's copies at faces, edges and corners (the reference's
+    mislabelled edge and corner cases included) against the reference,
+    NaNs at the same places and every other value bit for bit."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    case = special_cases.fdperiodic_box(dim)
+    case.check_period = 3
+    ref = oracle_mod.run_reference(case, 3)
+    o = oracle_mod.Oracle(case)
+    o.init_uniform()
+    o.step(3)
+    got, want = o.f(0), ref["f"][0]
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    assert np.array_equal(got[~np.isnan(got)], want[~np.isnan(want)])
+    assert (got == 0.0).any()
+

@@ -9,6 +9,7 @@ import pytest
 
 import golden_cases
 import random_cases
+import special_cases
 from mplb_b200 import abi, build, config
 
 
@@ -128,8 +129,8 @@ REJECTED = {
                                 abi.ERR_INVALID, "surface"),
     "bc_surface_value": (cav3, set_bc(1, surface=99), abi.ERR_INVALID,
                          "surface"),
-    "fdperiodic": (cav3, set_bc(0, scheme=abi.BC_SCHEMES["FDPeriodic"]),
-                   abi.ERR_UNSUPPORTED, "FDPeriodic"),
+    "fdperiodic_swap": (swap3, set_bc(0, scheme=abi.BC_SCHEMES["FDPeriodic"]),
+                        abi.ERR_UNSUPPORTED, "FDPeriodic"),
     "immersed_solid": (cav3, set_bc(3, vertex_type=abi.VERTEX_TYPES[
         "ImmersedSolid"]), abi.ERR_UNSUPPORTED, "immersed"),
     "connection_unknown_block": (two_blocks, set_conn(0, to_block=9),
@@ -164,6 +165,7 @@ def accepted_cases():
         out[f"swap_{p}"] = lambda p=p: swap3(precision=p)
     out["lchannel_bb"] = lambda: config.lchannel(leg=9, side=6, depth=4,
                                                  wall="HalfwayBounceBack")
+    out["fdperiodic"] = special_cases.fdperiodic_channel
     out["slab_middle"] = lambda: with_cut(
         dataclasses.replace(cav3(), boundaries=[
             b for b in cav3().boundaries
