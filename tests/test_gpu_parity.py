@@ -122,7 +122,8 @@ def test_mass_conserved_in_closed_cavity(gpu_lib):
 
 
 def test_errors_are_reported(gpu_lib):
-    case = config.cavity(2, 8, 0.05, re=10)
+    case = config.cavity(3, 8, 0.05, re=10,
+                         scheme="Scheme_StreamCollision_Swap")
     case.boundaries[0].scheme = "FDPeriodic"
     with pytest.raises(MplbGpuError) as e:
         Solver(case)
