@@ -19,8 +19,9 @@
 //            are bit-identical to the reference.
 //   float  : the shifted deviation h_i = f_i - w_i in FP32 with FP32
 //            arithmetic (rho = 1 + sum h, feq - w computed directly).
-//   __half : the same deviation normalised by its weight, h_i / w_i, in
-//            FP16 storage; arithmetic in FP32.
+//   __half : the same deviation scaled by its weight, 256 h_i / w_i, in
+//            FP16 storage (stochastic rounding); arithmetic in FP32, the
+//            interior pairs' on the stored values themselves.
 // Moments, residuals and the side stores are FP64 in every form.
 #pragma once
 

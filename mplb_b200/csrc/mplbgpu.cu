@@ -1,6 +1,7 @@
 // C ABI of the B200 stream-collision path (include/mplbgpu.h).
 //
-// A context owns one CUDA stream and, per block, two population arrays in
+// A context owns one CUDA stream (and side streams that a step forks from
+// it and joins back before it returns) and, per block, two population arrays in
 // the halo layout of kernels.cuh (ping-pong between steps; one array updated
 // in place under the swap scheme, swap.cuh), the boundary
 // tables produced by plan.cpp, the stale/deferred stores and the dense
