@@ -192,6 +192,14 @@ void FreeAll(mplbgpu_ctx* c) {
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
+// n doubles set to v (a macroscopic field not given at initialisation).
+__global__ void FillDoubleKernel(double* __restrict__ p, long long n,
+                                 double v) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         e < n; e += (long long)gridDim.x * blockDim.x)
+        p[e] = v;
+}
+
 // A population array of the context's storage form set to f = 0.
 cudaError_t FillZeroF(mplbgpu_ctx* c, void* p, long long popstride) {
     const int Q = c->plan.Q;
@@ -876,17 +884,15 @@ mplbgpu_status mplbgpu_init_macro(mplbgpu_ctx* ctx, int block,
     const int dim = ctx->plan.dim;
     const size_t nodes = (size_t)B->nodes();
     const double* src[4] = {rho, u, v, w};
-    std::vector<double> fill;   // host staging only for fields not given
     for (int m = 0; m < dim + 1; m++) {
         if (src[m]) {
             CK(cudaMemcpyAsync(b->macro[m], src[m], nodes * sizeof(double),
                                cudaMemcpyHostToDevice, ctx->stream));
         } else {
-            fill.resize(nodes);
-            std::fill(fill.begin(), fill.end(), m == 0 ? 1.0 : 0.0);
-            CK(cudaMemcpyAsync(b->macro[m], fill.data(), nodes * sizeof(double),
-                               cudaMemcpyHostToDevice, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            // a field not given: rho = 1, velocity components 0
+            FillDoubleKernel<<<1024, 256, 0, ctx->stream>>>(
+                b->macro[m], (long long)nodes, m == 0 ? 1.0 : 0.0);
+            CK_LAUNCH();
         }
         // CopyCurrentMacroVar after PreDefinedInitialCondition3D
         CK(cudaMemcpyAsync(b->macro_old[m], b->macro[m], nodes * sizeof(double),
