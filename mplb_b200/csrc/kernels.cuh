@@ -738,9 +738,6 @@ __device__ __forceinline__ void ApplyHbb(typename Prec<T>::C* f,
 #ifndef MPLB_F64_MIN_BLOCKS
 #define MPLB_F64_MIN_BLOCKS 5
 #endif
-#ifndef MPLB_F16_MIN_BLOCKS
-#define MPLB_F16_MIN_BLOCKS MPLB_LP_MIN_BLOCKS
-#endif
 // One node of the step, any region class.
 template <int D, typename T, int MODE, bool O32>
 __device__ __forceinline__ void StepNode(const BlockDev& b,
@@ -1171,11 +1168,6 @@ constexpr int kSplitWarps = kSplitCta / 32;
 #ifndef MPLB_LP_STAGED
 #define MPLB_LP_STAGED 1
 #endif
-// 1: the staged FP16 pairs read their populations from shared memory where
-// they are used (StagedHalfPair), 0: into registers first (PairFinish)
-#ifndef MPLB_F16_LAZY
-#define MPLB_F16_LAZY 0
-#endif
 #ifndef MPLB_STAGE_TASKS
 #define MPLB_STAGE_TASKS 8
 #endif
@@ -1253,153 +1245,6 @@ __device__ __forceinline__ void CpAsyncWait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// An FP16 node pair of the staged interior computed straight from its
-// shared-memory windows: MomentsCollideScaledPair and PairFinish's stores
-// with the same operations in the same order (the same bits), each
-// population read from shared memory where it is used and each m_i
-// evaluated again in the update instead of held, so the pair keeps no
-// per-population registers between the passes.  `win` points at the
-// lane's column of the first population's window.
-template <int D, bool O32, int kWin>
-__device__ __forceinline__ void StagedHalfPair(const BlockDev& b,
-                                               const PhysConst& pc,
-                                               __half* __restrict__ dst,
-                                               long long node, bool v0,
-                                               bool v1,
-                                               const __half* __restrict__ win) {
-    using L = Lattice<D>;
-    using O = VOps<float2>;
-    constexpr int Q = L::Q;
-    const bool fl = b.center_fluid != 0;
-    // volatile: each read stays where it is used (the compiler would
-    // otherwise hoist all of them and hold the values in registers)
-    auto sv = [&](int i) {
-        const volatile unsigned short* p =
-            reinterpret_cast<const volatile unsigned short*>(win + i * kWin -
-                                                             L::cx(i));
-        return make_float2(__half2float(__ushort_as_half(p[0])),
-                           __half2float(__ushort_as_half(p[32])));
-    };
-    auto wl = [&](int i) { return O::splat(pc.wlf[i]); };
-    // moments
-    float2 drho = O::mul(sv(0), wl(0));
-#pragma unroll
-    for (int i = 1; i < Q; i++)
-        if (i < L::opp(i))
-            drho = O::fma(O::add(sv(i), sv(L::opp(i))), wl(i), drho);
-    const float2 rho = O::add(O::splat(1.0f), drho);
-    const float2 rinv = O::rcp(rho);
-    float2 u[3];
-#pragma unroll
-    for (int a = 0; a < L::D; a++) {
-        float2 j = O::splat(0.0f);
-        bool first = true;
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-            if (comp<L>(i, a) > 0) {
-                const float2 d = O::sub(sv(i), sv(L::opp(i)));
-                j = first ? O::mul(d, wl(i)) : O::fma(d, wl(i), j);
-                first = false;
-            }
-        }
-        j = O::mul(O::mul(O::splat(pc.csf), j), rinv);
-        if (pc.force_vel && fl) j = O::add(j, O::splat(pc.hdtaf[a]));
-        u[a] = j;
-    }
-    if (L::D == 2) u[2] = O::splat(0.0f);
-    const float2 hr = O::mul(O::splat(0.5f), rho);
-    const float2 csf = O::splat(pc.csf);
-    const float2 comps[3] = {O::mul(csf, u[0]), O::mul(csf, u[1]),
-                             O::mul(csf, u[2])};
-    const float2 u2 =
-        O::fma(u[0], u[0], O::fma(u[1], u[1], O::mul(u[2], u[2])));
-    const float2 half = O::splat(0.5f);
-    const float2 nscale = O::splat(-kHalfScale);
-    auto cu_of = [&](int i) {
-        float2 cu = O::splat(0.0f);
-        bool first = true;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const int c = comp<L>(i, a);
-            if (c == 0 || a >= L::D) continue;
-            const float2 t = c > 0 ? comps[a] : O::neg(comps[a]);
-            cu = first ? t : O::add(cu, t);
-            first = false;
-        }
-        return cu;
-    };
-    // m_i of the pair (i, opp(i)), i < opp(i): (m_i, m_opp(i))
-    auto m_pair = [&](int i, float2& mi, float2& mj) {
-        const float2 cu = cu_of(i);
-        const float2 y = O::fma(cu, cu, O::neg(u2));
-        mi = O::fma(nscale, O::fma(rho, O::fma(half, y, cu), drho), sv(i));
-        mj = O::fma(nscale, O::fma(rho, O::fma(half, y, O::neg(cu)), drho),
-                    sv(L::opp(i)));
-    };
-    auto m_rest = [&]() {
-        return O::fma(nscale, O::fma(O::neg(hr), u2, drho), sv(0));
-    };
-    float2 m0 = O::mul(m_rest(), wl(0)), mv0 = O::splat(0.0f),
-           mv1 = O::splat(0.0f), mv2 = O::splat(0.0f);
-#pragma unroll
-    for (int i = 1; i < Q; i++) {
-        if (i > L::opp(i)) continue;
-        float2 mi, mj;
-        m_pair(i, mi, mj);
-        m0 = O::fma(O::add(mi, mj), wl(i), m0);
-        const float2 d = O::mul(O::sub(mi, mj), wl(i));
-        if (L::cx(i) > 0) mv0 = O::add(mv0, d);
-        if (L::cx(i) < 0) mv0 = O::sub(mv0, d);
-        if (L::cy(i) > 0) mv1 = O::add(mv1, d);
-        if (L::cy(i) < 0) mv1 = O::sub(mv1, d);
-        if (L::cz(i) > 0) mv2 = O::add(mv2, d);
-        if (L::cz(i) < 0) mv2 = O::sub(mv2, d);
-    }
-    if (pc.force_vel && fl) {
-        mv0 = O::fma(rho, O::splat(pc.hdta_csf[0]), mv0);
-        mv1 = O::fma(rho, O::splat(pc.hdta_csf[1]), mv1);
-        mv2 = O::fma(rho, O::splat(pc.hdta_csf[2]), mv2);
-    }
-    const float2 three = O::splat(3.0f);
-    mv0 = O::mul(mv0, three);
-    mv1 = O::mul(mv1, three);
-    mv2 = O::mul(mv2, three);
-    const float2 om = O::splat(1.0f - pc.omcf);
-    const bool force = pc.force && fl;
-    const float2 fr = O::mul(O::splat(pc.tw_omf), rho);
-    const float2 scale = O::splat(kHalfScale);
-    const Rng rg = SeedRng(pc.seed, v0 ? node : node + 32);
-    // update and store population i from its m_i
-    auto relax_store = [&](int i, float2 mi) {
-        float2 cm = m0;
-        if (L::cx(i) > 0) cm = O::add(cm, mv0);
-        if (L::cx(i) < 0) cm = O::sub(cm, mv0);
-        if (L::cy(i) > 0) cm = O::add(cm, mv1);
-        if (L::cy(i) < 0) cm = O::sub(cm, mv1);
-        if (L::cz(i) > 0) cm = O::add(cm, mv2);
-        if (L::cz(i) < 0) cm = O::sub(cm, mv2);
-        float2 t = O::fma(scale, cm, O::neg(mi));
-        if (force) t = O::fma(fr, O::splat(pc.cf256f[i]), t);
-        const float2 s = O::fma(om, t, sv(i));
-        const uint32_t pair = StochasticHalf2(s.x, s.y, SrDraw32(rg, i));
-        const long long k = O32 ? node + b.pop_off32[i] : OwnIndex(b, node, i);
-        if (v0)
-            PopStore(dst + k, __ushort_as_half((unsigned short)(pair & 0xffffu)));
-        if (v1)
-            PopStore(dst + k + 32,
-                     __ushort_as_half((unsigned short)(pair >> 16)));
-    };
-    relax_store(0, m_rest());
-#pragma unroll
-    for (int i = 1; i < Q; i++) {
-        if (i > L::opp(i)) continue;
-        float2 mi, mj;
-        m_pair(i, mi, mj);
-        relax_store(i, mi);
-        relax_store(L::opp(i), mj);
-    }
-}
-
 // The staged interior of one CTA of a chunk (see StagedStep): warp k takes
 // the chunk's tasks (w - 1) kSplitWarps kStageTasks + k kStageTasks + t,
 // t < kStageTasks (task -> row t / tasks per row, segment t % tasks per
@@ -1467,22 +1312,17 @@ __device__ __forceinline__ void StagedInterior(const BlockDev& b,
                 const T* win = stages + (t % S) * Q * kWin + lane + kLead;
                 const long long node = NodeIndexT<D, O32>(
                     b, x0, 1 + r % ny, D == 3 ? 1 + r / ny : 0);
-                if constexpr (std::is_same<T, __half>::value && MPLB_F16_LAZY) {
-                    StagedHalfPair<D, O32, kWin>(b, pc, dst, node, v0, v1,
-                                                 win);
-                } else {
-                    float2 h[Q];
+                float2 h[Q];
 #pragma unroll
-                    for (int i = 0; i < Q; i++) {
-                        const T* p = win + i * kWin - L::cx(i);
-                        if constexpr (std::is_same<T, __half>::value)
-                            h[i] = make_float2(__half2float(p[0]),
-                                               __half2float(p[32]));
-                        else
-                            h[i] = make_float2((float)p[0], (float)p[32]);
-                    }
-                    PairFinish<D, T, O32>(b, pc, dst, node, v0, v1, h);
+                for (int i = 0; i < Q; i++) {
+                    const T* p = win + i * kWin - L::cx(i);
+                    if constexpr (std::is_same<T, __half>::value)
+                        h[i] = make_float2(__half2float(p[0]),
+                                           __half2float(p[32]));
+                    else
+                        h[i] = make_float2((float)p[0], (float)p[32]);
                 }
+                PairFinish<D, T, O32>(b, pc, dst, node, v0, v1, h);
             }
         }
         __syncwarp();   // every lane is done with stage t % S
@@ -1507,8 +1347,6 @@ __device__ __forceinline__ void StagedInterior(const BlockDev& b,
 template <int D, typename T, bool O32>
 __global__ void __launch_bounds__(128, std::is_same<T, double>::value
                                            ? MPLB_F64_MIN_BLOCKS
-                                       : std::is_same<T, __half>::value
-                                           ? MPLB_F16_MIN_BLOCKS
                                            : MPLB_LP_MIN_BLOCKS)
     SplitStepKernel(BlockDev b, PhysConst pc, const T* __restrict__ src,
                     T* __restrict__ dst, unsigned blk0, unsigned spc) {
