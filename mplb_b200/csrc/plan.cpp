@@ -450,7 +450,7 @@ int PlanSwap(const Lat& L, BlockPlan& B, std::string* err) {
                 }
             }
             if (outside) continue;
-            int verdict = -1;
+            int exchanges = -1;
             for (int i0 = 0; i0 < nopt[0]; i0++)
                 for (int i1 = 0; i1 < nopt[1]; i1++)
                     for (int i2 = 0; i2 < nopt[2]; i2++) {
@@ -461,14 +461,14 @@ int PlanSwap(const Lat& L, BlockPlan& B, std::string* err) {
                         int za[3], zs[3];
                         const int zf = NodeFaces(3, B.n, Z.org, za, zs);
                         const int e = SwapExchanges(L, Z.vt, zf, za, zs, k);
-                        if (verdict >= 0 && verdict != e) {
+                        if (exchanges >= 0 && exchanges != e) {
                             *err = "swap exchange pattern differs within a "
                                    "region";
                             return MPLBGPU_ERR_UNSUPPORTED;
                         }
-                        verdict = e;
+                        exchanges = e;
                     }
-            if (verdict == 1) B.swap_exch[r] |= 1u << k;
+            if (exchanges == 1) B.swap_exch[r] |= 1u << k;
         }
     }
     return MPLBGPU_OK;
